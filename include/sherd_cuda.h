@@ -1,0 +1,316 @@
+/*
+ * sherd_cuda.h — C ABI of the B200 geometry backend for sherd-refit.
+ *
+ * This is the drop-in boundary. It mirrors the reference's `Executor` trait
+ * (crates/sherd-core/src/executor/mod.rs:105-137) method for method, adds the
+ * `cone_cast` extension the trait's own documentation reserves for the
+ * preprocessing rays (executor/mod.rs:9-10), and adds the batched
+ * ladder + verification entry point that replaces the per-rung, per-candidate
+ * call pattern of `Pair::stage2_batch` (matching/pair.rs:298-372).
+ *
+ * Conventions
+ *  - Every entry point returns an int status: SHERD_OK (0) or a negative
+ *    SHERD_E_* code. `sherd_last_error(ctx)` holds a message for the calling
+ *    thread's last failure. There is no CPU fallback: a failure is reported,
+ *    never answered on the host.
+ *  - Host arrays are caller-owned and copied in (or written out) during the
+ *    call. Device objects are opaque handles with explicit *_free calls.
+ *  - 4x4 poses are 16 doubles, row-major, mapping the moving fragment's frame
+ *    into the fixed one (the reference's `Matrix4<f64>`, written row by row).
+ *  - Points are f64 triples (the reference's `[[f64; 3]]` batches); triangle
+ *    meshes are f32 vertices (the reference's `RayScene` is f32,
+ *    spatial/bvh.rs:43-50) and u32 faces.
+ *  - A context is thread-safe: calls from several host threads serialise on
+ *    an internal lock and run on the context's stream.
+ */
+#ifndef SHERD_CUDA_H
+#define SHERD_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SHERD_OK 0
+#define SHERD_E_INVALID (-1)  /* bad argument (null, size, NaN pose, ...)  */
+#define SHERD_E_OOM (-2)      /* device allocation failed                    */
+#define SHERD_E_TIMEOUT (-3)  /* a kernel ran past the context's time budget */
+#define SHERD_E_ABORTED (-4)  /* sherd_abort() was called during the call    */
+#define SHERD_E_DEVICE (-5)   /* CUDA runtime error                          */
+#define SHERD_E_EMPTY (-6)    /* a result needs data the input does not have */
+
+/* ---- POD types shared with the host side ------------------------------- */
+
+/* InsideOutcome (executor/batch.rs:339-368): 8 bytes, depth when inside. */
+typedef struct sherd_inside_outcome {
+    float depth;
+    uint32_t inside;
+} sherd_inside_outcome;
+
+/* DistReduce (executor/batch.rs:270-281). */
+enum { SHERD_REDUCE_ALL = 0, SHERD_REDUCE_MIN = 1 };
+
+/* Estimation (matching/icp.rs:77-84). */
+enum { SHERD_POINT_TO_POINT = 0, SHERD_POINT_TO_PLANE = 1 };
+
+/* Options (matching/icp.rs:139-152), under the reference numerics. */
+typedef struct sherd_icp_options {
+    int32_t estimation;
+    int32_t max_iteration;
+    double max_correspondence_distance;
+} sherd_icp_options;
+
+/* Registration (matching/icp.rs:181-195). */
+typedef struct sherd_registration {
+    double transform[16];
+    double fitness;
+    double inlier_rmse;
+    uint64_t correspondences;
+    uint32_t iterations;
+    uint32_t converged;
+} sherd_registration;
+
+/* Scales (matching/scales.rs:28-56), field for field. */
+typedef struct sherd_scales {
+    double t, res, coarse, stage1, tight, facing, gap, seam, near, pen, nms, icp;
+} sherd_scales;
+
+/* The five limits of R 6.5's accept rule (matching/verify.rs:632-638) and the
+ * thresholds of Params (params.rs:141-190) that Scales::for_pair reads. */
+typedef struct sherd_params {
+    double min_tight, max_gap, max_pen, min_seam, min_cont_n;
+    double coarse_delta, stage1_delta, tight_delta, facing_delta, seam_delta,
+        near_delta, pen_delta, nms_delta, icp_delta;
+    double coarse_res, stage1_res, tight_res, facing_res, gap_res, seam_res,
+        near_res, pen_res, icp_res;
+} sherd_params;
+
+/* Scores (matching/verify.rs:72-135): the twenty numbers of R 6. */
+typedef struct sherd_scores {
+    double tight_a, tight_b, tight;
+    double gap_a, gap_b, gap;
+    double contact_a, contact_b, contact;
+    double seam, gap_limit, tight_delta;
+    double cont, cont_n;
+    double pen, pen_depth;
+    uint32_t pen_unavailable, partial;
+    double brk, brk_best;
+} sherd_scores;
+
+/* One (pair, start) of the batched stage-2 path. */
+typedef struct sherd_work_item {
+    uint32_t pair;   /* index into the pairs array of the batch call   */
+    uint32_t start;  /* caller's own id for the start, copied through  */
+    double init[16]; /* stage-1 pose the 4-rung ladder starts from     */
+} sherd_work_item;
+
+/* What one work item produces: every rung's registration (the fixture
+ * carries all four, s2.T_reg1..s2.T_frac2), the R 6 scores at the last
+ * pose and the R 6.5 verdict. */
+typedef struct sherd_candidate {
+    uint32_t pair;
+    uint32_t start;
+    uint32_t accepted;
+    uint32_t status; /* 0 ok; otherwise a SHERD_E_* code for this item   */
+    sherd_registration rungs[4];
+    sherd_scores scores;
+} sherd_candidate;
+
+/* Scheduling of sherd_ladder_verify_batch. */
+enum {
+    SHERD_SCHED_BATCHED = 0, /* every item in persistent kernels, one graph */
+    SHERD_SCHED_PLAIN = 1    /* one launch sequence per pair, synchronised  */
+};
+
+/* ---- opaque handles ---------------------------------------------------- */
+typedef struct sherd_ctx sherd_ctx;
+typedef struct sherd_mesh sherd_mesh;         /* triangle LBVH, f32       */
+typedef struct sherd_cloud sherd_cloud;       /* point LBVH, f64 + normals */
+typedef struct sherd_surfaces sherd_surfaces; /* one fragment as R 6 reads it */
+typedef struct sherd_pair sherd_pair;         /* two fragments + ladder clouds */
+
+/* ---- context ----------------------------------------------------------- */
+
+/* Opens device `device` (cudaSetDevice) and creates a context with its own
+ * stream. Replaces the reference's backend resolution of a GPU executor
+ * (crates/sherd-backend/src/lib.rs:377-484): it fails instead of falling back. */
+int sherd_open(int device, sherd_ctx **out);
+int sherd_close(sherd_ctx *ctx);
+/* Message of the calling thread's last failure on this context ("" if none). */
+const char *sherd_last_error(const sherd_ctx *ctx);
+/* Kernel time budget in milliseconds for the persistent kernels (0 = none).
+ * A kernel past its budget stops taking work and the call returns
+ * SHERD_E_TIMEOUT; no device wait is unbounded. */
+int sherd_set_timeout_ms(sherd_ctx *ctx, uint32_t ms);
+/* Sets the host-mapped abort flag the persistent kernels poll; the running
+ * call returns SHERD_E_ABORTED. Cleared at the start of every batch call.
+ * Mirrors the reference's cancellation flag (progress.rs:38-106). */
+int sherd_abort(sherd_ctx *ctx);
+/* A JSON object of per-method call counts, items and device milliseconds.
+ * Mirrors the wgpu executor's Stats (sherd-gpu/src/executor.rs:50-216). */
+int sherd_stats_json(sherd_ctx *ctx, char *buf, size_t len);
+/* Executor::name (executor/mod.rs:107): "cuda". */
+const char *sherd_name(void);
+/* Executor::device_slack (executor/mod.rs:134-136). */
+uint32_t sherd_device_slack(const sherd_ctx *ctx);
+
+/* ---- meshes (RayScene, spatial/bvh.rs:36-192) -------------------------- */
+
+/* Uploads a triangle mesh and builds its LBVH on the device.
+ * RayScene::of_mesh (spatial/bvh.rs:56-62). nf == 0 is SHERD_E_EMPTY, as
+ * RayScene refuses an empty mesh. */
+int sherd_mesh_upload(sherd_ctx *ctx, const float *v, uint32_t nv,
+                      const uint32_t *f, uint32_t nf, sherd_mesh **out);
+/* The faces `keep[i] != 0` selects, on the same vertices, falling back to the
+ * first face when nothing is selected. RayScene::of_subset (bvh.rs:71-78). */
+int sherd_mesh_subset(sherd_ctx *ctx, const sherd_mesh *mesh,
+                      const uint8_t *keep, sherd_mesh **out);
+int sherd_mesh_free(sherd_mesh *mesh);
+/* RayScene::aabb (bvh.rs:182-185) and RayScene::n_faces (bvh.rs:189-191). */
+int sherd_mesh_aabb(const sherd_mesh *mesh, float lo[3], float hi[3]);
+uint32_t sherd_mesh_faces(const sherd_mesh *mesh);
+
+/* RayScene::first_hit (bvh.rs:84-90) for n rays: t in units of |dir|,
+ * +inf and 0xFFFFFFFF on a miss. Tie rule: smallest t, then lowest face
+ * index (face indices are those of the uploaded mesh, or of the subset). */
+int sherd_first_hit(sherd_ctx *ctx, const sherd_mesh *mesh, const float *origins,
+                    const float *dirs, uint32_t n, float *t_out, uint32_t *prim_out);
+
+/* Executor::bounded_distance (executor/mod.rs:118, cpu.rs:84-113): points
+ * moved by `pose` in f64, narrowed to f32, distance to the nearest triangle
+ * when it is <= (float)max_dist, else +inf. REDUCE_MIN writes one value, the
+ * minimum (the shrinking-window scan of cpu.rs:98-111). */
+int sherd_bounded_distance(sherd_ctx *ctx, const sherd_mesh *mesh,
+                           const double *points, uint32_t n, const double pose[16],
+                           double max_dist, int reduce, double *out);
+
+/* Executor::inside (executor/mod.rs:121, cpu.rs:115-128, bvh.rs:146-175):
+ * AABB reject, then the majority of three axis-ray parities; depth is the
+ * unbounded point-to-surface distance of an inside point. */
+int sherd_inside(sherd_ctx *ctx, const sherd_mesh *mesh, const double *points,
+                 uint32_t n, const double pose[16], sherd_inside_outcome *out);
+
+/* ---- preprocessing rays: the cone_cast extension ----------------------- */
+
+/* mesh::geometry::face_geometry (mesh/geometry.rs:70-96) in f64 on the
+ * device: unit normals (floor 1e-12), areas and centroids. Outputs nf*3,
+ * nf and nf*3 doubles; any output may be NULL. */
+int sherd_face_geometry(sherd_ctx *ctx, const double *v, uint32_t nv,
+                        const uint32_t *f, uint32_t nf, double *normals,
+                        double *areas, double *centroids);
+
+/* R 3.2 wall thickness (fragment/thickness.rs:99-162): one inward ray per
+ * sampled face (stride ceil(nf / max_rays)), the 60-bin histogram mode over
+ * [0, p90] and the looks-back filter. `found` is 0 when fewer than 100 rays
+ * hit (the reference's signal for its OBB fallback). t_hit/prim (nullable,
+ * ceil(nf/stride) entries) receive the raw hits. */
+int sherd_thickness(sherd_ctx *ctx, const sherd_mesh *mesh, const double *centroids,
+                    const double *normals, uint32_t nf, uint32_t max_rays,
+                    float *t, float *thick_mode, uint32_t *found, float *t_hit,
+                    uint32_t *prim);
+
+/* R 3.2 from given hits (thickness.rs:139-162): the reference's injected
+ * mode, fed a fixture's thick.idx / t_hit / prim. Runs on the device. */
+int sherd_thickness_from_hits(sherd_ctx *ctx, const double *normals, uint32_t nf,
+                              const uint32_t *idx, const float *t_hit,
+                              const uint32_t *prim, uint32_t n, float *t,
+                              float *thick_mode, uint32_t *found);
+
+/* R 3.4.3 cone vote (fragment/segment.rs:318-376): seven rays per face round
+ * -NS within 15 degrees; `good[i]` counts the rays that reach the far wall.
+ * centroids/normals are the f64 face geometry, ns the smoothed normals,
+ * hit_normals the normals the hit face is judged by. */
+int sherd_cone_votes(sherd_ctx *ctx, const sherd_mesh *mesh, const double *centroids,
+                     const double *normals, const double *ns,
+                     const double *hit_normals, uint32_t nf, double thick,
+                     uint8_t *good);
+
+/* ---- point clouds (PointTree, spatial/kdtree.rs:31-258) ---------------- */
+
+/* Uploads a point cloud (and optional unit normals) and builds its point
+ * LBVH. np == 0 is SHERD_E_EMPTY, as PointTree::build refuses it. */
+int sherd_cloud_upload(sherd_ctx *ctx, const double *points, const double *normals,
+                       uint32_t np, sherd_cloud **out);
+int sherd_cloud_free(sherd_cloud *cloud);
+uint32_t sherd_cloud_points(const sherd_cloud *cloud);
+
+/* PointTree::nearest_within_squared (kdtree.rs:202-217): nearest point with
+ * d2 <= r2 (inclusive), lowest index on exact ties; miss = 0xFFFFFFFF, +inf. */
+int sherd_nearest_within_sq(sherd_ctx *ctx, const sherd_cloud *cloud,
+                            const double *queries, uint32_t n, double r2,
+                            uint32_t *idx, double *d2);
+/* PointTree::nearest_below (kdtree.rs:182-190): the unbounded nearest when
+ * sqrt(d2) < bound, else a miss. The NN queries/s unit. */
+int sherd_nearest_below(sherd_ctx *ctx, const sherd_cloud *cloud,
+                        const double *queries, uint32_t n, double bound,
+                        uint32_t *idx, double *dist);
+
+/* ---- ICP (matching/icp.rs:308-440) ------------------------------------- */
+
+/* Executor::icp_rung (executor/mod.rs:114, cpu.rs:70-82): one
+ * registration_icp per init, every candidate an independent rung. Only
+ * point-to-plane is implemented on the device (the stage-1 point-to-point
+ * rung returns SHERD_E_INVALID). The target cloud must carry normals. */
+int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source,
+                   const sherd_cloud *target, const double *inits, uint32_t k,
+                   sherd_icp_options options, sherd_registration *out);
+
+/* ---- verification (matching/verify.rs) ---------------------------------- */
+
+/* Surfaces (verify.rs:223-299): one fragment as R 6 reads it. `fracture` is
+ * the fracture-face scene, `mesh` the whole working mesh (NULL leaves the
+ * penetration test unavailable). Points are copied to the device. */
+int sherd_surfaces_create(sherd_ctx *ctx, const sherd_mesh *fracture,
+                          const sherd_mesh *mesh, uint32_t watertight,
+                          double frac_area, const double *pf, uint32_t n_pf,
+                          const double *s, uint32_t n_s, const double *brk_p,
+                          const double *brk_ns, uint32_t n_brk,
+                          const double *margin_p, const double *margin_n,
+                          uint32_t n_margin, sherd_surfaces **out);
+int sherd_surfaces_free(sherd_surfaces *s);
+
+/* verify::verify (verify.rs:590-626) for one pose, every score on the device.
+ * full = 0 computes only the fracture scores and the seam (partial = 1). */
+int sherd_verify(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfaces *b,
+                 const double pose[16], const sherd_scales *sc, int full,
+                 sherd_scores *out);
+
+/* Scales::for_pair (scales.rs:72-88). Pure host arithmetic. */
+int sherd_scales_for_pair(const sherd_params *p, double t, double res,
+                          sherd_scales *out);
+/* Params::default (params.rs:141-190), the thresholds this ABI reads. */
+void sherd_params_default(sherd_params *out);
+/* verify::accept (verify.rs:632-638). */
+uint32_t sherd_accept(const sherd_scores *s, const sherd_params *p,
+                      const sherd_scales *sc);
+
+/* ---- the batched stage-2 path ------------------------------------------ */
+
+/* A pair as Pair::stage2_batch reads it (pair.rs:298-372, 592-630): A's two
+ * ICP targets (pc_reg, pc_frac, with normals), B's two moving clouds, both
+ * fragments' Surfaces and the pair's Scales. */
+int sherd_pair_create(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfaces *b,
+                      const sherd_cloud *reg_target, const sherd_cloud *frac_target,
+                      const double *reg_source, uint32_t n_reg,
+                      const double *frac_source, uint32_t n_frac,
+                      const sherd_scales *sc, sherd_pair **out);
+int sherd_pair_free(sherd_pair *pair);
+
+/* R 5.6 + R 6 + R 6.5 for every (pair, start): the four point-to-plane rungs
+ * (0.2 t, 0.08 t on pc_reg; 0.08 t, 0.04 t on pc_frac; 30 iterations each,
+ * ladder.rs:51-61, 142-161), the full verification at the last pose and the
+ * verdict. SHERD_SCHED_BATCHED runs every item in persistent kernels fed by a
+ * device work queue, captured as one CUDA graph; SHERD_SCHED_PLAIN launches
+ * the same kernels once per pair and synchronises between pairs. */
+int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs,
+                              uint32_t n_pairs, const sherd_work_item *items,
+                              uint32_t n_items, const sherd_params *p, int sched,
+                              sherd_candidate *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SHERD_CUDA_H */

@@ -1,0 +1,356 @@
+"""ctypes view of the oracle (oracle.cpp), the CPU restatement of the reference's hot path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by bench.py's
+CPU-baseline leg. The product package never imports it.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import build as _build
+
+_HERE = Path(__file__).resolve().parent
+_lib = None
+
+F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+F64P = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+U32P = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+U8P = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+I32P = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+class IcpOptions(C.Structure):
+    _fields_ = [("estimation", C.c_int32), ("max_iteration", C.c_int32),
+                ("max_correspondence_distance", C.c_double)]
+
+
+class Registration(C.Structure):
+    _fields_ = [("transform", C.c_double * 16), ("fitness", C.c_double),
+                ("inlier_rmse", C.c_double), ("correspondences", C.c_uint64),
+                ("iterations", C.c_uint32), ("converged", C.c_uint32)]
+
+
+class Scales(C.Structure):
+    _fields_ = [(k, C.c_double) for k in (
+        "t", "res", "coarse", "stage1", "tight", "facing", "gap", "seam", "near", "pen", "nms",
+        "icp")]
+
+
+class Params(C.Structure):
+    _fields_ = [(k, C.c_double) for k in (
+        "min_tight", "max_gap", "max_pen", "min_seam", "min_cont_n",
+        "coarse_delta", "stage1_delta", "tight_delta", "facing_delta", "seam_delta",
+        "near_delta", "pen_delta", "nms_delta", "icp_delta",
+        "coarse_res", "stage1_res", "tight_res", "facing_res", "gap_res", "seam_res",
+        "near_res", "pen_res", "icp_res")]
+
+
+SCORE_FIELDS = ("tight_a", "tight_b", "tight", "gap_a", "gap_b", "gap", "contact_a",
+                "contact_b", "contact", "seam", "gap_limit", "tight_delta", "cont", "cont_n",
+                "pen", "pen_depth")
+
+
+class Scores(C.Structure):
+    _fields_ = [(k, C.c_double) for k in SCORE_FIELDS] + [
+        ("pen_unavailable", C.c_uint32), ("partial", C.c_uint32),
+        ("brk", C.c_double), ("brk_best", C.c_double)]
+
+
+class WorkItem(C.Structure):
+    _fields_ = [("pair", C.c_uint32), ("start", C.c_uint32), ("init", C.c_double * 16)]
+
+
+class Candidate(C.Structure):
+    _fields_ = [("pair", C.c_uint32), ("start", C.c_uint32), ("accepted", C.c_uint32),
+                ("status", C.c_uint32), ("rungs", Registration * 4), ("scores", Scores)]
+
+
+class InsideOutcome(C.Structure):
+    _fields_ = [("depth", C.c_float), ("inside", C.c_uint32)]
+
+
+def lib() -> C.CDLL:
+    """The loaded oracle, built first when its sources are newer than the library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.OUT
+    if (_HERE / "oracle.cpp").exists():
+        path = _build.build()
+    L = C.CDLL(str(path))
+    vp = C.c_void_p
+    sig = {
+        "or_mesh_new": (vp, [F32P, C.c_uint32, U32P, C.c_uint32]),
+        "or_mesh_subset": (vp, [vp, U8P]),
+        "or_mesh_free": (None, [vp]),
+        "or_mesh_aabb": (None, [vp, F32P, F32P]),
+        "or_first_hit": (None, [vp, F32P, F32P, C.c_uint32, F32P, U32P, C.c_int]),
+        "or_bounded_distance": (None, [vp, F64P, C.c_uint32, F64P, C.c_double, C.c_int, F64P]),
+        "or_inside": (None, [vp, F64P, C.c_uint32, F64P, vp, C.c_int]),
+        "or_crossings": (C.c_uint32, [vp, F32P, F32P]),
+        "or_cloud_new": (vp, [F64P, vp, C.c_uint32]),
+        "or_cloud_free": (None, [vp]),
+        "or_nearest_within_sq": (None, [vp, F64P, C.c_uint32, C.c_double, U32P, F64P, C.c_int]),
+        "or_nearest_below": (None, [vp, F64P, C.c_uint32, C.c_double, U32P, F64P, C.c_int]),
+        "or_icp_rung": (None, [F64P, C.c_uint32, vp, F64P, C.c_uint32, IcpOptions, vp, C.c_int]),
+        "or_surfaces_new": (vp, [vp, vp, C.c_uint32, C.c_double, F64P, C.c_uint32, F64P,
+                                 C.c_uint32, F64P, F64P, C.c_uint32, F64P, F64P, C.c_uint32]),
+        "or_surfaces_free": (None, [vp]),
+        "or_verify": (None, [vp, vp, F64P, C.POINTER(Scales), C.c_int, C.POINTER(Scores)]),
+        "or_accept": (C.c_uint32, [C.POINTER(Scores), C.POINTER(Params), C.POINTER(Scales)]),
+        "or_pair_new": (vp, [vp, vp, vp, vp, F64P, C.c_uint32, F64P, C.c_uint32,
+                             C.POINTER(Scales)]),
+        "or_pair_free": (None, [vp]),
+        "or_ladder_verify_batch": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Params),
+                                             C.c_int, vp]),
+        "or_face_geometry": (None, [F64P, U32P, C.c_uint32, vp, vp, vp]),
+        "or_face_indices": (C.c_uint32, [C.c_uint32, C.c_uint32, vp]),
+        "or_cast_inward_rays": (None, [vp, F64P, F64P, U32P, C.c_uint32, F32P, U32P, C.c_int]),
+        "or_thickness_from_hits": (C.c_int, [F64P, C.c_uint32, U32P, F32P, U32P, C.c_uint32,
+                                             C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "or_percentile90": (C.c_float, [F32P, C.c_uint32]),
+        "or_hist_mode": (C.c_float, [F32P, C.c_uint32]),
+        "or_cone_votes": (None, [vp, F64P, F64P, F64P, F64P, C.c_uint32, C.c_double, U8P,
+                                 C.c_int]),
+        "or_eigen_pivots": (None, [F64P, I32P]),
+        "or_solve_ldlt": (C.c_int, [F64P, F64P, F64P]),
+        "or_pose_inverse": (None, [F64P, F64P]),
+        "or_euler_zyx": (None, [C.c_double, C.c_double, C.c_double, F64P]),
+        "or_tri_distance": (C.c_float, [F32P, F32P, F32P, F32P]),
+        "or_moller_trumbore": (C.c_float, [F32P, F32P, F32P, F32P, F32P]),
+        "or_default_threads": (C.c_int, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+class Mesh:
+    """RayScene over f32 vertices (spatial/bvh.rs:36-192)."""
+
+    def __init__(self, v, f, _handle=None):
+        self.v = f32(v).reshape(-1, 3)
+        self.f = u32(f).reshape(-1, 3)
+        self.h = _handle or lib().or_mesh_new(self.v, len(self.v), self.f, len(self.f))
+        if not self.h:
+            raise ValueError("a mesh needs at least one face")
+
+    def subset(self, keep) -> "Mesh":
+        keep = np.ascontiguousarray(keep, dtype=np.uint8)
+        h = lib().or_mesh_subset(self.h, keep)
+        m = Mesh.__new__(Mesh)
+        m.v, m.f, m.h = self.v, self.f[keep.astype(bool)] if keep.any() else self.f[:1], h
+        return m
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_mesh_free(self.h)
+            self.h = None
+
+    def aabb(self):
+        lo = np.zeros(3, np.float32)
+        hi = np.zeros(3, np.float32)
+        lib().or_mesh_aabb(self.h, lo, hi)
+        return lo, hi
+
+    def first_hit(self, org, dirs, threads=0):
+        org, dirs = f32(org).reshape(-1, 3), f32(dirs).reshape(-1, 3)
+        n = len(org)
+        t = np.empty(n, np.float32)
+        prim = np.empty(n, np.uint32)
+        lib().or_first_hit(self.h, org, dirs, n, t, prim, threads or lib().or_default_threads())
+        return t, prim
+
+    def bounded_distance(self, pts, pose, max_dist, reduce=0):
+        pts = f64(pts).reshape(-1, 3)
+        out = np.empty(1 if reduce else len(pts), np.float64)
+        lib().or_bounded_distance(self.h, pts, len(pts), f64(pose).reshape(16), max_dist,
+                                  reduce, out)
+        return out
+
+    def inside(self, pts, pose, threads=0):
+        pts = f64(pts).reshape(-1, 3)
+        out = (InsideOutcome * max(len(pts), 1))()
+        lib().or_inside(self.h, pts, len(pts), f64(pose).reshape(16), C.cast(out, C.c_void_p),
+                        threads or lib().or_default_threads())
+        depth = np.array([o.depth for o in out[:len(pts)]], np.float32)
+        inside = np.array([o.inside for o in out[:len(pts)]], np.uint32)
+        return depth, inside
+
+
+class Cloud:
+    """PointTree over f64 points (spatial/kdtree.rs:31-258), with optional normals."""
+
+    def __init__(self, p, n=None):
+        self.p = f64(p).reshape(-1, 3)
+        self.n = None if n is None else f64(n).reshape(-1, 3)
+        nptr = None if self.n is None else self.n.ctypes.data_as(C.c_void_p)
+        self.h = lib().or_cloud_new(self.p, nptr, len(self.p))
+        if not self.h:
+            raise ValueError("a cloud needs at least one point")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_cloud_free(self.h)
+            self.h = None
+
+    def nearest_within_sq(self, q, r2, threads=0):
+        q = f64(q).reshape(-1, 3)
+        idx = np.empty(len(q), np.uint32)
+        d2 = np.empty(len(q), np.float64)
+        lib().or_nearest_within_sq(self.h, q, len(q), r2, idx, d2,
+                                   threads or lib().or_default_threads())
+        return idx, d2
+
+    def nearest_below(self, q, bound, threads=0):
+        q = f64(q).reshape(-1, 3)
+        idx = np.empty(len(q), np.uint32)
+        d = np.empty(len(q), np.float64)
+        lib().or_nearest_below(self.h, q, len(q), bound, idx, d,
+                               threads or lib().or_default_threads())
+        return idx, d
+
+
+def icp_rung(source, target: Cloud, inits, distance, max_iteration=30, threads=0):
+    source = f64(source).reshape(-1, 3)
+    inits = f64(inits).reshape(-1, 16)
+    out = (Registration * len(inits))()
+    opt = IcpOptions(1, max_iteration, distance)
+    lib().or_icp_rung(source, len(source), target.h, inits, len(inits), opt,
+                      C.cast(out, C.c_void_p), threads or lib().or_default_threads())
+    return list(out)
+
+
+class Surfaces:
+    """verify::Surfaces (verify.rs:223-299)."""
+
+    def __init__(self, fracture: Mesh, mesh: Mesh | None, watertight, frac_area, pf, s, brk_p,
+                 brk_ns, margin_p, margin_n):
+        self.keep = (fracture, mesh)
+        self.arrays = [f64(x).reshape(-1, 3) for x in (pf, s, brk_p, brk_ns, margin_p, margin_n)]
+        pf, s, bp, bn, mp, mn = self.arrays
+        self.h = lib().or_surfaces_new(fracture.h, mesh.h if mesh else None, int(watertight),
+                                       float(frac_area), pf, len(pf), s, len(s), bp, bn, len(bp),
+                                       mp, mn, len(mp))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_surfaces_free(self.h)
+            self.h = None
+
+
+def verify(a: Surfaces, b: Surfaces, pose, scales: Scales, full=True) -> Scores:
+    out = Scores()
+    lib().or_verify(a.h, b.h, f64(pose).reshape(16), C.byref(scales), int(full), C.byref(out))
+    return out
+
+
+def accept(scores: Scores, params: Params, scales: Scales) -> bool:
+    return bool(lib().or_accept(C.byref(scores), C.byref(params), C.byref(scales)))
+
+
+class Pair:
+    def __init__(self, a: Surfaces, b: Surfaces, reg_target: Cloud, frac_target: Cloud,
+                 reg_source, frac_source, scales: Scales):
+        self.keep = (a, b, reg_target, frac_target)
+        self.rs = f64(reg_source).reshape(-1, 3)
+        self.fs = f64(frac_source).reshape(-1, 3)
+        self.scales = scales
+        self.h = lib().or_pair_new(a.h, b.h, reg_target.h, frac_target.h, self.rs, len(self.rs),
+                                   self.fs, len(self.fs), C.byref(scales))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_pair_free(self.h)
+            self.h = None
+
+
+def ladder_verify_batch(pairs, items, params: Params, threads=0):
+    """The CPU baseline of the batched stage-2 path: returns (candidates, threads used)."""
+    arr = (C.c_void_p * len(pairs))(*[p.h for p in pairs])
+    it = (WorkItem * len(items))(*items)
+    out = (Candidate * len(items))()
+    used = lib().or_ladder_verify_batch(arr, len(pairs), C.cast(it, C.c_void_p), len(items),
+                                        C.byref(params), threads, C.cast(out, C.c_void_p))
+    return list(out), used
+
+
+def face_geometry(v, f):
+    v = f64(v).reshape(-1, 3)
+    f = u32(f).reshape(-1, 3)
+    n = np.empty((len(f), 3))
+    a = np.empty(len(f))
+    c = np.empty((len(f), 3))
+    lib().or_face_geometry(v, f, len(f), n.ctypes.data_as(C.c_void_p),
+                           a.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p))
+    return n, a, c
+
+
+def face_indices(n_faces, n=300_000):
+    k = lib().or_face_indices(n_faces, n, None)
+    out = np.empty(k, np.uint32)
+    lib().or_face_indices(n_faces, n, out.ctypes.data_as(C.c_void_p))
+    return out
+
+
+def cast_inward_rays(mesh: Mesh, centroids, normals, idx, threads=0):
+    idx = u32(idx)
+    t = np.empty(len(idx), np.float32)
+    prim = np.empty(len(idx), np.uint32)
+    lib().or_cast_inward_rays(mesh.h, f64(centroids), f64(normals), idx, len(idx), t, prim,
+                              threads or lib().or_default_threads())
+    return t, prim
+
+
+def thickness_from_hits(normals, idx, t_hit, prim):
+    normals = f64(normals).reshape(-1, 3)
+    t = C.c_float()
+    m = C.c_float()
+    ok = lib().or_thickness_from_hits(normals, len(normals), u32(idx), f32(t_hit), u32(prim),
+                                      len(idx), C.byref(t), C.byref(m))
+    return (np.float32(t.value), np.float32(m.value)) if ok else None
+
+
+def cone_votes(mesh: Mesh, centroids, normals, ns, hit_normals, thick, threads=0):
+    nf = len(normals)
+    good = np.empty(nf, np.uint8)
+    lib().or_cone_votes(mesh.h, f64(centroids), f64(normals), f64(ns), f64(hit_normals), nf,
+                        float(thick), good, threads or lib().or_default_threads())
+    return good
+
+
+def scales_array(s: Scales) -> np.ndarray:
+    return np.array([getattr(s, k) for k, _ in Scales._fields_])
+
+
+def scales_from(arr) -> Scales:
+    return Scales(*[float(x) for x in arr])
+
+
+def default_params() -> Params:
+    """Params::default (params.rs:141-190), the fields this ABI reads."""
+    return Params(min_tight=0.25, max_gap=0.03, max_pen=0.005, min_seam=3.0, min_cont_n=0.8,
+                  coarse_delta=0.15, stage1_delta=0.06, tight_delta=0.01, facing_delta=0.3,
+                  seam_delta=0.12, near_delta=0.5, pen_delta=0.06, nms_delta=0.5,
+                  icp_delta=0.04, coarse_res=2.3, stage1_res=0.9, tight_res=0.15,
+                  facing_res=1.0, gap_res=0.45, seam_res=1.8, near_res=4.0, pen_res=0.9,
+                  icp_res=0.6)

@@ -1,0 +1,1410 @@
+// oracle.cpp — CPU restatement of sherd-refit's geometry hot path.
+//
+// TEST INFRASTRUCTURE ONLY. This file is the checker the CUDA backend is
+// compared against; it is built into oracle/_build/liboracle.so and loaded by
+// the tests, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg,
+// never by the product library.
+//
+// Every function restates the reference (Rust crate `sherd-core`) and cites
+// the file:line it follows. The reference's third-party geometry (parry3d
+// 0.30.2 ray casts and point projection, kiddo 6.2.0 nearest neighbours) is
+// not vendored; its published algorithms are restated here with one tie rule
+// shared with the CUDA backend:
+//   * first hit: Moller-Trumbore in f32 (the inside test's own kernel,
+//     spatial/bvh.rs:199-220), smallest t, then lowest face index;
+//   * point-to-triangle distance: the Voronoi-region closest point of
+//     Ericson, "Real-Time Collision Detection", sec. 5.1.5, in f32;
+//   * nearest neighbour: smallest squared distance ((dx^2 + dy^2) + dz^2 in
+//     f64), then lowest point index (kiddo's observed rule, kdtree.rs:104-109).
+// Spatial pruning (BVH boxes, KD planes) is conservative, so every answer is
+// the brute-force answer under that rule.
+//
+// Built with -ffp-contract=off: the reference's arithmetic has no fused
+// multiply-adds (Rust does not contract), and neither may this.
+
+#include "../include/sherd_cuda.h"
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr float F_INF = std::numeric_limits<float>::infinity();
+constexpr double D_INF = std::numeric_limits<double>::infinity();
+constexpr uint32_t MISS = 0xFFFFFFFFu;
+
+struct V3f {
+  float x, y, z;
+};
+inline V3f sub(V3f a, V3f b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3f cross(V3f a, V3f b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline float dot(V3f a, V3f b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+
+// ---------------------------------------------------------------------------
+// Poses (row-major 4x4 doubles)
+// ---------------------------------------------------------------------------
+
+// types::apply_transform (types.rs:175-181): R p + tau, left to right.
+inline void apply(const double *t, const double *p, double *o) {
+  for (int i = 0; i < 3; ++i)
+    o[i] = t[4 * i] * p[0] + t[4 * i + 1] * p[1] + t[4 * i + 2] * p[2] + t[4 * i + 3];
+}
+// verify::rotate (verify.rs:711-717): R n, not renormalised.
+inline void rotate(const double *t, const double *n, double *o) {
+  for (int i = 0; i < 3; ++i) o[i] = t[4 * i] * n[0] + t[4 * i + 1] * n[1] + t[4 * i + 2] * n[2];
+}
+inline double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+void matmul4(const double *a, const double *b, double *o) {
+  double r[16];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      double s = a[4 * i] * b[j];
+      for (int k = 1; k < 4; ++k) s += a[4 * i + k] * b[4 * k + j];
+      r[4 * i + j] = s;
+    }
+  std::memcpy(o, r, sizeof r);
+}
+
+// verify::pose_inverse (verify.rs:739-798): dgetf2 partial pivoting then one
+// forward/back substitution per column of P*I.
+void pose_inverse(const double *t, double *out) {
+  double m[4][4];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) m[i][j] = t[4 * i + j];
+  int piv[4] = {0, 1, 2, 3};
+  for (int k = 0; k < 4; ++k) {
+    int best = k;
+    for (int i = k + 1; i < 4; ++i)
+      if (std::fabs(m[i][k]) > std::fabs(m[best][k])) best = i;
+    if (best != k) {
+      for (int c = 0; c < 4; ++c) std::swap(m[k][c], m[best][c]);
+      std::swap(piv[k], piv[best]);
+    }
+    double pivot = m[k][k];
+    if (pivot == 0.0) continue;
+    for (int r = k + 1; r < 4; ++r) {
+      m[r][k] /= pivot;
+      double factor = m[r][k];
+      for (int c = k + 1; c < 4; ++c) m[r][c] -= factor * m[k][c];
+    }
+  }
+  for (int col = 0; col < 4; ++col) {
+    double y[4], x[4];
+    for (int i = 0; i < 4; ++i) {
+      double acc = 0.0;
+      for (int j = 0; j < i; ++j) acc += m[i][j] * y[j];
+      y[i] = (piv[i] == col ? 1.0 : 0.0) - acc;
+    }
+    for (int i = 3; i >= 0; --i) {
+      double acc = 0.0;
+      for (int j = i + 1; j < 4; ++j) acc += m[i][j] * x[j];
+      x[i] = (y[i] - acc) / m[i][i];
+    }
+    for (int r = 0; r < 4; ++r) out[4 * r + col] = x[r];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Triangle BVH (RayScene, spatial/bvh.rs:36-192), f32 geometry
+// ---------------------------------------------------------------------------
+
+// Moller-Trumbore as spatial/bvh.rs:199-220 writes it. Returns the ray
+// parameter of a crossing, or a negative value when there is none.
+inline float moller_trumbore(V3f o, V3f d, V3f v0, V3f v1, V3f v2) {
+  const float EPS = 1e-9f;
+  V3f e1 = sub(v1, v0), e2 = sub(v2, v0);
+  V3f pvec = cross(d, e2);
+  float det = dot(e1, pvec);
+  if (std::fabs(det) < EPS) return -1.0f;
+  float inv = 1.0f / det;
+  V3f tvec = sub(o, v0);
+  float u = inv * dot(tvec, pvec);
+  if (!(u >= 0.0f && u <= 1.0f)) return -1.0f;
+  V3f qvec = cross(tvec, e1);
+  float v = inv * dot(d, qvec);
+  if (v < 0.0f || u + v > 1.0f) return -1.0f;
+  float t = inv * dot(e2, qvec);
+  return t > EPS ? t : -1.0f;
+}
+
+// Closest point on a triangle (Ericson 5.1.5, Voronoi regions), f32; returns
+// the Euclidean distance sqrt((dx^2 + dy^2) + dz^2).
+inline float tri_distance(V3f p, V3f a, V3f b, V3f c) {
+  V3f ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+  float d1 = dot(ab, ap), d2 = dot(ac, ap);
+  V3f q;
+  if (d1 <= 0.0f && d2 <= 0.0f) {
+    q = a;
+  } else {
+    V3f bp = sub(p, b);
+    float d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3) {
+      q = b;
+    } else {
+      float vc = d1 * d4 - d3 * d2;
+      if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+        float s = d1 / (d1 - d3);
+        q = {a.x + s * ab.x, a.y + s * ab.y, a.z + s * ab.z};
+      } else {
+        V3f cp = sub(p, c);
+        float d5 = dot(ab, cp), d6 = dot(ac, cp);
+        if (d6 >= 0.0f && d5 <= d6) {
+          q = c;
+        } else {
+          float vb = d5 * d2 - d1 * d6;
+          if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+            float s = d2 / (d2 - d6);
+            q = {a.x + s * ac.x, a.y + s * ac.y, a.z + s * ac.z};
+          } else {
+            float va = d3 * d6 - d5 * d4;
+            float e43 = d4 - d3, e56 = d5 - d6;
+            if (va <= 0.0f && e43 >= 0.0f && e56 >= 0.0f) {
+              float s = e43 / (e43 + e56);
+              V3f bc = sub(c, b);
+              q = {b.x + s * bc.x, b.y + s * bc.y, b.z + s * bc.z};
+            } else {
+              float den = (va + vb) + vc;
+              float v = vb / den, w = vc / den;
+              q = {(a.x + ab.x * v) + ac.x * w, (a.y + ab.y * v) + ac.y * w,
+                   (a.z + ab.z * v) + ac.z * w};
+            }
+          }
+        }
+      }
+    }
+  }
+  V3f dq = sub(q, p);
+  return std::sqrt(dot(dq, dq));
+}
+
+struct TriNode {
+  float lo[3], hi[3];
+  int32_t left, right;  // children, -1 for a leaf
+  uint32_t first, count;
+};
+
+struct Mesh {
+  std::vector<V3f> v;
+  std::vector<uint32_t> f;  // 3 per face, face ids are positions in this mesh
+  std::vector<TriNode> nodes;
+  std::vector<uint32_t> order;
+  float lo[3], hi[3];
+  double pad;  // conservative box padding for every pruning test
+
+  V3f vert(uint32_t face, int k) const { return v[f[3 * face + k]]; }
+  uint32_t n_faces() const { return uint32_t(f.size() / 3); }
+
+  void build() {
+    uint32_t nf = n_faces();
+    lo[0] = lo[1] = lo[2] = F_INF;
+    hi[0] = hi[1] = hi[2] = -F_INF;
+    double mag = 1.0;
+    for (uint32_t i = 0; i < nf; ++i)
+      for (int k = 0; k < 3; ++k) {
+        V3f p = vert(i, k);
+        float c[3] = {p.x, p.y, p.z};
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = std::min(lo[a], c[a]);
+          hi[a] = std::max(hi[a], c[a]);
+          mag = std::max(mag, std::fabs(double(c[a])));
+        }
+      }
+    pad = 1e-5 * mag;
+    order.resize(nf);
+    for (uint32_t i = 0; i < nf; ++i) order[i] = i;
+    nodes.clear();
+    nodes.reserve(2 * nf / 2 + 8);
+    if (nf) build_node(0, nf);
+  }
+
+  int build_node(uint32_t b, uint32_t e) {
+    int id = int(nodes.size());
+    nodes.push_back({});
+    TriNode nd;
+    for (int a = 0; a < 3; ++a) {
+      nd.lo[a] = F_INF;
+      nd.hi[a] = -F_INF;
+    }
+    float clo[3] = {F_INF, F_INF, F_INF}, chi[3] = {-F_INF, -F_INF, -F_INF};
+    for (uint32_t i = b; i < e; ++i) {
+      double cen[3] = {0, 0, 0};
+      for (int k = 0; k < 3; ++k) {
+        V3f p = vert(order[i], k);
+        float c[3] = {p.x, p.y, p.z};
+        for (int a = 0; a < 3; ++a) {
+          nd.lo[a] = std::min(nd.lo[a], c[a]);
+          nd.hi[a] = std::max(nd.hi[a], c[a]);
+          cen[a] += c[a];
+        }
+      }
+      for (int a = 0; a < 3; ++a) {
+        clo[a] = std::min(clo[a], float(cen[a] / 3));
+        chi[a] = std::max(chi[a], float(cen[a] / 3));
+      }
+    }
+    if (e - b <= 4) {
+      nd.left = nd.right = -1;
+      nd.first = b;
+      nd.count = e - b;
+      nodes[id] = nd;
+      return id;
+    }
+    int axis = 0;
+    for (int a = 1; a < 3; ++a)
+      if (chi[a] - clo[a] > chi[axis] - clo[axis]) axis = a;
+    uint32_t mid = (b + e) / 2;
+    auto key = [&](uint32_t face) {
+      float s = 0;
+      for (int k = 0; k < 3; ++k) {
+        V3f p = vert(face, k);
+        s += (axis == 0 ? p.x : axis == 1 ? p.y : p.z);
+      }
+      return s;
+    };
+    std::nth_element(order.begin() + b, order.begin() + mid, order.begin() + e,
+                     [&](uint32_t x, uint32_t y) {
+                       float kx = key(x), ky = key(y);
+                       return kx < ky || (kx == ky && x < y);
+                     });
+    nd.count = 0;
+    nd.first = 0;
+    nd.left = build_node(b, mid);
+    nd.right = build_node(mid, e);
+    nodes[id] = nd;
+    return id;
+  }
+
+  // Entry parameter of the ray into the padded box, or +inf when it misses.
+  double ray_box(const TriNode &n, const double *o, const double *invd) const {
+    double t0 = 0.0, t1 = D_INF;
+    for (int a = 0; a < 3; ++a) {
+      double l = double(n.lo[a]) - pad, h = double(n.hi[a]) + pad;
+      if (std::isinf(invd[a])) {
+        if (o[a] < l || o[a] > h) return D_INF;
+        continue;
+      }
+      double ta = (l - o[a]) * invd[a], tb = (h - o[a]) * invd[a];
+      if (ta > tb) std::swap(ta, tb);
+      t0 = std::max(t0, ta);
+      t1 = std::min(t1, tb);
+    }
+    return t0 <= t1 ? t0 : D_INF;
+  }
+
+  double box_dist(const TriNode &n, const float *p) const {
+    double s = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      double l = double(n.lo[a]) - pad, h = double(n.hi[a]) + pad, q = p[a];
+      double g = q < l ? l - q : (q > h ? q - h : 0.0);
+      s += g * g;
+    }
+    return std::sqrt(s);
+  }
+
+  // RayScene::first_hit (bvh.rs:84-90) under the tie rule of this file.
+  void first_hit(V3f o, V3f d, float *t_out, uint32_t *prim_out) const {
+    float best = F_INF;
+    uint32_t bi = MISS;
+    if (nodes.empty()) {
+      *t_out = best;
+      *prim_out = bi;
+      return;
+    }
+    double od[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z}, invd[3];
+    double dn = std::sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+    for (int a = 0; a < 3; ++a) invd[a] = 1.0 / dd[a];
+    double slack = dn > 0 ? 4.0 * pad / dn : D_INF;
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+      const TriNode &n = nodes[stack[--sp]];
+      double te = ray_box(n, od, invd);
+      if (te == D_INF || te > double(best) + slack) continue;
+      if (n.left < 0) {
+        for (uint32_t i = n.first; i < n.first + n.count; ++i) {
+          uint32_t face = order[i];
+          float t = moller_trumbore(o, d, vert(face, 0), vert(face, 1), vert(face, 2));
+          if (t < 0.0f) continue;
+          if (t < best || (t == best && face < bi)) {
+            best = t;
+            bi = face;
+          }
+        }
+      } else {
+        stack[sp++] = n.left;
+        stack[sp++] = n.right;
+      }
+    }
+    *t_out = best;
+    *prim_out = bi;
+  }
+
+  // RayScene::crossings (bvh.rs:160-175): every face the ray crosses.
+  uint32_t crossings(V3f o, V3f d) const {
+    if (nodes.empty()) return 0;
+    double od[3] = {o.x, o.y, o.z}, invd[3] = {1.0 / d.x, 1.0 / d.y, 1.0 / d.z};
+    uint32_t hits = 0;
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+      const TriNode &n = nodes[stack[--sp]];
+      if (ray_box(n, od, invd) == D_INF) continue;
+      if (n.left < 0) {
+        for (uint32_t i = n.first; i < n.first + n.count; ++i) {
+          uint32_t face = order[i];
+          if (moller_trumbore(o, d, vert(face, 0), vert(face, 1), vert(face, 2)) >= 0.0f) ++hits;
+        }
+      } else {
+        stack[sp++] = n.left;
+        stack[sp++] = n.right;
+      }
+    }
+    return hits;
+  }
+
+  // RayScene::inside (bvh.rs:146-157): majority of the +x, +y, +z parities.
+  bool inside(V3f p) const {
+    int votes = 0;
+    const V3f dirs[3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int a = 0; a < 3; ++a)
+      if (crossings(p, dirs[a]) % 2 == 1) ++votes;
+    return votes >= 2;
+  }
+
+  // Distance to the nearest face when it is <= window (inclusive), else +inf.
+  // RayScene::bounded_distance (bvh.rs:123-131) with window = +inf is
+  // RayScene::distance (bvh.rs:110-113).
+  float distance(V3f p, float window) const {
+    if (nodes.empty() || !(window > 0.0f)) return F_INF;
+    float best = F_INF;
+    float pf[3] = {p.x, p.y, p.z};
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+      const TriNode &n = nodes[stack[--sp]];
+      double bound = std::min(double(best), double(window));
+      if (box_dist(n, pf) > bound + pad) continue;
+      if (n.left < 0) {
+        for (uint32_t i = n.first; i < n.first + n.count; ++i) {
+          uint32_t face = order[i];
+          float dd = tri_distance(p, vert(face, 0), vert(face, 1), vert(face, 2));
+          if (dd <= window && dd < best) best = dd;
+        }
+      } else {
+        stack[sp++] = n.left;
+        stack[sp++] = n.right;
+      }
+    }
+    return best;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// KD tree over f64 points (PointTree, spatial/kdtree.rs:31-258)
+// ---------------------------------------------------------------------------
+
+struct KdNode {
+  int32_t axis;  // -1 for a leaf
+  double split;
+  int32_t left, right;
+  uint32_t first, count;
+};
+
+struct Cloud {
+  std::vector<double> p;  // 3 per point
+  std::vector<double> n;  // 3 per point, or empty
+  std::vector<uint32_t> order;
+  std::vector<KdNode> nodes;
+
+  uint32_t size() const { return uint32_t(p.size() / 3); }
+
+  void build() {
+    uint32_t np = size();
+    order.resize(np);
+    for (uint32_t i = 0; i < np; ++i) order[i] = i;
+    nodes.clear();
+    if (np) build_node(0, np);
+  }
+
+  int build_node(uint32_t b, uint32_t e) {
+    int id = int(nodes.size());
+    nodes.push_back({});
+    KdNode nd{};
+    if (e - b <= 8) {
+      nd.axis = -1;
+      nd.first = b;
+      nd.count = e - b;
+      nodes[id] = nd;
+      return id;
+    }
+    double lo[3] = {D_INF, D_INF, D_INF}, hi[3] = {-D_INF, -D_INF, -D_INF};
+    for (uint32_t i = b; i < e; ++i)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], p[3 * order[i] + a]);
+        hi[a] = std::max(hi[a], p[3 * order[i] + a]);
+      }
+    int axis = 0;
+    for (int a = 1; a < 3; ++a)
+      if (hi[a] - lo[a] > hi[axis] - lo[axis]) axis = a;
+    uint32_t mid = (b + e) / 2;
+    std::nth_element(order.begin() + b, order.begin() + mid, order.begin() + e,
+                     [&](uint32_t x, uint32_t y) {
+                       double kx = p[3 * x + axis], ky = p[3 * y + axis];
+                       return kx < ky || (kx == ky && x < y);
+                     });
+    nd.axis = axis;
+    nd.split = p[3 * order[mid] + axis];
+    nd.left = build_node(b, mid);
+    nd.right = build_node(mid, e);
+    nodes[id] = nd;
+    return id;
+  }
+
+  // PointTree::nearest_within_squared (kdtree.rs:202-217): the nearest point
+  // with d2 <= r2, lowest index on an exact tie.
+  bool nearest_within_sq(const double *q, double r2, uint32_t *bi, double *bd) const {
+    if (!(r2 >= 0.0) || nodes.empty()) return false;
+    bool found = false;
+    double best = r2;
+    uint32_t besti = MISS;
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+      const KdNode &nd = nodes[stack[--sp]];
+      if (nd.axis < 0) {
+        for (uint32_t k = nd.first; k < nd.first + nd.count; ++k) {
+          uint32_t i = order[k];
+          double dx = q[0] - p[3 * i], dy = q[1] - p[3 * i + 1], dz = q[2] - p[3 * i + 2];
+          double d2 = (dx * dx + dy * dy) + dz * dz;
+          if (d2 > r2) continue;
+          if (!found || d2 < best || (d2 == best && i < besti)) {
+            found = true;
+            best = d2;
+            besti = i;
+          }
+        }
+        continue;
+      }
+      double diff = q[nd.axis] - nd.split;
+      double lb = diff * diff;
+      int near_c = diff < 0 ? nd.left : nd.right, far_c = diff < 0 ? nd.right : nd.left;
+      // Both sides of the plane can hold points equal to the split value, so
+      // the far side is kept whenever its bound does not exceed the best.
+      if (lb <= best) stack[sp++] = far_c;
+      stack[sp++] = near_c;
+    }
+    if (found) {
+      *bi = besti;
+      *bd = best;
+    }
+    return found;
+  }
+
+  // PointTree::nearest_below (kdtree.rs:182-190).
+  bool nearest_below(const double *q, double bound, uint32_t *bi, double *dist) const {
+    if (!(bound > 0.0)) return false;
+    double widened = (bound * bound) * (1.0 + 4.0 * std::numeric_limits<double>::epsilon());
+    uint32_t i;
+    double d2;
+    if (!nearest_within_sq(q, widened, &i, &d2)) return false;
+    double d = std::sqrt(d2);
+    if (!(d < bound)) return false;
+    *bi = i;
+    *dist = d;
+    return true;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// ICP (matching/icp.rs:308-890), reference numerics (f64 point loops, World)
+// ---------------------------------------------------------------------------
+
+// icp::eigen_pivots (icp.rs:661-674).
+void eigen_pivots(const double a[6][6], int perm[6]) {
+  for (int k = 0; k < 6; ++k) perm[k] = k;
+  for (int k = 0; k < 6; ++k) {
+    int best = k;
+    for (int i = k + 1; i < 6; ++i)
+      if (std::fabs(a[perm[i]][perm[i]]) > std::fabs(a[perm[best]][perm[best]])) best = i;
+    std::swap(perm[k], perm[best]);
+  }
+}
+
+// icp::solve_ldlt (icp.rs:692-753).
+bool solve_ldlt(const double a[6][6], const double b[6], double x[6]) {
+  int perm[6];
+  eigen_pivots(a, perm);
+  double m[6][6];
+  for (int k = 0; k < 6; ++k)
+    for (int l = 0; l < 6; ++l) m[k][l] = a[perm[k]][perm[l]];
+  for (int k = 0; k < 6; ++k) {
+    if (k > 0) {
+      double temp[6] = {0, 0, 0, 0, 0, 0};
+      for (int j = 0; j < k; ++j) temp[j] = m[j][j] * m[k][j];
+      double diagonal = m[k][k];
+      for (int j = 0; j < k; ++j) diagonal -= m[k][j] * temp[j];
+      m[k][k] = diagonal;
+      for (int r = k + 1; r < 6; ++r) {
+        double below = m[r][k];
+        for (int j = 0; j < k; ++j) below -= m[r][j] * temp[j];
+        m[r][k] = below;
+      }
+    }
+    double pivot = m[k][k];
+    if (pivot != 0.0)
+      for (int r = k + 1; r < 6; ++r) m[r][k] /= pivot;
+  }
+  double y[6];
+  for (int k = 0; k < 6; ++k) y[k] = b[perm[k]];
+  for (int i = 0; i < 6; ++i) {
+    double value = y[i];
+    for (int j = 0; j < i; ++j) value -= m[i][j] * y[j];
+    y[i] = value;
+  }
+  for (int i = 0; i < 6; ++i) {
+    double pivot = m[i][i];
+    y[i] = std::fabs(pivot) > std::numeric_limits<double>::min() ? y[i] / pivot : 0.0;
+  }
+  for (int i = 5; i >= 0; --i) {
+    double value = y[i];
+    for (int j = i + 1; j < 6; ++j) value -= m[j][i] * y[j];
+    y[i] = value;
+  }
+  for (int k = 0; k < 6; ++k) x[perm[k]] = y[k];
+  for (int k = 0; k < 6; ++k)
+    if (!std::isfinite(x[k])) return false;
+  return true;
+}
+
+void mat3mul(const double a[3][3], const double b[3][3], double o[3][3]) {
+  double r[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r[i][j] = (a[i][0] * b[0][j] + a[i][1] * b[1][j]) + a[i][2] * b[2][j];
+  std::memcpy(o, r, sizeof r);
+}
+
+// icp::euler_zyx (icp.rs:770-778): Rz(g) Ry(b) Rx(a).
+void euler_zyx(double al, double be, double ga, double r[3][3]) {
+  double sa = std::sin(al), ca = std::cos(al), sb = std::sin(be), cb = std::cos(be);
+  double sg = std::sin(ga), cg = std::cos(ga);
+  double rx[3][3] = {{1, 0, 0}, {0, ca, -sa}, {0, sa, ca}};
+  double ry[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}};
+  double rz[3][3] = {{cg, -sg, 0}, {sg, cg, 0}, {0, 0, 1}};
+  double t[3][3];
+  mat3mul(rz, ry, t);
+  mat3mul(t, rx, r);
+}
+
+struct Corr {
+  uint32_t i, j;
+};
+
+// icp::correspondences (icp.rs:361-392).
+void correspondences(const std::vector<double> &moved, const Cloud &tgt, double distance,
+                     std::vector<Corr> &out, double *fit, double *rmse) {
+  out.clear();
+  *fit = 0.0;
+  *rmse = 0.0;
+  if (tgt.nodes.empty()) return;
+  if (!(distance > 0.0)) return;
+  double r2 = distance * distance;
+  double err = 0.0;
+  size_t n = moved.size() / 3;
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t j;
+    double d2;
+    if (!tgt.nearest_within_sq(&moved[3 * i], r2, &j, &d2)) continue;
+    if (d2 >= r2) continue;
+    err += d2;
+    out.push_back({uint32_t(i), j});
+  }
+  if (out.empty()) return;
+  double nc = double(out.size()), ns = double(n);
+  *fit = nc / ns;
+  *rmse = std::sqrt(err / nc);
+}
+
+// icp::point_to_plane (icp.rs:408-440) with normal_equations (icp.rs:599-640)
+// under Assembly::World and Precision::F64.
+void point_to_plane(const std::vector<double> &moved, const Cloud &tgt,
+                    const std::vector<Corr> &corr, double u[16]) {
+  for (int i = 0; i < 16; ++i) u[i] = (i % 5 == 0) ? 1.0 : 0.0;
+  if (corr.empty() || tgt.n.size() != tgt.p.size()) return;
+  double jtj[6][6] = {}, jtr[6] = {};
+  for (const Corr &c : corr) {
+    const double *p = &moved[3 * c.i], *q = &tgt.p[3 * c.j], *n = &tgt.n[3 * c.j];
+    double pc[3] = {p[0] - 0.0, p[1] - 0.0, p[2] - 0.0};
+    double row[6] = {pc[1] * n[2] - pc[2] * n[1], pc[2] * n[0] - pc[0] * n[2],
+                     pc[0] * n[1] - pc[1] * n[0], n[0], n[1], n[2]};
+    double r = (p[0] - q[0]) * n[0] + (p[1] - q[1]) * n[1] + (p[2] - q[2]) * n[2];
+    for (int k = 0; k < 6; ++k) {
+      for (int l = 0; l <= k; ++l) jtj[k][l] = jtj[k][l] + row[k] * row[l];
+      jtr[k] = jtr[k] + row[k] * r;
+    }
+  }
+  double a[6][6];
+  for (int k = 0; k < 6; ++k)
+    for (int l = 0; l <= k; ++l) {
+      a[k][l] = jtj[k][l];
+      a[l][k] = jtj[k][l];
+    }
+  double rhs[6], x[6];
+  for (int k = 0; k < 6; ++k) rhs[k] = -jtr[k];
+  if (!solve_ldlt(a, rhs, x)) return;
+  double r[3][3];
+  euler_zyx(x[0], x[1], x[2], r);
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) u[4 * i + j] = r[i][j];
+    u[4 * i + 3] = x[3 + i];
+  }
+}
+
+void transform_points(std::vector<double> &pts, const double *m) {
+  size_t n = pts.size() / 3;
+  for (size_t i = 0; i < n; ++i) {
+    double p[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]}, o[3];
+    apply(m, p, o);
+    pts[3 * i] = o[0];
+    pts[3 * i + 1] = o[1];
+    pts[3 * i + 2] = o[2];
+  }
+}
+
+// icp::register (icp.rs:308-356), point-to-plane.
+sherd_registration icp_register(const double *src, uint32_t ns, const Cloud &tgt,
+                                const double *init, const sherd_icp_options &opt) {
+  sherd_registration out{};
+  std::memcpy(out.transform, init, sizeof out.transform);
+  if (ns == 0 || tgt.size() == 0) return out;
+  double t[16];
+  std::memcpy(t, init, sizeof t);
+  std::vector<double> moved(src, src + 3 * size_t(ns));
+  transform_points(moved, init);
+  std::vector<Corr> corr;
+  double fit, rmse;
+  correspondences(moved, tgt, opt.max_correspondence_distance, corr, &fit, &rmse);
+  uint32_t iterations = 0;
+  bool converged = false;
+  for (int it = 0; it < opt.max_iteration; ++it) {
+    double u[16];
+    point_to_plane(moved, tgt, corr, u);
+    matmul4(u, t, t);
+    transform_points(moved, u);
+    ++iterations;
+    double nfit, nrmse;
+    correspondences(moved, tgt, opt.max_correspondence_distance, corr, &nfit, &nrmse);
+    converged = std::fabs(nfit - fit) < 1e-6 && std::fabs(nrmse - rmse) < 1e-6;
+    fit = nfit;
+    rmse = nrmse;
+    if (converged) break;
+  }
+  std::memcpy(out.transform, t, sizeof t);
+  out.fitness = fit;
+  out.inlier_rmse = rmse;
+  out.correspondences = corr.size();
+  out.iterations = iterations;
+  out.converged = converged ? 1u : 0u;
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// Verification (matching/verify.rs:318-638)
+// ---------------------------------------------------------------------------
+
+struct Surfaces {
+  const Mesh *fracture = nullptr;
+  const Mesh *mesh = nullptr;
+  bool watertight = false;
+  double frac_area = 0.0;
+  std::vector<double> pf, s, brk_p, brk_ns, margin_p, margin_n;
+  Cloud margin_tree;
+};
+
+// verify::median (verify.rs:693-700): numpy's median, sorted in place.
+double median(std::vector<double> &v) {
+  std::sort(v.begin(), v.end());
+  size_t n = v.size();
+  if (n == 0) return std::nan("");
+  if (n % 2 == 1) return v[n / 2];
+  return (v[n / 2 - 1] + v[n / 2]) / 2.0;
+}
+
+V3f narrow(const double *p) { return {float(p[0]), float(p[1]), float(p[2])}; }
+
+// CpuExecutor::bounded_distance (executor/cpu.rs:84-113).
+void bounded_distance(const Mesh &m, const double *pts, uint32_t n, const double *pose,
+                      double max_dist, int reduce, double *out) {
+  float window = float(max_dist);
+  if (reduce == SHERD_REDUCE_ALL) {
+    for (uint32_t i = 0; i < n; ++i) {
+      double q[3];
+      apply(pose, pts + 3 * i, q);
+      float d = m.distance(narrow(q), window);
+      out[i] = d == F_INF ? D_INF : double(d);
+    }
+  } else {
+    float best = window;
+    for (uint32_t i = 0; i < n; ++i) {
+      double q[3];
+      apply(pose, pts + 3 * i, q);
+      float d = m.distance(narrow(q), best);
+      if (d != F_INF) best = std::min(best, d);
+    }
+    out[0] = double(best);
+  }
+}
+
+// CpuExecutor::inside (executor/cpu.rs:115-128) and depth_inside (cpu.rs:182-188).
+void inside_batch(const Mesh &m, const double *pts, uint32_t n, const double *pose,
+                  sherd_inside_outcome *out) {
+  for (uint32_t i = 0; i < n; ++i) {
+    double q[3];
+    apply(pose, pts + 3 * i, q);
+    V3f p = narrow(q);
+    float c[3] = {p.x, p.y, p.z};
+    bool outside_box = false;
+    for (int k = 0; k < 3; ++k)
+      if (c[k] < m.lo[k] || c[k] > m.hi[k]) outside_box = true;
+    if (outside_box || !m.inside(p)) {
+      out[i] = {0.0f, 0u};
+      continue;
+    }
+    out[i] = {float(double(m.distance(p, F_INF))), 1u};
+  }
+}
+
+// verify::one_side (verify.rs:338-349).
+void one_side(const std::vector<double> &d, double area, const sherd_scales &sc, double *tight,
+              double *gap, double *contact) {
+  std::vector<double> facing;
+  for (double x : d)
+    if (x < sc.facing) facing.push_back(x);
+  if (facing.size() < 20) {
+    *tight = 0.0;
+    *gap = 1.0;
+    *contact = 0.0;
+    return;
+  }
+  size_t nt = 0;
+  for (double x : facing)
+    if (x < sc.tight) ++nt;
+  *tight = double(nt) / double(facing.size());
+  *gap = median(facing) / sc.t;
+  size_t touching = 0;
+  for (double x : d)
+    if (x < 2.0 * sc.tight) ++touching;
+  double share = double(touching) / double(d.size());
+  *contact = share * area / (sc.t * sc.t);
+}
+
+// verify::seam_points + seam_cells + seam_score (verify.rs:378-442, 809-811).
+double seam_score(const Surfaces &a, const Surfaces &b, const double *t, const sherd_scales &sc) {
+  size_t nb = b.brk_p.size() / 3, na = a.brk_p.size() / 3;
+  Cloud moved;
+  moved.p.resize(3 * nb);
+  std::vector<double> normals(3 * nb);
+  for (size_t j = 0; j < nb; ++j) {
+    apply(t, &b.brk_p[3 * j], &moved.p[3 * j]);
+    rotate(t, &b.brk_ns[3 * j], &normals[3 * j]);
+  }
+  if (nb == 0) return 0.0;
+  moved.build();
+  double voxel = sc.t / 3.0;
+  std::vector<std::array<int64_t, 3>> cells;
+  for (size_t i = 0; i < na; ++i) {
+    uint32_t j;
+    double dist;
+    if (!moved.nearest_below(&a.brk_p[3 * i], sc.seam, &j, &dist)) continue;
+    if (dot3(&a.brk_ns[3 * i], &normals[3 * j]) > 0.7) {
+      const double *p = &a.brk_p[3 * i];
+      cells.push_back({int64_t(std::floor(p[0] / voxel)), int64_t(std::floor(p[1] / voxel)),
+                       int64_t(std::floor(p[2] / voxel))});
+    }
+  }
+  if (cells.empty()) return 0.0;
+  std::sort(cells.begin(), cells.end());
+  cells.erase(std::unique(cells.begin(), cells.end()), cells.end());
+  return double(cells.size()) / 3.0;
+}
+
+// verify::continuity_scores (verify.rs:450-474).
+void continuity_scores(const Surfaces &a, const Surfaces &b, const double *t,
+                       const sherd_scales &sc, double *cont, double *cont_n) {
+  *cont = 1.0;
+  *cont_n = -1.0;
+  if (a.margin_tree.nodes.empty() || b.margin_p.empty()) return;
+  std::vector<double> steps, agreements;
+  size_t nb = b.margin_p.size() / 3;
+  for (size_t k = 0; k < nb; ++k) {
+    double moved[3];
+    apply(t, &b.margin_p[3 * k], moved);
+    uint32_t j;
+    double dist;
+    if (!a.margin_tree.nearest_below(moved, sc.near, &j, &dist)) continue;
+    const double *np = &a.margin_p[3 * j], *nn = &a.margin_n[3 * j];
+    double delta[3] = {moved[0] - np[0], moved[1] - np[1], moved[2] - np[2]};
+    steps.push_back(std::fabs(dot3(delta, nn)));
+    double rn[3];
+    rotate(t, &b.margin_n[3 * k], rn);
+    agreements.push_back(dot3(rn, nn));
+  }
+  if (steps.size() <= 20) return;
+  *cont = median(steps) / sc.t;
+  *cont_n = median(agreements);
+}
+
+// verify::one_penetration (verify.rs:541-580).
+void one_penetration(const std::vector<double> &pts, const double *t, const Mesh &scene,
+                     double pen, double *fraction, double *mins) {
+  *fraction = 0.0;
+  *mins = 0.0;
+  uint32_t n = uint32_t(pts.size() / 3);
+  if (n == 0) return;
+  std::vector<sherd_inside_outcome> outc(n);
+  inside_batch(scene, pts.data(), n, t, outc.data());
+  double deepest = -D_INF;
+  size_t deeper = 0;
+  for (auto &o : outc) {
+    if (!o.inside) continue;
+    double dd = double(o.depth);
+    deepest = std::max(deepest, dd);
+    if (dd > pen) ++deeper;
+  }
+  *fraction = double(deeper) / double(n);
+  if (deepest > -D_INF) {
+    *mins = -deepest;
+    return;
+  }
+  double best;
+  bounded_distance(scene, pts.data(), n, t, double(std::numeric_limits<float>::max()),
+                   SHERD_REDUCE_MIN, &best);
+  *mins = best;
+}
+
+// verify::verify (verify.rs:590-626).
+sherd_scores verify(const Surfaces &a, const Surfaces &b, const double *t, const sherd_scales &sc,
+                    bool full) {
+  sherd_scores s{};
+  double inv[16];
+  pose_inverse(t, inv);
+  std::vector<double> d1(b.pf.size() / 3), d2(a.pf.size() / 3);
+  bounded_distance(*a.fracture, b.pf.data(), uint32_t(d1.size()), t, sc.facing,
+                   SHERD_REDUCE_ALL, d1.data());
+  bounded_distance(*b.fracture, a.pf.data(), uint32_t(d2.size()), inv, sc.facing,
+                   SHERD_REDUCE_ALL, d2.data());
+  one_side(d2, a.frac_area, sc, &s.tight_a, &s.gap_a, &s.contact_a);
+  one_side(d1, b.frac_area, sc, &s.tight_b, &s.gap_b, &s.contact_b);
+  s.tight = std::min(s.tight_a, s.tight_b);
+  s.gap = std::max(s.gap_a, s.gap_b);
+  s.contact = std::min(s.contact_a, s.contact_b);
+  s.seam = seam_score(a, b, t, sc);
+  s.gap_limit = sc.gap / sc.t;
+  s.tight_delta = sc.tight / sc.t;
+  s.cont = 1.0;
+  s.cont_n = -1.0;
+  s.pen = 0.0;
+  s.pen_depth = 0.0;
+  if (!full) {
+    s.partial = 1;
+    return s;
+  }
+  continuity_scores(a, b, t, sc, &s.cont, &s.cont_n);
+  if (!a.mesh || !b.mesh || !(a.watertight && b.watertight)) {
+    s.pen_unavailable = 1;
+    return s;
+  }
+  double pen_b, min_b, pen_a, min_a;
+  one_penetration(b.s, t, *a.mesh, sc.pen, &pen_b, &min_b);
+  one_penetration(a.s, inv, *b.mesh, sc.pen, &pen_a, &min_a);
+  s.pen = std::max(pen_a, pen_b);
+  s.pen_depth = std::max(-min_a, -min_b) / sc.t;
+  return s;
+}
+
+uint32_t accept(const sherd_scores &s, const sherd_params &p, const sherd_scales &sc) {
+  return (s.tight >= p.min_tight && s.gap * sc.t <= sc.gap && s.pen <= p.max_pen &&
+          s.seam >= p.min_seam && s.cont_n >= p.min_cont_n)
+             ? 1u
+             : 0u;
+}
+
+// ---------------------------------------------------------------------------
+// The stage-2 ladder of one candidate (ladder.rs:105-161, pair.rs:298-372)
+// ---------------------------------------------------------------------------
+
+struct Pair {
+  const Surfaces *a, *b;
+  const Cloud *reg_target, *frac_target;
+  std::vector<double> reg_source, frac_source;
+  sherd_scales sc;
+};
+
+sherd_candidate ladder_verify(const Pair &pr, const sherd_work_item &item,
+                              const sherd_params &p, uint32_t pair_index) {
+  sherd_candidate c{};
+  c.pair = pair_index;
+  c.start = item.start;
+  static const double K[4] = {0.2, 0.08, 0.08, 0.04};
+  double pose[16];
+  std::memcpy(pose, item.init, sizeof pose);
+  for (int r = 0; r < 4; ++r) {
+    sherd_icp_options o{SHERD_POINT_TO_PLANE, 30, K[r] * pr.sc.t * pr.sc.icp};
+    const std::vector<double> &src = r < 2 ? pr.reg_source : pr.frac_source;
+    const Cloud &tgt = r < 2 ? *pr.reg_target : *pr.frac_target;
+    c.rungs[r] = icp_register(src.data(), uint32_t(src.size() / 3), tgt, pose, o);
+    std::memcpy(pose, c.rungs[r].transform, sizeof pose);
+  }
+  c.scores = verify(*pr.a, *pr.b, pose, pr.sc, true);
+  c.accepted = accept(c.scores, p, pr.sc);
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// Thickness (fragment/thickness.rs:99-390)
+// ---------------------------------------------------------------------------
+
+// thickness::percentile90 (thickness.rs:272-290).
+float percentile90(std::vector<float> v) {
+  std::sort(v.begin(), v.end());
+  size_t n = v.size();
+  if (n == 1) return v[0];
+  double vi = double(n - 1) * (90.0 / 100.0);
+  double prev = std::floor(vi);
+  size_t i = size_t(prev);
+  double gamma = vi - prev;
+  float a = v[i], b = v[std::min(i + 1, n - 1)];
+  float diff = b - a;
+  if (gamma >= 0.5) return b - diff * float(1.0 - gamma);
+  return a + diff * float(gamma);
+}
+
+// thickness::hist_mode and bin_edges (thickness.rs:212-262).
+float hist_mode(const std::vector<float> &x) {
+  const int BINS = 60;
+  float p90 = percentile90(x);
+  float first = 0.0f, last = p90;
+  if (p90 == 0.0f) {
+    first = -0.5f;
+    last = 0.5f;
+  }
+  float step = (last - first) / float(BINS);
+  float edges[BINS + 1];
+  for (int k = 0; k <= BINS; ++k) edges[k] = float(k) * step + first;
+  edges[BINS] = last;
+  float denom = last - first;
+  uint64_t counts[BINS] = {};
+  for (float v : x) {
+    if (!(v >= first && v <= last)) continue;
+    size_t i = size_t(((v - first) / denom) * float(BINS));
+    if (i == size_t(BINS)) i -= 1;
+    if (v < edges[i]) i -= 1;
+    if (i != size_t(BINS - 1) && v >= edges[i + 1]) i += 1;
+    counts[i] += 1;
+  }
+  int k = 0;
+  for (int i = 1; i < BINS; ++i)
+    if (counts[i] > counts[k]) k = i;
+  return 0.5f * (edges[k] + edges[k + 1]);
+}
+
+// thickness::thickness_from_hits (thickness.rs:139-162) with looking_back
+// (thickness.rs:185-204).
+bool thickness_from_hits(const double *normals, uint32_t nf, const uint32_t *idx,
+                         const float *t_hit, const uint32_t *prim, uint32_t n, float *t,
+                         float *mode) {
+  std::vector<float> ok_d, far;
+  for (uint32_t k = 0; k < n; ++k) {
+    float d = t_hit[k];
+    uint32_t p = prim[k];
+    if (!(std::isfinite(d) && p < nf)) continue;
+    ok_d.push_back(d);
+    const double *hit = normals + 3 * size_t(p), *from = normals + 3 * size_t(idx[k]);
+    double dd = -((hit[0] * from[0] + hit[1] * from[1]) + hit[2] * from[2]);
+    if (dd > 0.7) far.push_back(d);
+  }
+  if (ok_d.size() < 100) return false;
+  float raw = hist_mode(ok_d);
+  *mode = raw;
+  *t = far.size() >= 100 ? hist_mode(far) : raw;
+  return true;
+}
+
+// mesh::geometry::face_geometry (mesh/geometry.rs:70-96).
+void face_geometry(const double *v, const uint32_t *f, uint32_t nf, double *normals,
+                   double *areas, double *centroids) {
+  for (uint32_t i = 0; i < nf; ++i) {
+    const double *a = v + 3 * size_t(f[3 * i]), *b = v + 3 * size_t(f[3 * i + 1]),
+                 *c = v + 3 * size_t(f[3 * i + 2]);
+    double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    double e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+    double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                   e1[0] * e2[1] - e1[1] * e2[0]};
+    double len = std::sqrt((n[0] * n[0] + n[1] * n[1]) + n[2] * n[2]);
+    double den = std::max(len, 1e-12);
+    if (normals)
+      for (int k = 0; k < 3; ++k) normals[3 * i + k] = n[k] / den;
+    if (areas) areas[i] = 0.5 * len;
+    if (centroids)
+      for (int k = 0; k < 3; ++k) centroids[3 * i + k] = (a[k] + b[k] + c[k]) / 3.0;
+  }
+}
+
+// segment::cone_basis (segment.rs:383-395).
+bool cone_basis(const double *n, double e1[3], double e2[3]) {
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(n[k])) return false;
+  double a[3] = {1, 0, 0};
+  if (!(std::fabs(n[0]) < 0.9)) {
+    a[0] = 0;
+    a[1] = 1;
+  }
+  double c[3] = {n[1] * a[2] - n[2] * a[1], n[2] * a[0] - n[0] * a[2], n[0] * a[1] - n[1] * a[0]};
+  double len = std::sqrt((c[0] * c[0] + c[1] * c[1]) + c[2] * c[2]);
+  if (len <= 0.0) return false;
+  for (int k = 0; k < 3; ++k) e1[k] = c[k] / len;
+  e2[0] = n[1] * e1[2] - n[2] * e1[1];
+  e2[1] = n[2] * e1[0] - n[0] * e1[2];
+  e2[2] = n[0] * e1[1] - n[1] * e1[0];
+  return true;
+}
+
+// segment::classify_faces (segment.rs:318-376).
+uint8_t cone_vote(const Mesh &m, const double *c, const double *fnv, const double *n,
+                  const double *hit_normals, uint32_t nf, double thick) {
+  double e1[3], e2[3];
+  if (!cone_basis(n, e1, e2)) return 0;
+  const double PI = 3.14159265358979323846;
+  double angle = 15.0 * (PI / 180.0);
+  double cos_a = std::cos(angle), sin_a = std::sin(angle);
+  float min_hit = float(0.1 * thick);
+  float thick_f = float(thick);
+  V3f origin = {float(c[0] - fnv[0] * 1e-3), float(c[1] - fnv[1] * 1e-3),
+                float(c[2] - fnv[2] * 1e-3)};
+  uint8_t good = 0;
+  for (int k = 0; k < 7; ++k) {
+    double d[3];
+    if (k == 0) {
+      d[0] = -n[0];
+      d[1] = -n[1];
+      d[2] = -n[2];
+    } else {
+      double phi = 2.0 * PI * double(k - 1) / 6.0;
+      double cp = std::cos(phi), sp = std::sin(phi);
+      for (int q = 0; q < 3; ++q) d[q] = -(cos_a * n[q]) + sin_a * (cp * e1[q] + sp * e2[q]);
+    }
+    V3f dir = {float(d[0]), float(d[1]), float(d[2])};
+    float dh;
+    uint32_t prim;
+    m.first_hit(origin, dir, &dh, &prim);
+    if (prim == MISS) continue;
+    if (!std::isfinite(dh) || prim >= nf || dh <= min_hit) continue;
+    float ratio = dh / thick_f;
+    if (ratio <= 0.5f || ratio >= 1.8f) continue;
+    const double *h = hit_normals + 3 * size_t(prim);
+    double al = (h[0] * d[0] + h[1] * d[1]) + h[2] * d[2];
+    if (al > 0.7) ++good;
+  }
+  return good;
+}
+
+template <class F>
+void parallel_for(uint32_t n, int threads, F &&fn) {
+  if (threads <= 1 || n < 2) {
+    for (uint32_t i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::atomic<uint32_t> next{0};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([&] {
+      for (;;) {
+        uint32_t i = next.fetch_add(1);
+        if (i >= n) break;
+        fn(i);
+      }
+    });
+  for (auto &th : pool) th.join();
+}
+
+int default_threads() {
+  unsigned h = std::thread::hardware_concurrency();
+  return h ? int(h) : 1;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI (loaded by the tests through ctypes)
+// ===========================================================================
+extern "C" {
+
+void *or_mesh_new(const float *v, uint32_t nv, const uint32_t *f, uint32_t nf) {
+  if (nf == 0) return nullptr;
+  Mesh *m = new Mesh;
+  m->v.resize(nv);
+  for (uint32_t i = 0; i < nv; ++i) m->v[i] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+  m->f.assign(f, f + 3 * size_t(nf));
+  m->build();
+  return m;
+}
+
+// RayScene::of_subset (bvh.rs:71-78): the kept faces, or face 0.
+void *or_mesh_subset(const void *mesh, const uint8_t *keep) {
+  const Mesh *m = static_cast<const Mesh *>(mesh);
+  Mesh *s = new Mesh;
+  s->v = m->v;
+  uint32_t nf = m->n_faces();
+  for (uint32_t i = 0; i < nf; ++i)
+    if (keep[i])
+      for (int k = 0; k < 3; ++k) s->f.push_back(m->f[3 * i + k]);
+  if (s->f.empty())
+    for (int k = 0; k < 3; ++k) s->f.push_back(m->f[k]);
+  s->build();
+  return s;
+}
+
+void or_mesh_free(void *m) { delete static_cast<Mesh *>(m); }
+
+void or_mesh_aabb(const void *mesh, float *lo, float *hi) {
+  const Mesh *m = static_cast<const Mesh *>(mesh);
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = m->lo[k];
+    hi[k] = m->hi[k];
+  }
+}
+
+void or_first_hit(const void *mesh, const float *org, const float *dir, uint32_t n, float *t,
+                  uint32_t *prim, int threads) {
+  const Mesh *m = static_cast<const Mesh *>(mesh);
+  parallel_for(n, threads, [&](uint32_t i) {
+    m->first_hit({org[3 * i], org[3 * i + 1], org[3 * i + 2]},
+                 {dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]}, &t[i], &prim[i]);
+  });
+}
+
+void or_bounded_distance(const void *mesh, const double *pts, uint32_t n, const double *pose,
+                         double max_dist, int reduce, double *out) {
+  bounded_distance(*static_cast<const Mesh *>(mesh), pts, n, pose, max_dist, reduce, out);
+}
+
+void or_inside(const void *mesh, const double *pts, uint32_t n, const double *pose,
+               sherd_inside_outcome *out, int threads) {
+  const Mesh *m = static_cast<const Mesh *>(mesh);
+  parallel_for(n, threads, [&](uint32_t i) { inside_batch(*m, pts + 3 * size_t(i), 1, pose, out + i); });
+}
+
+uint32_t or_crossings(const void *mesh, const float *org, const float *dir) {
+  return static_cast<const Mesh *>(mesh)->crossings({org[0], org[1], org[2]},
+                                                     {dir[0], dir[1], dir[2]});
+}
+
+void *or_cloud_new(const double *p, const double *nrm, uint32_t np) {
+  if (np == 0) return nullptr;
+  Cloud *c = new Cloud;
+  c->p.assign(p, p + 3 * size_t(np));
+  if (nrm) c->n.assign(nrm, nrm + 3 * size_t(np));
+  c->build();
+  return c;
+}
+
+void or_cloud_free(void *c) { delete static_cast<Cloud *>(c); }
+
+void or_nearest_within_sq(const void *cloud, const double *q, uint32_t n, double r2,
+                          uint32_t *idx, double *d2, int threads) {
+  const Cloud *c = static_cast<const Cloud *>(cloud);
+  parallel_for(n, threads, [&](uint32_t i) {
+    if (!c->nearest_within_sq(q + 3 * size_t(i), r2, &idx[i], &d2[i])) {
+      idx[i] = MISS;
+      d2[i] = D_INF;
+    }
+  });
+}
+
+void or_nearest_below(const void *cloud, const double *q, uint32_t n, double bound,
+                      uint32_t *idx, double *dist, int threads) {
+  const Cloud *c = static_cast<const Cloud *>(cloud);
+  parallel_for(n, threads, [&](uint32_t i) {
+    if (!c->nearest_below(q + 3 * size_t(i), bound, &idx[i], &dist[i])) {
+      idx[i] = MISS;
+      dist[i] = D_INF;
+    }
+  });
+}
+
+void or_icp_rung(const double *src, uint32_t ns, const void *target, const double *inits,
+                 uint32_t k, sherd_icp_options opt, sherd_registration *out, int threads) {
+  const Cloud *c = static_cast<const Cloud *>(target);
+  parallel_for(k, threads, [&](uint32_t i) {
+    out[i] = icp_register(src, ns, *c, inits + 16 * size_t(i), opt);
+  });
+}
+
+void *or_surfaces_new(const void *fracture, const void *mesh, uint32_t watertight,
+                      double frac_area, const double *pf, uint32_t n_pf, const double *s,
+                      uint32_t n_s, const double *brk_p, const double *brk_ns, uint32_t n_brk,
+                      const double *margin_p, const double *margin_n, uint32_t n_margin) {
+  Surfaces *x = new Surfaces;
+  x->fracture = static_cast<const Mesh *>(fracture);
+  x->mesh = static_cast<const Mesh *>(mesh);
+  x->watertight = watertight != 0;
+  x->frac_area = frac_area;
+  x->pf.assign(pf, pf + 3 * size_t(n_pf));
+  x->s.assign(s, s + 3 * size_t(n_s));
+  x->brk_p.assign(brk_p, brk_p + 3 * size_t(n_brk));
+  x->brk_ns.assign(brk_ns, brk_ns + 3 * size_t(n_brk));
+  x->margin_p.assign(margin_p, margin_p + 3 * size_t(n_margin));
+  x->margin_n.assign(margin_n, margin_n + 3 * size_t(n_margin));
+  x->margin_tree.p = x->margin_p;
+  x->margin_tree.build();
+  return x;
+}
+
+void or_surfaces_free(void *s) { delete static_cast<Surfaces *>(s); }
+
+void or_verify(const void *a, const void *b, const double *pose, const sherd_scales *sc,
+               int full, sherd_scores *out) {
+  *out = verify(*static_cast<const Surfaces *>(a), *static_cast<const Surfaces *>(b), pose, *sc,
+                full != 0);
+}
+
+uint32_t or_accept(const sherd_scores *s, const sherd_params *p, const sherd_scales *sc) {
+  return accept(*s, *p, *sc);
+}
+
+void *or_pair_new(const void *a, const void *b, const void *reg_target, const void *frac_target,
+                  const double *reg_source, uint32_t n_reg, const double *frac_source,
+                  uint32_t n_frac, const sherd_scales *sc) {
+  Pair *p = new Pair;
+  p->a = static_cast<const Surfaces *>(a);
+  p->b = static_cast<const Surfaces *>(b);
+  p->reg_target = static_cast<const Cloud *>(reg_target);
+  p->frac_target = static_cast<const Cloud *>(frac_target);
+  p->reg_source.assign(reg_source, reg_source + 3 * size_t(n_reg));
+  p->frac_source.assign(frac_source, frac_source + 3 * size_t(n_frac));
+  p->sc = *sc;
+  return p;
+}
+
+void or_pair_free(void *p) { delete static_cast<Pair *>(p); }
+
+// The CPU baseline of the batched path: every item on `threads` host threads
+// (0 = all cores). Returns the thread count used.
+int or_ladder_verify_batch(void *const *pairs, uint32_t n_pairs, const sherd_work_item *items,
+                           uint32_t n_items, const sherd_params *p, int threads,
+                           sherd_candidate *out) {
+  if (threads <= 0) threads = default_threads();
+  parallel_for(n_items, threads, [&](uint32_t i) {
+    uint32_t pi = items[i].pair;
+    if (pi >= n_pairs) {
+      out[i] = sherd_candidate{};
+      out[i].status = uint32_t(-SHERD_E_INVALID);
+      return;
+    }
+    out[i] = ladder_verify(*static_cast<const Pair *>(pairs[pi]), items[i], *p, pi);
+  });
+  return threads;
+}
+
+void or_face_geometry(const double *v, const uint32_t *f, uint32_t nf, double *normals,
+                      double *areas, double *centroids) {
+  face_geometry(v, f, nf, normals, areas, centroids);
+}
+
+// thickness::face_indices (thickness.rs:387-390).
+uint32_t or_face_indices(uint32_t n_faces, uint32_t n, uint32_t *out) {
+  uint32_t nn = n ? n : 1;
+  uint32_t stride = (n_faces + nn - 1) / nn;
+  if (stride < 1) stride = 1;
+  uint32_t k = 0;
+  for (uint32_t i = 0; i < n_faces; i += stride) {
+    if (out) out[k] = i;
+    ++k;
+  }
+  return k;
+}
+
+// thickness::cast_inward_rays (thickness.rs:115-132).
+void or_cast_inward_rays(const void *mesh, const double *centroids, const double *normals,
+                         const uint32_t *idx, uint32_t n, float *t_hit, uint32_t *prim,
+                         int threads) {
+  const Mesh *m = static_cast<const Mesh *>(mesh);
+  parallel_for(n, threads, [&](uint32_t k) {
+    const double *c = centroids + 3 * size_t(idx[k]), *nn = normals + 3 * size_t(idx[k]);
+    double d[3] = {-nn[0], -nn[1], -nn[2]};
+    V3f o = {float(c[0] + d[0] * 1e-3), float(c[1] + d[1] * 1e-3), float(c[2] + d[2] * 1e-3)};
+    V3f dir = {float(d[0]), float(d[1]), float(d[2])};
+    m->first_hit(o, dir, &t_hit[k], &prim[k]);
+  });
+}
+
+int or_thickness_from_hits(const double *normals, uint32_t nf, const uint32_t *idx,
+                           const float *t_hit, const uint32_t *prim, uint32_t n, float *t,
+                           float *mode) {
+  return thickness_from_hits(normals, nf, idx, t_hit, prim, n, t, mode) ? 1 : 0;
+}
+
+float or_percentile90(const float *x, uint32_t n) {
+  return percentile90(std::vector<float>(x, x + n));
+}
+
+float or_hist_mode(const float *x, uint32_t n) { return hist_mode(std::vector<float>(x, x + n)); }
+
+void or_cone_votes(const void *mesh, const double *centroids, const double *normals,
+                   const double *ns, const double *hit_normals, uint32_t nf, double thick,
+                   uint8_t *good, int threads) {
+  const Mesh *m = static_cast<const Mesh *>(mesh);
+  parallel_for(nf, threads, [&](uint32_t i) {
+    good[i] = cone_vote(*m, centroids + 3 * size_t(i), normals + 3 * size_t(i),
+                        ns + 3 * size_t(i), hit_normals, nf, thick);
+  });
+}
+
+void or_eigen_pivots(const double *a36, int *perm) {
+  double a[6][6];
+  std::memcpy(a, a36, sizeof a);
+  eigen_pivots(a, perm);
+}
+
+int or_solve_ldlt(const double *a36, const double *b, double *x) {
+  double a[6][6];
+  std::memcpy(a, a36, sizeof a);
+  return solve_ldlt(a, b, x) ? 1 : 0;
+}
+
+void or_pose_inverse(const double *t, double *out) { pose_inverse(t, out); }
+
+void or_euler_zyx(double a, double b, double g, double *r9) {
+  double r[3][3];
+  euler_zyx(a, b, g, r);
+  std::memcpy(r9, r, sizeof r);
+}
+
+float or_tri_distance(const float *p, const float *a, const float *b, const float *c) {
+  return tri_distance({p[0], p[1], p[2]}, {a[0], a[1], a[2]}, {b[0], b[1], b[2]},
+                      {c[0], c[1], c[2]});
+}
+
+float or_moller_trumbore(const float *o, const float *d, const float *a, const float *b,
+                         const float *c) {
+  return moller_trumbore({o[0], o[1], o[2]}, {d[0], d[1], d[2]}, {a[0], a[1], a[2]},
+                         {b[0], b[1], b[2]}, {c[0], c[1], c[2]});
+}
+
+int or_default_threads(void) { return default_threads(); }
+
+}  // extern "C"

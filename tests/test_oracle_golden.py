@@ -1,0 +1,125 @@
+"""The oracle pinned against the reference's own golden vectors (the slab fixture).
+
+Rows follow the reference's parity harness (crates/sherd-parity/src/stages/*.rs):
+thickness bit-exact from injected hits, first hits and cone votes statistically against the
+Embree answers the fixture carries, the stage-2 ladder within D 10.2's pose rows and the
+verification within its score rows with identical verdicts.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from _slab import (CHAOTIC_SHARE, ROT_DEG, TRANS_T, VERIFY_TOL, origin_t, oracle_pair, piece,
+                   reference_scores, score_dict, slab_params, trace_deg)
+
+
+@pytest.mark.parametrize("name", ["pieceA", "pieceB"])
+def test_thickness_from_the_fixture_hits_is_bit_exact(slab, oracle, name):
+    """thickness.rs:139-162 fed thick.idx/t_hit/prim reproduces thick.t and thick_mode."""
+    p = piece(slab, name)
+    normals, _, _ = oracle.face_geometry(p["V0"], p["F"])
+    t, mode = oracle.thickness_from_hits(normals, p["thick_idx"], p["thick_t_hit"], p["thick_prim"])
+    assert t == p["thick_t"] and mode == p["thick_mode"], (t, p["thick_t"], mode, p["thick_mode"])
+
+
+@pytest.mark.parametrize("name", ["pieceA", "pieceB"])
+def test_face_geometry_matches_numpy_element_for_element(slab, oracle, name):
+    p = piece(slab, name)
+    normals, areas, cent = oracle.face_geometry(p["V"], p["F"])
+    v = p["V"]
+    f = p["F"].astype(np.int64)
+    assert np.array_equal(cent, (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3.0)
+    assert np.all(np.abs(np.linalg.norm(normals, axis=1) - 1.0) < 1e-12)
+    assert np.isclose(areas[p["frac"].astype(bool)].sum(), p["frac_area"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["pieceA", "pieceB"])
+def test_first_hits_agree_with_the_fixture_rays(slab, oracle, name):
+    """E4's measurement (spatial/bvh.rs:10-19): the same rays, the same answers up to grazing
+    edges; and the thickness from our own hits lands in the reference's histogram bin."""
+    p = piece(slab, name)
+    normals, _, cent = oracle.face_geometry(p["V0"], p["F"])
+    mesh = oracle.Mesh(p["V0"], p["F"])
+    idx = oracle.face_indices(len(p["F"]))
+    assert np.array_equal(idx, p["thick_idx"])
+    t, prim = oracle.cast_inward_rays(mesh, cent, normals, idx)
+    ref_t, ref_prim = p["thick_t_hit"], p["thick_prim"]
+    hit, ref_hit = np.isfinite(t), np.isfinite(ref_t)
+    assert np.mean(hit == ref_hit) > 0.999
+    both = hit & ref_hit
+    assert np.mean(prim[both] == ref_prim[both]) > 0.995
+    same = both & (prim == ref_prim)
+    assert np.max(np.abs(t[same] - ref_t[same])) < 1e-4 * float(p["thick_t"])
+    mine = oracle.thickness_from_hits(normals, idx, t, prim)
+    bin_width = float(p["thick_t"]) * 2.0 / 60.0
+    assert abs(float(mine[0]) - float(p["thick_t"])) <= bin_width
+
+
+@pytest.mark.parametrize("name", ["pieceA", "pieceB"])
+def test_cone_votes_agree_with_the_fixture(slab, oracle, name):
+    """R 3.4.3 over the dump's own smoothed normals (segment.rs:318-376) against seg.good."""
+    p = piece(slab, name)
+    normals, _, cent = oracle.face_geometry(p["V"], p["F"])
+    mesh = oracle.Mesh(p["V"], p["F"])
+    good = oracle.cone_votes(mesh, cent, normals, p["seg_NS"], normals, float(p["thick_t"]))
+    ref = p["seg_good"]
+    assert np.mean(good == ref) > 0.998
+    assert np.mean((good >= 5) == (ref >= 5)) > 0.999
+
+
+def test_stage2_ladder_matches_the_reference(slab, oracle):
+    """The four rungs from s1.T[nms2.kept] against s2.T_reg1..T_frac2 (stage2.rs:40-50): every
+    rung within 0.05 deg / 0.01 t, except chaotic ladders the reference itself refused."""
+    op = oracle_pair(oracle, slab)
+    sc = op["scales"]
+    t = sc.t
+    poses = slab["starts"].reshape(-1, 16)
+    rungs = [(op["b"]["arrays"]["reg_p"], op["reg_t"], 0.2), (op["b"]["arrays"]["reg_p"], op["reg_t"], 0.08),
+             (op["b"]["arrays"]["frac_p"], op["frac_t"], 0.08), (op["b"]["arrays"]["frac_p"], op["frac_t"], 0.04)]
+    names = ("s2_T_reg1", "s2_T_reg2", "s2_T_frac1", "s2_T_frac2")
+    chaotic = set()
+    for (src, tgt, k), name in zip(rungs, names):
+        regs = oracle.icp_rung(src, tgt, poses, k * t * sc.icp, 30)
+        poses = np.array([np.array(r.transform[:]) for r in regs])
+        for c in range(len(poses)):
+            mine = poses[c].reshape(4, 4)
+            ref = slab[name][c]
+            if trace_deg(mine, ref) > ROT_DEG or origin_t(mine, ref, t) > TRANS_T:
+                chaotic.add(c)
+    accepted = slab["s2_accepted"].astype(bool)
+    assert len(chaotic) <= CHAOTIC_SHARE * len(accepted), chaotic
+    assert not any(accepted[c] for c in chaotic), chaotic
+
+
+def test_verify_matches_the_reference_scores(slab, oracle):
+    """R 6 at s2.T_frac2 against s2.scores.json and s2.accepted (verify.rs:74-86)."""
+    op = oracle_pair(oracle, slab)
+    params = slab_params(oracle, slab)
+    for k, pose in enumerate(slab["s2_T_frac2"]):
+        s = oracle.verify(op["a"]["surf"], op["b"]["surf"], pose, op["scales"], True)
+        mine, ref = score_dict(s), reference_scores(slab, k)
+        for key, tol in VERIFY_TOL.items():
+            assert abs(mine[key] - ref[key]) <= tol, (k, key, mine[key], ref[key])
+        assert oracle.accept(s, params, op["scales"]) == bool(slab["s2_accepted"][k]), k
+
+
+def test_the_batched_ladder_reproduces_the_reference_verdicts(slab, oracle):
+    """The whole stage-2 work item (4 rungs + R 6 + R 6.5) on the oracle's thread pool."""
+    op = oracle_pair(oracle, slab)
+    params = slab_params(oracle, slab)
+    items = [oracle.WorkItem(0, k, (C.c_double * 16)(*slab["starts"][k].reshape(16)))
+             for k in range(len(slab["starts"]))]
+    cands, used = oracle.ladder_verify_batch([op["pair"]], items, params)
+    assert used >= 1
+    got = np.array([c.accepted for c in cands], bool)
+    assert np.array_equal(got, slab["s2_accepted"].astype(bool))
+    for k, c in enumerate(cands):
+        ref = slab["s2_T_frac2"][k]
+        mine = np.array(c.rungs[3].transform[:]).reshape(4, 4)
+        if slab["s2_accepted"][k]:
+            assert trace_deg(mine, ref) <= ROT_DEG and origin_t(mine, ref, op["scales"].t) <= TRANS_T
+            assert abs(c.scores.tight - reference_scores(slab, k)["tight"]) <= VERIFY_TOL["tight"]
