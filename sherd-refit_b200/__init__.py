@@ -1,0 +1,22 @@
+"""sherd-refit B200 backend: the geometry hot path of sherd-refit on sm_100a CUDA kernels.
+
+The package wraps the C ABI of include/sherd_cuda.h (built into `_lib/libsherd_cuda.so`):
+device LBVHs over fragment meshes and point clouds, first-hit and parity rays, bounded
+point-to-mesh distances, exact nearest neighbours, the point-to-plane ICP ladder, the R 6
+verification and the batched persistent stage-2 path, plus the differentiable pose objective
+(`adjoint`). There is no CPU fallback: if the library is missing, using it raises.
+"""
+
+from ._abi import (Candidate, IcpOptions, InsideOutcome, Params, Registration, Scales, Scores,
+                   SherdError, WorkItem, REDUCE_ALL, REDUCE_MIN, SCHED_BATCHED, SCHED_PLAIN,
+                   exported_symbols, lib)
+from .backend import (Cloud, Context, CudaExecutor, DistBatch, IcpBatch, InsideBatch, Mesh, Pair,
+                      Surfaces, accept, default_params, scales_for_pair, work_items)
+
+__all__ = [
+    "Candidate", "Cloud", "Context", "CudaExecutor", "DistBatch", "IcpBatch", "IcpOptions",
+    "InsideBatch", "InsideOutcome", "Mesh", "Pair", "Params", "Registration", "Scales", "Scores",
+    "SherdError", "Surfaces", "WorkItem", "REDUCE_ALL", "REDUCE_MIN", "SCHED_BATCHED",
+    "SCHED_PLAIN", "accept", "default_params", "exported_symbols", "lib", "scales_for_pair",
+    "work_items",
+]

@@ -1,0 +1,406 @@
+"""The CUDA backend as Python objects: a context, device meshes and clouds, and the calls of
+include/sherd_cuda.h with numpy arrays in and out.
+
+Names follow the reference: `Mesh` is its `RayScene` (spatial/bvh.rs:36-192), `Cloud` its
+`PointTree` with optional normals (spatial/kdtree.rs:31-258; `IcpTarget`, matching/icp.rs:
+205-302), `Surfaces` its R 6 view of a fragment (matching/verify.rs:223-299), `Pair` what
+`Pair::stage2_batch` reads (matching/pair.rs:298-372, 592-630).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import json
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi as A
+from ._abi import check, ptr
+
+
+def _f32(a, shape=(-1, 3)):
+    return np.ascontiguousarray(a, dtype=np.float32).reshape(shape)
+
+
+def _f64(a, shape=(-1, 3)):
+    return np.ascontiguousarray(a, dtype=np.float64).reshape(shape)
+
+
+def _u32(a, shape=(-1,)):
+    return np.ascontiguousarray(a, dtype=np.uint32).reshape(shape)
+
+
+def _pose(t) -> np.ndarray:
+    return _f64(t, (16,))
+
+
+def default_params() -> A.Params:
+    """Params::default (params.rs:141-190), the fields the C ABI reads."""
+    p = A.Params()
+    A.lib().sherd_params_default(C.byref(p))
+    return p
+
+
+def scales_for_pair(params: A.Params, t: float, res: float) -> A.Scales:
+    """Scales::for_pair (matching/scales.rs:72-88)."""
+    s = A.Scales()
+    rc = A.lib().sherd_scales_for_pair(C.byref(params), float(t), float(res), C.byref(s))
+    if rc:
+        raise A.SherdError(rc, "scales_for_pair")
+    return s
+
+
+def accept(scores: A.Scores, params: A.Params, scales: A.Scales) -> bool:
+    """verify::accept (matching/verify.rs:632-638)."""
+    return bool(A.lib().sherd_accept(C.byref(scores), C.byref(params), C.byref(scales)))
+
+
+class Context:
+    """One device and its stream (sherd_open); every call of this backend goes through one."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        rc = A.lib().sherd_open(int(device), C.byref(self.h))
+        if rc:
+            msg = A.lib().sherd_last_error(None)
+            raise A.SherdError(rc, msg.decode() if msg else "sherd_open failed")
+        self.device = device
+
+    def close(self):
+        if self.h:
+            A.lib().sherd_close(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- context ---------------------------------------------------------------------------
+    @property
+    def name(self) -> str:
+        """Executor::name (executor/mod.rs:107)."""
+        return A.lib().sherd_name().decode()
+
+    def device_slack(self) -> int:
+        """Executor::device_slack (executor/mod.rs:134-136)."""
+        return int(A.lib().sherd_device_slack(self.h))
+
+    def set_timeout_ms(self, ms: int) -> None:
+        check(self.h, A.lib().sherd_set_timeout_ms(self.h, int(ms)))
+
+    def abort(self) -> None:
+        check(self.h, A.lib().sherd_abort(self.h))
+
+    def stats(self) -> dict:
+        buf = C.create_string_buffer(1 << 16)
+        check(self.h, A.lib().sherd_stats_json(self.h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    # -- objects -------------------------------------------------------------------------------
+    def mesh(self, v, f) -> "Mesh":
+        return Mesh(self, v, f)
+
+    def cloud(self, p, n=None) -> "Cloud":
+        return Cloud(self, p, n)
+
+    # -- Executor-shaped calls -------------------------------------------------------------------
+    def first_hit(self, mesh: "Mesh", origins, dirs):
+        """RayScene::first_hit for every ray: (t f32, prim u32), +inf / 0xFFFFFFFF on a miss."""
+        o, d = _f32(origins), _f32(dirs)
+        n = len(o)
+        t = np.empty(n, np.float32)
+        prim = np.empty(n, np.uint32)
+        check(self.h, A.lib().sherd_first_hit(self.h, mesh.h, o, d, n, t, prim))
+        return t, prim
+
+    def bounded_distance(self, mesh: "Mesh", points, pose, max_dist, reduce=A.REDUCE_ALL):
+        """Executor::bounded_distance (executor/cpu.rs:84-113)."""
+        p = _f64(points)
+        out = np.empty(1 if reduce == A.REDUCE_MIN else len(p), np.float64)
+        check(self.h, A.lib().sherd_bounded_distance(self.h, mesh.h, p, len(p), _pose(pose),
+                                                    float(max_dist), int(reduce), out))
+        return out
+
+    def inside(self, mesh: "Mesh", points, pose):
+        """Executor::inside (executor/cpu.rs:115-128): (depth f32, inside u32) per point."""
+        p = _f64(points)
+        out = (A.InsideOutcome * max(len(p), 1))()
+        check(self.h, A.lib().sherd_inside(self.h, mesh.h, p, len(p), _pose(pose),
+                                          C.cast(out, C.c_void_p)))
+        arr = np.frombuffer(out, dtype=np.dtype([("depth", np.float32), ("inside", np.uint32)]),
+                            count=len(p))
+        return arr["depth"].copy(), arr["inside"].copy()
+
+    def icp_rung(self, source, target: "Cloud", inits, distance, max_iteration=30):
+        """Executor::icp_rung (executor/cpu.rs:70-82), point-to-plane."""
+        s = _f64(source)
+        inits = _f64(inits, (-1, 16))
+        out = (A.Registration * max(len(inits), 1))()
+        opt = A.IcpOptions(A.POINT_TO_PLANE, int(max_iteration), float(distance))
+        check(self.h, A.lib().sherd_icp_rung(self.h, ptr(s), len(s), target.h, inits, len(inits),
+                                            opt, C.cast(out, C.c_void_p)))
+        return list(out)[:len(inits)]
+
+    # -- preprocessing rays ---------------------------------------------------------------------
+    def face_geometry(self, v, f):
+        """mesh::geometry::face_geometry (mesh/geometry.rs:70-96): normals, areas, centroids."""
+        v, f = _f64(v), _u32(f, (-1, 3))
+        nf = len(f)
+        n = np.empty((nf, 3))
+        a = np.empty(nf)
+        c = np.empty((nf, 3))
+        check(self.h, A.lib().sherd_face_geometry(self.h, v, len(v), f, nf, ptr(n), ptr(a), ptr(c)))
+        return n, a, c
+
+    def thickness(self, mesh: "Mesh", centroids, normals, max_rays=300_000, return_hits=False):
+        """R 3.2 (fragment/thickness.rs:99-162): (t, thick_mode) or None when < 100 rays hit."""
+        cen, nrm = _f64(centroids), _f64(normals)
+        nf = len(nrm)
+        stride = max(1, -(-nf // max(max_rays, 1)))
+        n = -(-nf // stride)
+        t, m, found = C.c_float(), C.c_float(), C.c_uint32()
+        th = np.empty(n, np.float32) if return_hits else None
+        pr = np.empty(n, np.uint32) if return_hits else None
+        check(self.h, A.lib().sherd_thickness(self.h, mesh.h, cen, nrm, nf, int(max_rays),
+                                             C.byref(t), C.byref(m), C.byref(found), ptr(th),
+                                             ptr(pr)))
+        res = (np.float32(t.value), np.float32(m.value)) if found.value else None
+        return (res, th, pr) if return_hits else res
+
+    def thickness_from_hits(self, normals, idx, t_hit, prim):
+        """thickness_from_hits (fragment/thickness.rs:139-162) on the device."""
+        nrm = _f64(normals)
+        t, m, found = C.c_float(), C.c_float(), C.c_uint32()
+        idx, th, pr = _u32(idx), _f32(t_hit, (-1,)), _u32(prim)
+        check(self.h, A.lib().sherd_thickness_from_hits(self.h, nrm, len(nrm), idx, th, pr,
+                                                       len(idx), C.byref(t), C.byref(m),
+                                                       C.byref(found)))
+        return (np.float32(t.value), np.float32(m.value)) if found.value else None
+
+    def cone_votes(self, mesh: "Mesh", centroids, normals, ns, hit_normals, thick):
+        """R 3.4.3's seven-ray cone vote per face (fragment/segment.rs:318-376)."""
+        nf = len(normals)
+        good = np.empty(nf, np.uint8)
+        check(self.h, A.lib().sherd_cone_votes(self.h, mesh.h, _f64(centroids), _f64(normals),
+                                              _f64(ns), _f64(hit_normals), nf, float(thick), good))
+        return good
+
+    # -- verification and the batched stage-2 path ---------------------------------------------
+    def surfaces(self, fracture: "Mesh", mesh: "Mesh | None", watertight, frac_area, pf, s,
+                 brk_p, brk_ns, margin_p, margin_n) -> "Surfaces":
+        return Surfaces(self, fracture, mesh, watertight, frac_area, pf, s, brk_p, brk_ns,
+                        margin_p, margin_n)
+
+    def verify(self, a: "Surfaces", b: "Surfaces", pose, scales: A.Scales, full=True) -> A.Scores:
+        """verify::verify (matching/verify.rs:590-626) on the device."""
+        out = A.Scores()
+        check(self.h, A.lib().sherd_verify(self.h, a.h, b.h, _pose(pose), C.byref(scales),
+                                          int(full), C.byref(out)))
+        return out
+
+    def pair(self, a: "Surfaces", b: "Surfaces", reg_target: "Cloud", frac_target: "Cloud",
+             reg_source, frac_source, scales: A.Scales) -> "Pair":
+        return Pair(self, a, b, reg_target, frac_target, reg_source, frac_source, scales)
+
+    def ladder_verify_batch(self, pairs, items, params: A.Params, sched=A.SCHED_BATCHED):
+        """R 5.6 + R 6 + R 6.5 for every (pair, start); `items` is a ctypes WorkItem array or a
+        list of (pair, start, init 4x4) tuples. Returns the ctypes Candidate array."""
+        if not isinstance(items, C.Array):
+            items = work_items(items)
+        arr = (C.c_void_p * max(len(pairs), 1))(*[p.h for p in pairs])
+        out = (A.Candidate * max(len(items), 1))()
+        check(self.h, A.lib().sherd_ladder_verify_batch(self.h, arr, len(pairs),
+                                                       C.cast(items, C.c_void_p), len(items),
+                                                       C.byref(params), int(sched),
+                                                       C.cast(out, C.c_void_p)))
+        return out
+
+
+def work_items(items) -> C.Array:
+    """(pair index, start id, 4x4 init) tuples as the C ABI's work-item array."""
+    arr = (A.WorkItem * max(len(items), 1))()
+    for k, (p, s, t) in enumerate(items):
+        arr[k].pair = int(p)
+        arr[k].start = int(s)
+        arr[k].init[:] = [float(x) for x in _pose(t)]
+    return arr
+
+
+class _Handle:
+    _free = ""
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                getattr(A.lib(), self._free)(h)
+            except Exception:
+                pass
+            self.h = None
+
+
+class Mesh(_Handle):
+    """A device triangle LBVH (RayScene::of_mesh, spatial/bvh.rs:56-62)."""
+    _free = "sherd_mesh_free"
+
+    def __init__(self, ctx: Context, v, f, _handle=None):
+        self.ctx = ctx
+        if _handle is not None:
+            self.h = _handle
+            return
+        v, f = _f32(v), _u32(f, (-1, 3))
+        h = C.c_void_p()
+        check(ctx.h, A.lib().sherd_mesh_upload(ctx.h, v, len(v), f, len(f), C.byref(h)))
+        self.h = h
+
+    def subset(self, keep) -> "Mesh":
+        """RayScene::of_subset (spatial/bvh.rs:71-78)."""
+        keep = np.ascontiguousarray(keep, dtype=np.uint8)
+        h = C.c_void_p()
+        check(self.ctx.h, A.lib().sherd_mesh_subset(self.ctx.h, self.h, keep, C.byref(h)))
+        return Mesh(self.ctx, None, None, _handle=h)
+
+    @property
+    def n_faces(self) -> int:
+        return int(A.lib().sherd_mesh_faces(self.h))
+
+    def aabb(self):
+        lo, hi = np.empty(3, np.float32), np.empty(3, np.float32)
+        A.lib().sherd_mesh_aabb(self.h, lo, hi)
+        return lo, hi
+
+
+class Cloud(_Handle):
+    """A device point LBVH with optional normals (PointTree / IcpTarget)."""
+    _free = "sherd_cloud_free"
+
+    def __init__(self, ctx: Context, p, n=None):
+        self.ctx = ctx
+        p = _f64(p)
+        nn = None if n is None else _f64(n)
+        h = C.c_void_p()
+        check(ctx.h, A.lib().sherd_cloud_upload(ctx.h, p, ptr(nn), len(p), C.byref(h)))
+        self.h = h
+        self.n = len(p)
+
+    def nearest_within_sq(self, queries, r2):
+        """PointTree::nearest_within_squared (spatial/kdtree.rs:202-217)."""
+        q = _f64(queries)
+        idx = np.empty(len(q), np.uint32)
+        d2 = np.empty(len(q), np.float64)
+        check(self.ctx.h, A.lib().sherd_nearest_within_sq(self.ctx.h, self.h, q, len(q),
+                                                         float(r2), idx, d2))
+        return idx, d2
+
+    def nearest_below(self, queries, bound):
+        """PointTree::nearest_below (spatial/kdtree.rs:182-190)."""
+        q = _f64(queries)
+        idx = np.empty(len(q), np.uint32)
+        d = np.empty(len(q), np.float64)
+        check(self.ctx.h, A.lib().sherd_nearest_below(self.ctx.h, self.h, q, len(q), float(bound),
+                                                     idx, d))
+        return idx, d
+
+
+class Surfaces(_Handle):
+    """verify::Surfaces (matching/verify.rs:223-299) on the device."""
+    _free = "sherd_surfaces_free"
+
+    def __init__(self, ctx, fracture, mesh, watertight, frac_area, pf, s, brk_p, brk_ns, margin_p,
+                 margin_n):
+        self.ctx = ctx
+        self.keep = (fracture, mesh)
+        arrs = [_f64(x) for x in (pf, s, brk_p, brk_ns, margin_p, margin_n)]
+        pf, s, bp, bn, mp, mn = arrs
+        h = C.c_void_p()
+        check(ctx.h, A.lib().sherd_surfaces_create(
+            ctx.h, fracture.h, mesh.h if mesh is not None else None, int(bool(watertight)),
+            float(frac_area), ptr(pf), len(pf), ptr(s), len(s), ptr(bp), ptr(bn), len(bp),
+            ptr(mp), ptr(mn), len(mp), C.byref(h)))
+        self.h = h
+
+
+class Pair(_Handle):
+    """One pair of the batched stage-2 path (matching/pair.rs:298-372, 592-630)."""
+    _free = "sherd_pair_free"
+
+    def __init__(self, ctx, a, b, reg_target, frac_target, reg_source, frac_source, scales):
+        self.ctx = ctx
+        self.keep = (a, b, reg_target, frac_target)
+        rs, fs = _f64(reg_source), _f64(frac_source)
+        self.scales = scales
+        self.n_reg, self.n_frac = len(rs), len(fs)
+        h = C.c_void_p()
+        check(ctx.h, A.lib().sherd_pair_create(ctx.h, a.h, b.h, reg_target.h, frac_target.h,
+                                              ptr(rs), len(rs), ptr(fs), len(fs),
+                                              C.byref(scales), C.byref(h)))
+        self.h = h
+
+
+# ---------------------------------------------------------------------------------------------
+# The reference's Executor trait (executor/mod.rs:105-137), over this backend
+# ---------------------------------------------------------------------------------------------
+
+@dataclass
+class IcpBatch:
+    """IcpBatch (executor/batch.rs:218-228)."""
+    source: np.ndarray
+    target: Cloud
+    inits: np.ndarray
+    max_correspondence_distance: float
+    max_iteration: int = 30
+    estimation: int = A.POINT_TO_PLANE
+
+
+@dataclass
+class DistBatch:
+    """DistBatch (executor/batch.rs:283-296)."""
+    points: np.ndarray
+    transform: np.ndarray
+    scene: Mesh
+    max_dist: float
+    reduce: int = A.REDUCE_ALL
+
+
+@dataclass
+class InsideBatch:
+    """InsideBatch (executor/batch.rs:314-323)."""
+    points: np.ndarray
+    transform: np.ndarray
+    scene: Mesh
+
+
+class CudaExecutor:
+    """`impl Executor for CudaExecutor`: the trait's methods, answered on the device only.
+
+    `coarse_scores` (R 5.2) is not part of this backend; it raises rather than answering on
+    the host. Errors raise `SherdError`: there is no silent CPU fallback.
+    """
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def name(self) -> str:
+        return self.ctx.name
+
+    def coarse_scores(self, batch):
+        raise NotImplementedError("the coarse breakline score is not on this backend")
+
+    def icp_rung(self, batch: IcpBatch):
+        if batch.estimation != A.POINT_TO_PLANE:
+            raise A.SherdError(A.E_INVALID, "only the point-to-plane rung runs on the device")
+        return self.ctx.icp_rung(batch.source, batch.target, batch.inits,
+                                 batch.max_correspondence_distance, batch.max_iteration)
+
+    def bounded_distance(self, batch: DistBatch) -> np.ndarray:
+        return self.ctx.bounded_distance(batch.scene, batch.points, batch.transform,
+                                         batch.max_dist, batch.reduce)
+
+    def inside(self, batch: InsideBatch):
+        return self.ctx.inside(batch.scene, batch.points, batch.transform)
+
+    def device_slack(self) -> int:
+        return self.ctx.device_slack()

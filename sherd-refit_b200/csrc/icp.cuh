@@ -1,0 +1,263 @@
+// icp.cuh — one point-to-plane registration_icp rung as a CTA-cooperative
+// routine (matching/icp.rs:308-440, 599-778).
+//
+// Every pass over the moving cloud is one fused loop: transform the point by
+// the current pose (f64, R p + tau), find the nearest target inside the strict
+// radius (exact, lowest index on ties), and accumulate the correspondence
+// count, the squared error and the 27 normal-equation terms (21 of the lower
+// triangle of J^T J, 6 of J^T r) in f64 registers. A pass ends with a warp
+// shuffle tree and a fixed-order sum over the warps, so a rung is bit-for-bit
+// reproducible run to run. One thread then runs Open3D's convergence test,
+// Eigen's pivoted LDLT (f64) and the Rz Ry Rx update, and publishes the pose.
+//
+// The points are the reference numerics (Numerics::REFERENCE, f64 point loops,
+// World assembly); the difference from the CPU oracle is the summation order
+// of the per-pass sums and the pose being re-applied to the source each pass
+// (T S) where the reference moves the previous pass's points (U P).
+#pragma once
+
+#include "traverse.cuh"
+
+namespace sherd {
+
+constexpr int ICP_BLOCK = 256;
+constexpr int ICP_SUMS = 29;  // count, err2, jtj[21], jtr[6]
+
+struct IcpShared {
+  double red[ICP_BLOCK / 32][ICP_SUMS];
+  double sums[ICP_SUMS];
+  double t[16];
+  int stop;
+};
+
+// icp::eigen_pivots (icp.rs:661-674).
+__device__ void eigen_pivots(const double a[6][6], int perm[6]) {
+  for (int k = 0; k < 6; ++k) perm[k] = k;
+  for (int k = 0; k < 6; ++k) {
+    int best = k;
+    for (int i = k + 1; i < 6; ++i)
+      if (fabs(a[perm[i]][perm[i]]) > fabs(a[perm[best]][perm[best]])) best = i;
+    int tmp = perm[k];
+    perm[k] = perm[best];
+    perm[best] = tmp;
+  }
+}
+
+// icp::solve_ldlt (icp.rs:692-753).
+__device__ bool solve_ldlt(const double a[6][6], const double b[6], double x[6]) {
+  int perm[6];
+  eigen_pivots(a, perm);
+  double m[6][6];
+  for (int k = 0; k < 6; ++k)
+    for (int l = 0; l < 6; ++l) m[k][l] = a[perm[k]][perm[l]];
+  for (int k = 0; k < 6; ++k) {
+    if (k > 0) {
+      double temp[6];
+      for (int j = 0; j < k; ++j) temp[j] = m[j][j] * m[k][j];
+      double diagonal = m[k][k];
+      for (int j = 0; j < k; ++j) diagonal -= m[k][j] * temp[j];
+      m[k][k] = diagonal;
+      for (int r = k + 1; r < 6; ++r) {
+        double below = m[r][k];
+        for (int j = 0; j < k; ++j) below -= m[r][j] * temp[j];
+        m[r][k] = below;
+      }
+    }
+    double pivot = m[k][k];
+    if (pivot != 0.0)
+      for (int r = k + 1; r < 6; ++r) m[r][k] /= pivot;
+  }
+  double y[6];
+  for (int k = 0; k < 6; ++k) y[k] = b[perm[k]];
+  for (int i = 0; i < 6; ++i) {
+    double value = y[i];
+    for (int j = 0; j < i; ++j) value -= m[i][j] * y[j];
+    y[i] = value;
+  }
+  for (int i = 0; i < 6; ++i) {
+    double pivot = m[i][i];
+    y[i] = fabs(pivot) > 2.2250738585072014e-308 ? y[i] / pivot : 0.0;
+  }
+  for (int i = 5; i >= 0; --i) {
+    double value = y[i];
+    for (int j = i + 1; j < 6; ++j) value -= m[j][i] * y[j];
+    y[i] = value;
+  }
+  for (int k = 0; k < 6; ++k) x[perm[k]] = y[k];
+  for (int k = 0; k < 6; ++k)
+    if (!isfinite(x[k])) return false;
+  return true;
+}
+
+__device__ void mat3mul(const double a[3][3], const double b[3][3], double o[3][3]) {
+  double r[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r[i][j] = (a[i][0] * b[0][j] + a[i][1] * b[1][j]) + a[i][2] * b[2][j];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) o[i][j] = r[i][j];
+}
+
+// icp::euler_zyx (icp.rs:770-778).
+__device__ void euler_zyx(double al, double be, double ga, double r[3][3]) {
+  double sa, ca, sb, cb, sg, cg;
+  sincos(al, &sa, &ca);
+  sincos(be, &sb, &cb);
+  sincos(ga, &sg, &cg);
+  double rx[3][3] = {{1, 0, 0}, {0, ca, -sa}, {0, sa, ca}};
+  double ry[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}};
+  double rz[3][3] = {{cg, -sg, 0}, {sg, cg, 0}, {0, 0, 1}};
+  double t[3][3];
+  mat3mul(rz, ry, t);
+  mat3mul(t, rx, r);
+}
+
+__device__ void matmul4(const double *a, const double *b, double *o) {
+  double r[16];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      double s = a[4 * i] * b[j];
+      for (int k = 1; k < 4; ++k) s += a[4 * i + k] * b[4 * k + j];
+      r[4 * i + j] = s;
+    }
+  for (int i = 0; i < 16; ++i) o[i] = r[i];
+}
+
+// The point-to-plane update from the pass sums (icp.rs:408-440): identity when
+// there is no correspondence, no normal or no finite solution.
+__device__ void plane_update(const double *s, bool has_normals, double u[16]) {
+  for (int i = 0; i < 16; ++i) u[i] = (i % 5 == 0) ? 1.0 : 0.0;
+  if (s[0] == 0.0 || !has_normals) return;
+  double a[6][6], rhs[6], x[6];
+  int q = 2;
+  for (int k = 0; k < 6; ++k)
+    for (int l = 0; l <= k; ++l) {
+      a[k][l] = s[q];
+      a[l][k] = s[q];
+      ++q;
+    }
+  for (int k = 0; k < 6; ++k) rhs[k] = -s[23 + k];
+  if (!solve_ldlt(a, rhs, x)) return;
+  double r[3][3];
+  euler_zyx(x[0], x[1], x[2], r);
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) u[4 * i + j] = r[i][j];
+    u[4 * i + 3] = x[3 + i];
+  }
+}
+
+// One correspondence pass (icp::correspondences + icp::normal_equations) over
+// `src` under the pose sh.t; leaves the block totals in sh.sums.
+__device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, double r2,
+                         bool valid, IcpShared &sh, uint32_t &status) {
+  double acc[ICP_SUMS];
+#pragma unroll
+  for (int k = 0; k < ICP_SUMS; ++k) acc[k] = 0.0;
+  double t[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) t[k] = sh.t[k];
+  if (valid) {
+    for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) {
+      double4 p = src[i];
+      double x, y, z;
+      apply_pose(t, p.x, p.y, p.z, x, y, z);
+      double d2;
+      int s = nearest_within_sq(tgt, x, y, z, r2, d2, status);
+      if (s < 0 || !(d2 < r2)) continue;
+      acc[0] += 1.0;
+      acc[1] += d2;
+      if (tgt.nrm) {
+        double4 q = tgt.pts[s];
+        double4 n = tgt.nrm[s];
+        double row[6] = {y * n.z - z * n.y, z * n.x - x * n.z, x * n.y - y * n.x, n.x, n.y, n.z};
+        double r = (x - q.x) * n.x + (y - q.y) * n.y + (z - q.z) * n.z;
+        int m = 2;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+#pragma unroll
+          for (int l = 0; l <= k; ++l) acc[m++] += row[k] * row[l];
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[23 + k] += row[k] * r;
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < ICP_SUMS; ++k) {
+    double v = acc[k];
+    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh.red[warp][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < ICP_SUMS) {
+    double v = sh.red[0][threadIdx.x];
+    for (int w = 1; w < ICP_BLOCK / 32; ++w) v += sh.red[w][threadIdx.x];
+    sh.sums[threadIdx.x] = v;
+  }
+  __syncthreads();
+}
+
+// Open3D's (fitness, inlier_rmse) from the pass sums (icp.rs:385-391).
+__device__ __forceinline__ void fit_rmse(const double *s, uint32_t ns, double &fit, double &rmse) {
+  if (s[0] == 0.0) {
+    fit = 0.0;
+    rmse = 0.0;
+    return;
+  }
+  fit = s[0] / double(ns);
+  rmse = sqrt(s[1] / s[0]);
+}
+
+// icp::register (icp.rs:308-356) for the pose in sh.t; every thread of the
+// block calls it. On return sh.t holds the refined pose and thread 0 has
+// written *out.
+__device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView &tgt,
+                               double distance, int max_iter, IcpShared &sh,
+                               sherd_registration *out, uint32_t &status) {
+  if (ns == 0 || tgt.n == 0) {
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < 16; ++k) out->transform[k] = sh.t[k];
+      out->fitness = 0.0;
+      out->inlier_rmse = 0.0;
+      out->correspondences = 0;
+      out->iterations = 0;
+      out->converged = 0;
+    }
+    __syncthreads();
+    return;
+  }
+  bool valid = distance > 0.0;  // a NaN radius is not valid either
+  double r2 = distance * distance;
+  icp_pass(src, ns, tgt, r2, valid, sh, status);
+  double fit, rmse;
+  fit_rmse(sh.sums, ns, fit, rmse);
+  uint32_t iterations = 0;
+  bool converged = false;
+  for (int it = 0; it < max_iter; ++it) {
+    if (threadIdx.x == 0) {
+      double u[16];
+      plane_update(sh.sums, tgt.nrm != nullptr, u);
+      matmul4(u, sh.t, sh.t);
+    }
+    __syncthreads();
+    icp_pass(src, ns, tgt, r2, valid, sh, status);
+    ++iterations;
+    double nfit, nrmse;
+    fit_rmse(sh.sums, ns, nfit, nrmse);
+    converged = fabs(nfit - fit) < 1e-6 && fabs(nrmse - rmse) < 1e-6;
+    fit = nfit;
+    rmse = nrmse;
+    if (converged) break;
+  }
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 16; ++k) out->transform[k] = sh.t[k];
+    out->fitness = fit;
+    out->inlier_rmse = rmse;
+    out->correspondences = (unsigned long long)sh.sums[0];
+    out->iterations = iterations;
+    out->converged = converged ? 1u : 0u;
+  }
+  __syncthreads();
+}
+
+}  // namespace sherd

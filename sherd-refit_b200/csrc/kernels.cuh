@@ -1,0 +1,377 @@
+// kernels.cuh — the __global__ entry points of the backend.
+#pragma once
+
+#include "verify.cuh"
+
+namespace sherd {
+
+struct Pose16 {
+  double m[16];
+};
+
+// ---- Executor-shaped batch kernels (one thread per query) -------------------
+
+__global__ void k_first_hit(MeshView m, const float *org, const float *dir, uint32_t n, float *t,
+                            uint32_t *prim, uint32_t *status) {
+  uint32_t st = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    F3 o = {org[3 * i], org[3 * i + 1], org[3 * i + 2]};
+    F3 d = {dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]};
+    first_hit(m, o, d, t[i], prim[i], st);
+  }
+  if (st) atomicOr(status, st);
+}
+
+__global__ void k_bounded_all(MeshView m, const double *pts, uint32_t n, Pose16 pose, float window,
+                              double *out, uint32_t *status) {
+  uint32_t st = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double x, y, z;
+    apply_pose(pose.m, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], x, y, z);
+    float d = mesh_distance(m, {float(x), float(y), float(z)}, window, st);
+    out[i] = d == f_inf() ? d_inf() : double(d);
+  }
+  if (st) atomicOr(status, st);
+}
+
+// DistReduce::Min: every query searches with the best distance so far as its
+// window; the minimum is order-independent, so this is the CPU's scan.
+__global__ void k_bounded_min(MeshView m, const double *pts, uint32_t n, Pose16 pose,
+                              unsigned *best_key, uint32_t *status) {
+  uint32_t st = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double x, y, z;
+    apply_pose(pose.m, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], x, y, z);
+    float window = key2f(*((volatile unsigned *)best_key));
+    float d = mesh_distance(m, {float(x), float(y), float(z)}, window, st);
+    if (d != f_inf()) atomicMin(best_key, f2key(d));
+  }
+  if (st) atomicOr(status, st);
+}
+
+__global__ void k_inside(MeshView m, const double *pts, uint32_t n, Pose16 pose,
+                         sherd_inside_outcome *out, uint32_t *status) {
+  uint32_t st = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double x, y, z;
+    apply_pose(pose.m, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], x, y, z);
+    F3 p = {float(x), float(y), float(z)};
+    sherd_inside_outcome o = {0.0f, 0u};
+    bool in_box = !(p.x < m.lo[0] || p.x > m.hi[0] || p.y < m.lo[1] || p.y > m.hi[1] ||
+                    p.z < m.lo[2] || p.z > m.hi[2]);
+    if (in_box && inside_mesh(m, p, st)) o = {mesh_distance(m, p, f_inf(), st), 1u};
+    out[i] = o;
+  }
+  if (st) atomicOr(status, st);
+}
+
+__global__ void k_nn_within(CloudView c, const double *q, uint32_t n, double r2, uint32_t *idx,
+                            double *d2, uint32_t *status) {
+  uint32_t st = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double best;
+    int s = nearest_within_sq(c, q[3 * i], q[3 * i + 1], q[3 * i + 2], r2, best, st);
+    idx[i] = s < 0 ? MISS : uint32_t(c.pts[s].w);
+    d2[i] = s < 0 ? d_inf() : best;
+  }
+  if (st) atomicOr(status, st);
+}
+
+__global__ void k_nn_below(CloudView c, const double *q, uint32_t n, double bound, uint32_t *idx,
+                           double *dist, uint32_t *status) {
+  uint32_t st = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = 0.0;
+    int s = nearest_below(c, q[3 * i], q[3 * i + 1], q[3 * i + 2], bound, d, st);
+    idx[i] = s < 0 ? MISS : uint32_t(c.pts[s].w);
+    dist[i] = s < 0 ? d_inf() : d;
+  }
+  if (st) atomicOr(status, st);
+}
+
+// ---- preprocessing rays -------------------------------------------------------
+
+// mesh::geometry::face_geometry (mesh/geometry.rs:70-96).
+__global__ void k_face_geometry(const double *v, const uint32_t *f, uint32_t nf, double *normals,
+                                double *areas, double *centroids) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const double *a = v + 3 * size_t(f[3 * i]), *b = v + 3 * size_t(f[3 * i + 1]),
+               *c = v + 3 * size_t(f[3 * i + 2]);
+  double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+  double e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+  double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                 e1[0] * e2[1] - e1[1] * e2[0]};
+  double len = sqrt((n[0] * n[0] + n[1] * n[1]) + n[2] * n[2]);
+  double den = len > 1e-12 ? len : 1e-12;
+  if (normals)
+    for (int k = 0; k < 3; ++k) normals[3 * i + k] = n[k] / den;
+  if (areas) areas[i] = 0.5 * len;
+  if (centroids)
+    for (int k = 0; k < 3; ++k) centroids[3 * i + k] = (a[k] + b[k] + c[k]) / 3.0;
+}
+
+// thickness::cast_inward_rays (thickness.rs:115-132) fused with the filter of
+// thickness_from_hits (thickness.rs:139-162, looking_back 185-204): valid hit
+// distances are appended to ok[], the ones whose face looks back to far[].
+__global__ void k_thickness_rays(MeshView m, const double *centroids, const double *normals,
+                                 uint32_t nf, uint32_t stride, uint32_t n, float *t_out,
+                                 uint32_t *prim_out, float *ok, float *far, unsigned *counts,
+                                 uint32_t *status) {
+  uint32_t st = 0;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    uint32_t face = k * stride;
+    const double *c = centroids + 3 * size_t(face), *nn = normals + 3 * size_t(face);
+    double d[3] = {-nn[0], -nn[1], -nn[2]};
+    F3 o = {float(c[0] + d[0] * 1e-3), float(c[1] + d[1] * 1e-3), float(c[2] + d[2] * 1e-3)};
+    F3 dir = {float(d[0]), float(d[1]), float(d[2])};
+    float t;
+    uint32_t prim;
+    first_hit(m, o, dir, t, prim, st);
+    if (t_out) t_out[k] = t;
+    if (prim_out) prim_out[k] = prim;
+    if (!(isfinite(t) && prim < nf)) continue;
+    ok[atomicAdd(&counts[0], 1u)] = t;
+    const double *hit = normals + 3 * size_t(prim);
+    double dd = -((hit[0] * nn[0] + hit[1] * nn[1]) + hit[2] * nn[2]);
+    if (dd > 0.7) far[atomicAdd(&counts[1], 1u)] = t;
+  }
+  if (st) atomicOr(status, st);
+}
+
+// The same filter over given hits (the injected mode).
+__global__ void k_thickness_filter(const double *normals, uint32_t nf, const uint32_t *idx,
+                                   const float *t_hit, const uint32_t *prim, uint32_t n, float *ok,
+                                   float *far, unsigned *counts) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    float t = t_hit[k];
+    uint32_t p = prim[k];
+    if (!(isfinite(t) && p < nf)) continue;
+    ok[atomicAdd(&counts[0], 1u)] = t;
+    const double *hit = normals + 3 * size_t(p), *from = normals + 3 * size_t(idx[k]);
+    double dd = -((hit[0] * from[0] + hit[1] * from[1]) + hit[2] * from[2]);
+    if (dd > 0.7) far[atomicAdd(&counts[1], 1u)] = t;
+  }
+}
+
+// thickness::hist_mode (thickness.rs:212-262) over an ascending array, in one
+// block: numpy's percentile(90) interpolation in the array's dtype, 60 equal
+// bins over [0, p90] with numpy's edge corrections, the first fullest bin.
+__global__ void k_hist_mode(const float *sorted, uint32_t n, float *out) {
+  __shared__ unsigned counts[60];
+  __shared__ float edges[61];
+  __shared__ float range[2];
+  if (threadIdx.x < 60) counts[threadIdx.x] = 0;
+  if (threadIdx.x == 0) {
+    float p90;
+    if (n == 1) {
+      p90 = sorted[0];
+    } else {
+      double vi = double(n - 1) * (90.0 / 100.0);
+      double prev = floor(vi);
+      uint32_t i = uint32_t(prev);
+      double gamma = vi - prev;
+      float a = sorted[i], b = sorted[i + 1 < n ? i + 1 : n - 1];
+      float diff = b - a;
+      p90 = gamma >= 0.5 ? b - diff * float(1.0 - gamma) : a + diff * float(gamma);
+    }
+    float first = 0.0f, last = p90;
+    if (p90 == 0.0f) {
+      first = -0.5f;
+      last = 0.5f;
+    }
+    float step = (last - first) / 60.0f;
+    for (int k = 0; k <= 60; ++k) edges[k] = float(k) * step + first;
+    edges[60] = last;
+    range[0] = first;
+    range[1] = last;
+  }
+  __syncthreads();
+  float first = range[0], last = range[1], denom = last - first;
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    float v = sorted[j];
+    if (!(v >= first && v <= last)) continue;
+    unsigned i = unsigned(((v - first) / denom) * 60.0f);
+    if (i == 60u) i -= 1;
+    if (v < edges[i]) i -= 1;
+    if (i != 59u && v >= edges[i + 1]) i += 1;
+    atomicAdd(&counts[i], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int k = 0;
+    for (int i = 1; i < 60; ++i)
+      if (counts[i] > counts[k]) k = i;
+    *out = 0.5f * (edges[k] + edges[k + 1]);
+  }
+}
+
+struct ConeConsts {
+  double cos_a, sin_a;
+  double cp[6], sp[6];
+};
+
+// segment::classify_faces (segment.rs:318-376): seven rays per face.
+__global__ void k_cone_votes(MeshView m, const double *centroids, const double *normals,
+                             const double *ns, const double *hit_normals, uint32_t nf, double thick,
+                             ConeConsts cc, uint8_t *good, uint32_t *status) {
+  uint32_t st = 0;
+  float min_hit = float(0.1 * thick);
+  float thick_f = float(thick);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x) {
+    const double *n = ns + 3 * size_t(i), *fnv = normals + 3 * size_t(i),
+                 *c = centroids + 3 * size_t(i);
+    uint8_t g = 0;
+    bool finite = isfinite(n[0]) && isfinite(n[1]) && isfinite(n[2]);
+    double a[3] = {1.0, 0.0, 0.0};
+    if (!(fabs(n[0]) < 0.9)) {
+      a[0] = 0.0;
+      a[1] = 1.0;
+    }
+    double cr[3] = {n[1] * a[2] - n[2] * a[1], n[2] * a[0] - n[0] * a[2],
+                    n[0] * a[1] - n[1] * a[0]};
+    double len = sqrt((cr[0] * cr[0] + cr[1] * cr[1]) + cr[2] * cr[2]);
+    if (finite && len > 0.0) {
+      double e1[3] = {cr[0] / len, cr[1] / len, cr[2] / len};
+      double e2[3] = {n[1] * e1[2] - n[2] * e1[1], n[2] * e1[0] - n[0] * e1[2],
+                      n[0] * e1[1] - n[1] * e1[0]};
+      F3 o = {float(c[0] - fnv[0] * 1e-3), float(c[1] - fnv[1] * 1e-3),
+              float(c[2] - fnv[2] * 1e-3)};
+      for (int k = 0; k < 7; ++k) {
+        double d[3];
+        if (k == 0) {
+          d[0] = -n[0];
+          d[1] = -n[1];
+          d[2] = -n[2];
+        } else {
+          double cp = cc.cp[k - 1], sp = cc.sp[k - 1];
+          for (int q = 0; q < 3; ++q) d[q] = -(cc.cos_a * n[q]) + cc.sin_a * (cp * e1[q] + sp * e2[q]);
+        }
+        F3 dir = {float(d[0]), float(d[1]), float(d[2])};
+        float dh;
+        uint32_t prim;
+        first_hit(m, o, dir, dh, prim, st);
+        if (prim == MISS) continue;
+        if (!isfinite(dh) || prim >= nf || dh <= min_hit) continue;
+        float ratio = dh / thick_f;
+        if (ratio <= 0.5f || ratio >= 1.8f) continue;
+        const double *h = hit_normals + 3 * size_t(prim);
+        double al = (h[0] * d[0] + h[1] * d[1]) + h[2] * d[2];
+        if (al > 0.7) ++g;
+      }
+    }
+    good[i] = g;
+  }
+  if (st) atomicOr(status, st);
+}
+
+// ---- ICP -----------------------------------------------------------------------
+
+// Executor::icp_rung: one block per candidate.
+__global__ void __launch_bounds__(ICP_BLOCK) k_icp_rung(const double4 *src, uint32_t ns,
+                                                        CloudView tgt, const double *inits,
+                                                        sherd_icp_options opt,
+                                                        sherd_registration *out, uint32_t *status) {
+  __shared__ IcpShared sh;
+  uint32_t st = 0;
+  if (threadIdx.x < 16) sh.t[threadIdx.x] = inits[16 * blockIdx.x + threadIdx.x];
+  __syncthreads();
+  icp_rung_block(src, ns, tgt, opt.max_correspondence_distance, opt.max_iteration, sh,
+                 out + blockIdx.x, st);
+  if (st) atomicOr(status, st);
+}
+
+// ---- the batched stage-2 path ----------------------------------------------------
+
+struct QueueCtl {
+  unsigned *head;             // next queue position to take
+  const uint32_t *order;      // item indices, most expensive first
+  uint32_t n;                 // queue length
+  const uint32_t *abort_flag; // host-mapped; non-zero asks the kernel to stop
+  unsigned long long budget_ns;
+};
+
+// Takes the next queue entry for the whole block, or returns false when the
+// queue is empty, the host asked to stop or the time budget is spent.
+__device__ __forceinline__ bool take(const QueueCtl &q, unsigned long long start, unsigned &slot,
+                                     uint32_t &st) {
+  __shared__ unsigned s_item;
+  if (threadIdx.x == 0) {
+    unsigned item = 0xFFFFFFFFu;
+    if (q.abort_flag && *((volatile const uint32_t *)q.abort_flag)) {
+      st |= ST_ABORTED;
+    } else if (q.budget_ns && global_ns() - start > q.budget_ns) {
+      st |= ST_TIMEOUT;
+    } else {
+      unsigned pos = atomicAdd(q.head, 1u);
+      if (pos < q.n) item = q.order[pos];
+    }
+    s_item = item;
+  }
+  __syncthreads();
+  slot = s_item;
+  __syncthreads();
+  return slot != 0xFFFFFFFFu;
+}
+
+// R 5.6's four point-to-plane rungs per (pair, start) (ladder.rs:142-161).
+__global__ void __launch_bounds__(ICP_BLOCK) k_ladder(const PairView *pairs,
+                                                      const sherd_work_item *items, QueueCtl q,
+                                                      sherd_candidate *out, uint32_t *status) {
+  __shared__ IcpShared sh;
+  uint32_t st = 0;
+  unsigned long long start = global_ns();
+  unsigned it;
+  while (take(q, start, it, st)) {
+    const sherd_work_item &w = items[it];
+    const PairView &pr = pairs[w.pair];
+    sherd_candidate *c = out + it;
+    if (threadIdx.x < 16) sh.t[threadIdx.x] = w.init[threadIdx.x];
+    if (threadIdx.x == 0) {
+      c->pair = w.pair;
+      c->start = w.start;
+    }
+    __syncthreads();
+    const double k[4] = {0.2, 0.08, 0.08, 0.04};
+    for (int r = 0; r < 4; ++r) {
+      double distance = k[r] * pr.sc.t * pr.sc.icp;
+      if (r < 2)
+        icp_rung_block(pr.reg_src, pr.n_reg, pr.reg_tgt, distance, 30, sh, &c->rungs[r], st);
+      else
+        icp_rung_block(pr.frac_src, pr.n_frac, pr.frac_tgt, distance, 30, sh, &c->rungs[r], st);
+    }
+  }
+  if (threadIdx.x == 0 && st) atomicOr(status, st);
+}
+
+// R 6 + R 6.5 at each item's last rung pose (verify.rs:590-638).
+__global__ void __launch_bounds__(VER_BLOCK) k_verify_items(const PairView *pairs,
+                                                            const sherd_work_item *items,
+                                                            QueueCtl q, sherd_params p,
+                                                            unsigned *scratch, size_t stride,
+                                                            sherd_candidate *out, int full,
+                                                            uint32_t *status) {
+  __shared__ VerShared sh;
+  uint32_t st = 0;
+  unsigned long long start = global_ns();
+  unsigned *mine = scratch + stride * blockIdx.x;
+  unsigned it;
+  while (take(q, start, it, st)) {
+    const PairView &pr = pairs[items[it].pair];
+    sherd_candidate *c = out + it;
+    if (threadIdx.x < 16) sh.t[threadIdx.x] = c->rungs[3].transform[threadIdx.x];
+    __syncthreads();
+    if (pr.scratch_floats > stride) {
+      if (threadIdx.x == 0) {
+        st |= ST_SCRATCH;
+        c->status = uint32_t(-SHERD_E_INVALID);
+      }
+      __syncthreads();
+      continue;
+    }
+    verify_block(pr, full != 0, p, mine, sh, &c->scores, &c->accepted, st);
+  }
+  if (st) atomicOr(status, st);
+}
+
+}  // namespace sherd

@@ -1,0 +1,330 @@
+// lbvh.cuh — device-built linear BVH (Karras 2012) over triangles or points.
+//
+// Build: 63-bit Morton codes of the primitive centres over the scene box, a
+// CUB radix sort of (code, primitive) pairs, the Karras hierarchy over the
+// sorted codes (equal codes split by index), a bottom-up box refit with one
+// atomic arrival counter per node, and a final pass that writes the compact
+// traversal layout:
+//
+//   BNode (64 B, four 16-byte loads): both children's boxes, already padded
+//   outward, and for each child either an internal node index or a leaf range
+//   (first, count) of consecutive sorted primitives. A Karras subtree holding
+//   at most TRI_LEAF / POINT_LEAF primitives is a leaf range, so leaves hold
+//   several primitives without a separate collapse pass.
+//
+// Primitives are stored in sorted (leaf) order next to their original index,
+// so a leaf is one contiguous, coalesced run of memory.
+#pragma once
+
+#include "common.cuh"
+
+namespace sherd {
+
+struct __align__(16) BNode {
+  float4 a;  // lo0.x lo0.y lo0.z hi0.x
+  float4 b;  // hi0.y hi0.z lo1.x lo1.y
+  float4 c;  // lo1.z hi1.x hi1.y hi1.z
+  int4 d;    // ref0 ref1 cnt0 cnt1  (cnt > 0: leaf range at ref; cnt == 0: node ref)
+};
+
+// What the traversal kernels take by value.
+struct MeshView {
+  const BNode *nodes;
+  const float4 *tri;  // 3 per sorted slot: (v0, original face id bits), (v1, 0), (v2, 0)
+  uint32_t nf;
+  uint32_t root_leaf;  // nf when the whole mesh is one leaf, else 0
+  float pad;           // outward padding of every node box
+  float lo[3], hi[3];  // exact vertex box (RayScene::aabb)
+};
+
+struct CloudView {
+  const BNode *nodes;
+  const double4 *pts;  // sorted: (x, y, z, original index)
+  const double4 *nrm;  // sorted unit normals (x, y, z, 0), or null
+  uint32_t n;
+  uint32_t root_leaf;
+  float pad;
+};
+
+// ---- Morton codes -----------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long expand21(unsigned v) {
+  unsigned long long x = v & 0x1fffffu;
+  x = (x | x << 32) & 0x1f00000000ffffULL;
+  x = (x | x << 16) & 0x1f0000ff0000ffULL;
+  x = (x | x << 8) & 0x100f00f00f00f00fULL;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+  x = (x | x << 2) & 0x1249249249249249ULL;
+  return x;
+}
+
+__device__ __forceinline__ unsigned quant21(double c, double lo, double inv_ext) {
+  double u = (c - lo) * inv_ext;
+  u = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
+  unsigned q = unsigned(u * 2097151.0);
+  return q > 2097151u ? 2097151u : q;
+}
+
+__device__ __forceinline__ unsigned long long morton3(double x, double y, double z,
+                                                      const double *lo, const double *inv) {
+  return (expand21(quant21(x, lo[0], inv[0])) << 2) | (expand21(quant21(y, lo[1], inv[1])) << 1) |
+         expand21(quant21(z, lo[2], inv[2]));
+}
+
+// Order-preserving float -> uint, for atomic min/max of signed floats.
+__device__ __forceinline__ unsigned ford(float x) {
+  unsigned b = __float_as_uint(x);
+  return (b >> 31) ? ~b : (b | 0x80000000u);
+}
+__host__ __device__ inline float fordinv(unsigned k) {
+  unsigned b = (k >> 31) ? (k & 0x7fffffffu) : ~k;
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+}
+
+// Scene box of f32 vertices: bounds[0..2] = ford(min), bounds[3..5] = ford(max).
+__global__ void k_bounds_f32(const float *v, uint32_t nv, unsigned *bounds) {
+  float lo[3] = {f_inf(), f_inf(), f_inf()}, hi[3] = {-f_inf(), -f_inf(), -f_inf()};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
+    for (int k = 0; k < 3; ++k) {
+      float x = v[3 * i + k];
+      lo[k] = fminf(lo[k], x);
+      hi[k] = fmaxf(hi[k], x);
+    }
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o; o >>= 1) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&bounds[k], ford(lo[k]));
+      atomicMax(&bounds[3 + k], ford(hi[k]));
+    }
+  }
+}
+
+// Scene box of f64 points, rounded outward to f32.
+__global__ void k_bounds_f64(const double *p, uint32_t n, unsigned *bounds) {
+  float lo[3] = {f_inf(), f_inf(), f_inf()}, hi[3] = {-f_inf(), -f_inf(), -f_inf()};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int k = 0; k < 3; ++k) {
+      double x = p[3 * i + k];
+      lo[k] = fminf(lo[k], __double2float_rd(x));
+      hi[k] = fmaxf(hi[k], __double2float_ru(x));
+    }
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o; o >>= 1) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&bounds[k], ford(lo[k]));
+      atomicMax(&bounds[3 + k], ford(hi[k]));
+    }
+  }
+}
+
+struct BuildBox {
+  double lo[3], inv[3];
+};
+
+__global__ void k_morton_tri(const float *v, const uint32_t *f, uint32_t nf, BuildBox box,
+                             unsigned long long *keys, uint32_t *vals) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  double c[3];
+  for (int k = 0; k < 3; ++k)
+    c[k] = (double(v[3 * f[3 * i] + k]) + double(v[3 * f[3 * i + 1] + k]) +
+            double(v[3 * f[3 * i + 2] + k])) / 3.0;
+  keys[i] = morton3(c[0], c[1], c[2], box.lo, box.inv);
+  vals[i] = i;
+}
+
+__global__ void k_morton_pts(const double *p, uint32_t n, BuildBox box, unsigned long long *keys,
+                             uint32_t *vals) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = morton3(p[3 * i], p[3 * i + 1], p[3 * i + 2], box.lo, box.inv);
+  vals[i] = i;
+}
+
+// ---- Karras hierarchy -------------------------------------------------------
+
+__device__ __forceinline__ int kdelta(const unsigned long long *keys, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  unsigned long long a = keys[i], b = keys[j];
+  if (a == b) return 64 + __clz(unsigned(i) ^ unsigned(j));
+  return __clzll(a ^ b);
+}
+
+// Internal node i of n-1: children (leaf primitive k encoded as k | 0x80000000),
+// the primitive range it covers and the parent links.
+__global__ void k_karras(const unsigned long long *keys, int n, int *left, int *right, int *first,
+                         int *last, int *parent_int, int *parent_leaf) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  int d = (kdelta(keys, n, i, i + 1) - kdelta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+  int dmin = kdelta(keys, n, i, i - d);
+  int lmax = 2;
+  while (kdelta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (kdelta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+  int j = i + l * d;
+  int dnode = kdelta(keys, n, i, j);
+  int s = 0;
+  for (int div = 2;; div <<= 1) {
+    int t = (l + div - 1) / div;
+    if (kdelta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    if (t <= 1) break;
+  }
+  int gamma = i + s * d + (d < 0 ? -1 : 0);
+  int lo = i < j ? i : j, hi = i < j ? j : i;
+  first[i] = lo;
+  last[i] = hi;
+  if (lo == gamma) {
+    left[i] = gamma | int(0x80000000);
+    parent_leaf[gamma] = i;
+  } else {
+    left[i] = gamma;
+    parent_int[gamma] = i;
+  }
+  if (hi == gamma + 1) {
+    right[i] = (gamma + 1) | int(0x80000000);
+    parent_leaf[gamma + 1] = i;
+  } else {
+    right[i] = gamma + 1;
+    parent_int[gamma + 1] = i;
+  }
+}
+
+struct Box {
+  float lo[3], hi[3];
+};
+
+__device__ __forceinline__ Box tri_box(const float *v, const uint32_t *f, uint32_t face) {
+  Box b;
+  for (int k = 0; k < 3; ++k) {
+    float a0 = v[3 * f[3 * face] + k], a1 = v[3 * f[3 * face + 1] + k], a2 = v[3 * f[3 * face + 2] + k];
+    b.lo[k] = fminf(a0, fminf(a1, a2));
+    b.hi[k] = fmaxf(a0, fmaxf(a1, a2));
+  }
+  return b;
+}
+
+__device__ __forceinline__ Box pt_box(const double *p, uint32_t i) {
+  Box b;
+  for (int k = 0; k < 3; ++k) {
+    b.lo[k] = __double2float_rd(p[3 * i + k]);
+    b.hi[k] = __double2float_ru(p[3 * i + k]);
+  }
+  return b;
+}
+
+template <bool TRI>
+__device__ __forceinline__ Box prim_box(const float *v, const uint32_t *f, const double *p,
+                                        const uint32_t *sorted, int k) {
+  return TRI ? tri_box(v, f, sorted[k]) : pt_box(p, sorted[k]);
+}
+
+__device__ __forceinline__ Box load_box(const float *ib, int node) {
+  Box b;
+  for (int k = 0; k < 3; ++k) {
+    b.lo[k] = __ldcg(ib + 6 * node + k);
+    b.hi[k] = __ldcg(ib + 6 * node + 3 + k);
+  }
+  return b;
+}
+
+// Bottom-up refit: one thread per primitive walks to the root; the second
+// thread to reach a node computes its box.
+template <bool TRI>
+__global__ void k_refit(const float *v, const uint32_t *f, const double *p, const uint32_t *sorted,
+                        int n, const int *left, const int *right, const int *parent_int,
+                        const int *parent_leaf, unsigned *flags, float *ibox) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int node = parent_leaf[k];
+  for (int steps = 0; node >= 0 && steps < 256; ++steps) {
+    __threadfence();
+    if (atomicAdd(&flags[node], 1u) == 0u) return;
+    __threadfence();
+    Box out;
+    for (int c = 0; c < 2; ++c) {
+      int ref = c == 0 ? left[node] : right[node];
+      Box b = ref < 0 ? prim_box<TRI>(v, f, p, sorted, ref & 0x7fffffff) : load_box(ibox, ref);
+      for (int a = 0; a < 3; ++a) {
+        out.lo[a] = c == 0 ? b.lo[a] : fminf(out.lo[a], b.lo[a]);
+        out.hi[a] = c == 0 ? b.hi[a] : fmaxf(out.hi[a], b.hi[a]);
+      }
+    }
+    for (int a = 0; a < 3; ++a) {
+      __stcg(ibox + 6 * node + a, out.lo[a]);
+      __stcg(ibox + 6 * node + 3 + a, out.hi[a]);
+    }
+    node = parent_int[node];
+  }
+}
+
+// The traversal layout, one BNode per internal node, boxes padded outward.
+template <bool TRI>
+__global__ void k_emit(const float *v, const uint32_t *f, const double *p, const uint32_t *sorted,
+                       int n, const int *left, const int *right, const int *first, const int *last,
+                       const float *ibox, float pad, int leaf_max, BNode *nodes) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  Box bx[2];
+  int ref[2], cnt[2];
+  for (int c = 0; c < 2; ++c) {
+    int r = c == 0 ? left[i] : right[i];
+    if (r < 0) {
+      int k = r & 0x7fffffff;
+      bx[c] = prim_box<TRI>(v, f, p, sorted, k);
+      ref[c] = k;
+      cnt[c] = 1;
+    } else {
+      bx[c] = load_box(ibox, r);
+      int size = last[r] - first[r] + 1;
+      if (size <= leaf_max) {
+        ref[c] = first[r];
+        cnt[c] = size;
+      } else {
+        ref[c] = r;
+        cnt[c] = 0;
+      }
+    }
+    for (int a = 0; a < 3; ++a) {
+      bx[c].lo[a] = __fsub_rd(bx[c].lo[a], pad);
+      bx[c].hi[a] = __fadd_ru(bx[c].hi[a], pad);
+    }
+  }
+  BNode nd;
+  nd.a = make_float4(bx[0].lo[0], bx[0].lo[1], bx[0].lo[2], bx[0].hi[0]);
+  nd.b = make_float4(bx[0].hi[1], bx[0].hi[2], bx[1].lo[0], bx[1].lo[1]);
+  nd.c = make_float4(bx[1].lo[2], bx[1].hi[0], bx[1].hi[1], bx[1].hi[2]);
+  nd.d = make_int4(ref[0], ref[1], cnt[0], cnt[1]);
+  nodes[i] = nd;
+}
+
+__global__ void k_store_tris(const float *v, const uint32_t *f, const uint32_t *sorted, uint32_t nf,
+                             float4 *tri) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nf) return;
+  uint32_t face = sorted[s];
+  const float *a = v + 3 * f[3 * face], *b = v + 3 * f[3 * face + 1], *c = v + 3 * f[3 * face + 2];
+  tri[3 * s] = make_float4(a[0], a[1], a[2], __uint_as_float(face));
+  tri[3 * s + 1] = make_float4(b[0], b[1], b[2], 0.0f);
+  tri[3 * s + 2] = make_float4(c[0], c[1], c[2], 0.0f);
+}
+
+__global__ void k_store_pts(const double *p, const double *nrm, const uint32_t *sorted, uint32_t n,
+                            double4 *pts, double4 *nout) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t i = sorted[s];
+  pts[s] = make_double4(p[3 * i], p[3 * i + 1], p[3 * i + 2], double(i));
+  if (nrm) nout[s] = make_double4(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2], 0.0);
+}
+
+}  // namespace sherd

@@ -1,0 +1,1206 @@
+// sherd.cu — the C ABI of the B200 geometry backend (include/sherd_cuda.h).
+//
+// One translation unit: the device code lives in the headers it includes.
+// Host responsibilities: the context (device, stream, lock, status word,
+// host-mapped abort flag, statistics), device handles for meshes, clouds,
+// surfaces and pairs (each built on the device: LBVHs, sorted primitives),
+// argument checking, and the launch sequences. No entry point computes a
+// result on the host; a CUDA failure is an error status, never a fallback.
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "kernels.cuh"
+
+using namespace sherd;
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+
+struct MethodStats {
+  uint64_t calls = 0, items = 0;
+  double ms = 0.0;
+};
+
+struct sherd_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::mutex mu;
+  uint32_t timeout_ms = 0;
+  uint32_t *abort_host = nullptr;  // pinned, mapped
+  uint32_t *abort_dev = nullptr;
+  uint32_t *d_status = nullptr;
+  std::map<std::string, MethodStats> stats;
+};
+
+namespace {
+
+thread_local std::map<const sherd_ctx *, std::string> t_errors;
+
+int fail(const sherd_ctx *ctx, int code, const std::string &msg) {
+  t_errors[ctx] = msg;
+  return code;
+}
+
+int cuda_fail(const sherd_ctx *ctx, cudaError_t e, const char *what) {
+  int code = e == cudaErrorMemoryAllocation ? SHERD_E_OOM : SHERD_E_DEVICE;
+  cudaGetLastError();
+  return fail(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                          \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+template <typename T>
+struct DBuf {  // owning device buffer
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    reset();
+    n = count;
+    if (!count) return cudaSuccess;
+    return cudaMalloc(&p, count * sizeof(T));
+  }
+};
+
+unsigned blocks_for(size_t n, int threads = 256) {
+  size_t b = (n + threads - 1) / threads;
+  return unsigned(std::max<size_t>(1, std::min<size_t>(b, 1u << 30)));
+}
+
+bool finite_pose(const double *t) {
+  if (!t) return false;
+  for (int i = 0; i < 16; ++i)
+    if (!std::isfinite(t[i])) return false;
+  return true;
+}
+
+Pose16 pose_of(const double *t) {
+  Pose16 p;
+  std::memcpy(p.m, t, sizeof p.m);
+  return p;
+}
+
+// Runs the status check after a launch sequence: synchronises the stream and
+// turns the kernels' status bits into an error code.
+int finish(sherd_ctx *ctx, const char *method, size_t items, bool timed) {
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+  uint32_t st = 0;
+  CK(cudaMemcpy(&st, ctx->d_status, 4, cudaMemcpyDeviceToHost));
+  MethodStats &m = ctx->stats[method];
+  m.calls += 1;
+  m.items += items;
+  if (timed) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) m.ms += ms;
+  }
+  if (st & ST_ABORTED) return fail(ctx, SHERD_E_ABORTED, std::string(method) + ": aborted");
+  if (st & ST_TIMEOUT) return fail(ctx, SHERD_E_TIMEOUT, std::string(method) + ": time budget spent");
+  if (st & ST_STACK) return fail(ctx, SHERD_E_DEVICE, std::string(method) + ": traversal stack overflow");
+  if (st & ST_SCRATCH) return fail(ctx, SHERD_E_INVALID, std::string(method) + ": scratch too small");
+  return SHERD_OK;
+}
+
+int begin(sherd_ctx *ctx) {
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  return SHERD_OK;
+}
+
+template <typename T>
+int upload(sherd_ctx *ctx, DBuf<T> &buf, const T *host, size_t n) {
+  CK(buf.alloc(n));
+  if (n) CK(cudaMemcpyAsync(buf.p, host, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  return SHERD_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// handles
+// ---------------------------------------------------------------------------
+
+struct sherd_mesh {
+  sherd_ctx *ctx = nullptr;
+  std::vector<float> hv;     // host copy of the vertices (subsets reuse them)
+  std::vector<uint32_t> hf;  // host copy of the faces
+  DBuf<BNode> nodes;
+  DBuf<float4> tri;
+  MeshView view{};
+};
+
+struct sherd_cloud {
+  sherd_ctx *ctx = nullptr;
+  DBuf<BNode> nodes;
+  DBuf<double4> pts, nrm;
+  CloudView view{};
+};
+
+struct sherd_surfaces {
+  sherd_ctx *ctx = nullptr;
+  const sherd_mesh *fracture = nullptr, *mesh = nullptr;
+  std::vector<double> brk_p_host;
+  DBuf<double> pf, s, brk_p, brk_ns, margin_p, margin_n;
+  sherd_cloud brk_tree, margin_tree;
+  bool has_brk_tree = false, has_margin_tree = false;
+  SurfView view{};
+};
+
+struct sherd_pair {
+  sherd_ctx *ctx = nullptr;
+  const sherd_surfaces *a = nullptr, *b = nullptr;
+  sherd_cloud reg_src, frac_src;
+  DBuf<uint32_t> a_cell;
+  PairView view{};
+};
+
+namespace {
+
+// Builds the LBVH over f32 triangles (TRI) or f64 points (!TRI) already on the
+// device; fills nodes, the sorted slot order and the root description.
+template <bool TRI>
+int build_lbvh(sherd_ctx *ctx, const float *d_v, uint32_t nv, const uint32_t *d_f, const double *d_p,
+               uint32_t n, float pad, int leaf_max, DBuf<BNode> &nodes, DBuf<uint32_t> &sorted,
+               float lo[3], float hi[3]) {
+  cudaStream_t s = ctx->stream;
+  DBuf<unsigned> bounds;
+  CK(bounds.alloc(6));
+  unsigned init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+  CK(cudaMemcpyAsync(bounds.p, init, sizeof init, cudaMemcpyHostToDevice, s));
+  if (TRI)
+    k_bounds_f32<<<std::min(blocks_for(nv), 1024u), 256, 0, s>>>(d_v, nv, bounds.p);
+  else
+    k_bounds_f64<<<std::min(blocks_for(n), 1024u), 256, 0, s>>>(d_p, n, bounds.p);
+  CK(cudaGetLastError());
+  unsigned hb[6];
+  CK(cudaMemcpyAsync(hb, bounds.p, sizeof hb, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  BuildBox box;
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = fordinv(hb[k]);
+    hi[k] = fordinv(hb[3 + k]);
+    box.lo[k] = lo[k];
+    double ext = double(hi[k]) - double(lo[k]);
+    box.inv[k] = ext > 0.0 ? 1.0 / ext : 0.0;
+  }
+  DBuf<unsigned long long> keys, keys2;
+  DBuf<uint32_t> vals;
+  CK(keys.alloc(n));
+  CK(keys2.alloc(n));
+  CK(vals.alloc(n));
+  CK(sorted.alloc(n));
+  if (TRI)
+    k_morton_tri<<<blocks_for(n), 256, 0, s>>>(d_v, d_f, n, box, keys.p, vals.p);
+  else
+    k_morton_pts<<<blocks_for(n), 256, 0, s>>>(d_p, n, box, keys.p, vals.p);
+  CK(cudaGetLastError());
+  size_t temp_bytes = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys.p, keys2.p, vals.p, sorted.p,
+                                     int(n), 0, 63, s));
+  DBuf<unsigned char> temp;
+  CK(temp.alloc(temp_bytes));
+  CK(cub::DeviceRadixSort::SortPairs(temp.p, temp_bytes, keys.p, keys2.p, vals.p, sorted.p, int(n),
+                                     0, 63, s));
+  if (int(n) <= leaf_max) {
+    nodes.reset();
+    CK(cudaStreamSynchronize(s));
+    return SHERD_OK;
+  }
+  int ni = int(n) - 1;
+  DBuf<int> left, right, first, last, pint, pleaf;
+  DBuf<unsigned> flags;
+  DBuf<float> ibox;
+  CK(left.alloc(ni));
+  CK(right.alloc(ni));
+  CK(first.alloc(ni));
+  CK(last.alloc(ni));
+  CK(pint.alloc(ni));
+  CK(pleaf.alloc(n));
+  CK(flags.alloc(ni));
+  CK(ibox.alloc(size_t(6) * ni));
+  CK(nodes.alloc(ni));
+  CK(cudaMemsetAsync(flags.p, 0, sizeof(unsigned) * ni, s));
+  CK(cudaMemsetAsync(pint.p, 0xFF, sizeof(int) * ni, s));  // root's parent is -1
+  k_karras<<<blocks_for(ni), 256, 0, s>>>(keys2.p, int(n), left.p, right.p, first.p, last.p, pint.p,
+                                          pleaf.p);
+  CK(cudaGetLastError());
+  k_refit<TRI><<<blocks_for(n), 256, 0, s>>>(d_v, d_f, d_p, sorted.p, int(n), left.p, right.p,
+                                             pint.p, pleaf.p, flags.p, ibox.p);
+  CK(cudaGetLastError());
+  k_emit<TRI><<<blocks_for(ni), 256, 0, s>>>(d_v, d_f, d_p, sorted.p, int(n), left.p, right.p,
+                                             first.p, last.p, ibox.p, pad, leaf_max, nodes.p);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  return SHERD_OK;
+}
+
+int mesh_build(sherd_ctx *ctx, sherd_mesh *m) {
+  uint32_t nv = uint32_t(m->hv.size() / 3), nf = uint32_t(m->hf.size() / 3);
+  DBuf<float> dv;
+  DBuf<uint32_t> df, sorted;
+  int rc = upload(ctx, dv, m->hv.data(), m->hv.size());
+  if (rc) return rc;
+  rc = upload(ctx, df, m->hf.data(), m->hf.size());
+  if (rc) return rc;
+  double mag = 1.0;
+  for (float x : m->hv) mag = std::max(mag, double(std::fabs(x)));
+  float pad = float(1e-5 * mag);
+  float lo[3], hi[3];
+  rc = build_lbvh<true>(ctx, dv.p, nv, df.p, nullptr, nf, pad, TRI_LEAF, m->nodes, sorted, lo, hi);
+  if (rc) return rc;
+  CK(m->tri.alloc(size_t(3) * nf));
+  k_store_tris<<<blocks_for(nf), 256, 0, ctx->stream>>>(dv.p, df.p, sorted.p, nf, m->tri.p);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  // The exact vertex box of RayScene::aabb (bvh.rs:182-185).
+  float vlo[3] = {f_inf(), f_inf(), f_inf()}, vhi[3] = {-f_inf(), -f_inf(), -f_inf()};
+  for (uint32_t i = 0; i < nv; ++i)
+    for (int k = 0; k < 3; ++k) {
+      vlo[k] = std::min(vlo[k], m->hv[3 * i + k]);
+      vhi[k] = std::max(vhi[k], m->hv[3 * i + k]);
+    }
+  MeshView &v = m->view;
+  v.nodes = m->nodes.p;
+  v.tri = m->tri.p;
+  v.nf = nf;
+  v.root_leaf = nf <= uint32_t(TRI_LEAF) ? nf : 0;
+  v.pad = pad;
+  for (int k = 0; k < 3; ++k) {
+    v.lo[k] = vlo[k];
+    v.hi[k] = vhi[k];
+  }
+  return SHERD_OK;
+}
+
+int cloud_build(sherd_ctx *ctx, const double *p, const double *nrm, uint32_t np, sherd_cloud *c) {
+  DBuf<double> dp, dn;
+  DBuf<uint32_t> sorted;
+  int rc = upload(ctx, dp, p, size_t(3) * np);
+  if (rc) return rc;
+  if (nrm) {
+    rc = upload(ctx, dn, nrm, size_t(3) * np);
+    if (rc) return rc;
+  }
+  double mag = 1.0;
+  for (size_t i = 0; i < size_t(3) * np; ++i) mag = std::max(mag, std::fabs(p[i]));
+  float pad = float(1e-6 * mag);
+  float lo[3], hi[3];
+  rc = build_lbvh<false>(ctx, nullptr, 0, nullptr, dp.p, np, pad, POINT_LEAF, c->nodes, sorted, lo,
+                         hi);
+  if (rc) return rc;
+  CK(c->pts.alloc(np));
+  if (nrm) CK(c->nrm.alloc(np));
+  k_store_pts<<<blocks_for(np), 256, 0, ctx->stream>>>(dp.p, nrm ? dn.p : nullptr, sorted.p, np,
+                                                       c->pts.p, nrm ? c->nrm.p : nullptr);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  c->ctx = ctx;
+  CloudView &v = c->view;
+  v.nodes = c->nodes.p;
+  v.pts = c->pts.p;
+  v.nrm = nrm ? c->nrm.p : nullptr;
+  v.n = np;
+  v.root_leaf = np <= uint32_t(POINT_LEAF) ? np : 0;
+  v.pad = pad;
+  return SHERD_OK;
+}
+
+bool has_nan(const double *p, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (std::isnan(p[i])) return true;
+  return false;
+}
+
+// The dense ids of R 6.2's voxels floor(A.brk_p / (t/3)) (verify.rs:400-414,
+// 809-811): equal voxels share an id, so the device counts distinct ids.
+int seam_cells(sherd_ctx *ctx, const std::vector<double> &brk, double t, DBuf<uint32_t> &out,
+               uint32_t &n_cells) {
+  size_t n = brk.size() / 3;
+  double voxel = t / 3.0;
+  std::vector<std::array<int64_t, 3>> cells(n);
+  for (size_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) cells[i][k] = int64_t(std::floor(brk[3 * i + k] / voxel));
+  std::vector<std::array<int64_t, 3>> uniq = cells;
+  std::sort(uniq.begin(), uniq.end());
+  uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+  std::vector<uint32_t> ids(n);
+  for (size_t i = 0; i < n; ++i)
+    ids[i] = uint32_t(std::lower_bound(uniq.begin(), uniq.end(), cells[i]) - uniq.begin());
+  n_cells = uint32_t(uniq.size());
+  if (n_cells > uint32_t(MAX_CELL_WORDS) * 32u)
+    return fail(ctx, SHERD_E_INVALID, "breakline spans more than 65536 seam voxels");
+  return upload(ctx, out, ids.data(), n);
+}
+
+// Per-item scratch in 4-byte words, a multiple of 64 so that every CTA's slot
+// (and the 8-byte keys of the continuity medians) stays 256-byte aligned.
+uint32_t scratch_words(const PairView &v) {
+  uint32_t w = std::max<uint32_t>({v.a.n_pf, v.b.n_pf, 4u * v.b.n_margin, 1u});
+  return (w + 63u) / 64u * 64u;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *sherd_name(void) { return "cuda"; }
+
+int sherd_open(int device, sherd_ctx **out) {
+  if (!out) return SHERD_E_INVALID;
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || device < 0 || device >= count) {
+    cudaGetLastError();
+    t_errors[nullptr] = "no such CUDA device";
+    return SHERD_E_DEVICE;
+  }
+  sherd_ctx *ctx = new sherd_ctx;
+  ctx->device = device;
+  auto bad = [&](cudaError_t err) {
+    t_errors[nullptr] = cudaGetErrorString(err);
+    delete ctx;
+    return SHERD_E_DEVICE;
+  };
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return bad(e);
+  if ((e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device)) !=
+      cudaSuccess)
+    return bad(e);
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bad(e);
+  if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess) return bad(e);
+  if ((e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) return bad(e);
+  if ((e = cudaHostAlloc(&ctx->abort_host, 4, cudaHostAllocMapped)) != cudaSuccess) return bad(e);
+  *ctx->abort_host = 0;
+  if ((e = cudaHostGetDevicePointer(&ctx->abort_dev, ctx->abort_host, 0)) != cudaSuccess) return bad(e);
+  if ((e = cudaMalloc(&ctx->d_status, 4)) != cudaSuccess) return bad(e);
+  *out = ctx;
+  return SHERD_OK;
+}
+
+int sherd_close(sherd_ctx *ctx) {
+  if (!ctx) return SHERD_E_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->abort_host) cudaFreeHost(ctx->abort_host);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  t_errors.erase(ctx);
+  delete ctx;
+  return SHERD_OK;
+}
+
+const char *sherd_last_error(const sherd_ctx *ctx) {
+  auto it = t_errors.find(ctx);
+  return it == t_errors.end() ? "" : it->second.c_str();
+}
+
+int sherd_set_timeout_ms(sherd_ctx *ctx, uint32_t ms) {
+  if (!ctx) return SHERD_E_INVALID;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->timeout_ms = ms;
+  return SHERD_OK;
+}
+
+int sherd_abort(sherd_ctx *ctx) {
+  if (!ctx) return SHERD_E_INVALID;
+  // Deliberately not under the lock: it is meant to reach a running call.
+  __atomic_store_n(ctx->abort_host, 1u, __ATOMIC_SEQ_CST);
+  return SHERD_OK;
+}
+
+int sherd_stats_json(sherd_ctx *ctx, char *buf, size_t len) {
+  if (!ctx || !buf || !len) return SHERD_E_INVALID;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  std::string s = "{\"backend\": \"cuda\", \"device\": " + std::to_string(ctx->device) +
+                  ", \"sm_count\": " + std::to_string(ctx->sm_count) + ", \"methods\": {";
+  bool firstm = true;
+  for (auto &kv : ctx->stats) {
+    char tmp[256];
+    std::snprintf(tmp, sizeof tmp, "%s\"%s\": {\"calls\": %llu, \"items\": %llu, \"ms\": %.3f}",
+                  firstm ? "" : ", ", kv.first.c_str(), (unsigned long long)kv.second.calls,
+                  (unsigned long long)kv.second.items, kv.second.ms);
+    s += tmp;
+    firstm = false;
+  }
+  s += "}}";
+  if (s.size() + 1 > len) return fail(ctx, SHERD_E_INVALID, "stats buffer too small");
+  std::memcpy(buf, s.c_str(), s.size() + 1);
+  return SHERD_OK;
+}
+
+uint32_t sherd_device_slack(const sherd_ctx *ctx) {
+  // A caller parked on the device is a worker not preparing the next batch
+  // (executor/mod.rs:123-136): one extra worker per 37 SMs.
+  return ctx ? uint32_t(std::max(1, ctx->sm_count / 37)) : 0u;
+}
+
+// ---- meshes -------------------------------------------------------------
+
+int sherd_mesh_upload(sherd_ctx *ctx, const float *v, uint32_t nv, const uint32_t *f, uint32_t nf,
+                      sherd_mesh **out) {
+  if (!ctx || !out || (!v && nv) || (!f && nf)) return fail(ctx, SHERD_E_INVALID, "null argument");
+  *out = nullptr;
+  if (nf == 0) return fail(ctx, SHERD_E_EMPTY, "a mesh needs at least one face");
+  for (size_t i = 0; i < size_t(3) * nf; ++i)
+    if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
+  for (size_t i = 0; i < size_t(3) * nv; ++i)
+    if (!std::isfinite(v[i])) return fail(ctx, SHERD_E_INVALID, "non-finite vertex");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CK(cudaSetDevice(ctx->device));
+  sherd_mesh *m = new sherd_mesh;
+  m->ctx = ctx;
+  m->hv.assign(v, v + size_t(3) * nv);
+  m->hf.assign(f, f + size_t(3) * nf);
+  int rc = mesh_build(ctx, m);
+  if (rc) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return SHERD_OK;
+}
+
+int sherd_mesh_subset(sherd_ctx *ctx, const sherd_mesh *mesh, const uint8_t *keep, sherd_mesh **out) {
+  if (!ctx || !mesh || !keep || !out) return fail(ctx, SHERD_E_INVALID, "null argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CK(cudaSetDevice(ctx->device));
+  sherd_mesh *m = new sherd_mesh;
+  m->ctx = ctx;
+  m->hv = mesh->hv;
+  size_t nf = mesh->hf.size() / 3;
+  for (size_t i = 0; i < nf; ++i)
+    if (keep[i]) m->hf.insert(m->hf.end(), mesh->hf.begin() + 3 * i, mesh->hf.begin() + 3 * i + 3);
+  if (m->hf.empty()) m->hf.assign(mesh->hf.begin(), mesh->hf.begin() + 3);
+  int rc = mesh_build(ctx, m);
+  if (rc) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return SHERD_OK;
+}
+
+int sherd_mesh_free(sherd_mesh *mesh) {
+  if (!mesh) return SHERD_E_INVALID;
+  cudaSetDevice(mesh->ctx->device);
+  delete mesh;
+  return SHERD_OK;
+}
+
+int sherd_mesh_aabb(const sherd_mesh *mesh, float lo[3], float hi[3]) {
+  if (!mesh || !lo || !hi) return SHERD_E_INVALID;
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = mesh->view.lo[k];
+    hi[k] = mesh->view.hi[k];
+  }
+  return SHERD_OK;
+}
+
+uint32_t sherd_mesh_faces(const sherd_mesh *mesh) { return mesh ? mesh->view.nf : 0; }
+
+int sherd_first_hit(sherd_ctx *ctx, const sherd_mesh *mesh, const float *origins, const float *dirs,
+                    uint32_t n, float *t_out, uint32_t *prim_out) {
+  if (!ctx || !mesh || ((!origins || !dirs || !t_out || !prim_out) && n))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (n == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<float> o, d, t;
+  DBuf<uint32_t> p;
+  if ((rc = upload(ctx, o, origins, size_t(3) * n)) || (rc = upload(ctx, d, dirs, size_t(3) * n)))
+    return rc;
+  CK(t.alloc(n));
+  CK(p.alloc(n));
+  k_first_hit<<<blocks_for(n), 128, 0, ctx->stream>>>(mesh->view, o.p, d.p, n, t.p, p.p,
+                                                     ctx->d_status);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(t_out, t.p, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(prim_out, p.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, "first_hit", n, true);
+}
+
+int sherd_bounded_distance(sherd_ctx *ctx, const sherd_mesh *mesh, const double *points, uint32_t n,
+                           const double pose[16], double max_dist, int reduce, double *out) {
+  if (!ctx || !mesh || !out || (!points && n)) return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (!finite_pose(pose)) return fail(ctx, SHERD_E_INVALID, "pose is not finite");
+  if (reduce != SHERD_REDUCE_ALL && reduce != SHERD_REDUCE_MIN)
+    return fail(ctx, SHERD_E_INVALID, "unknown reduction");
+  float window = float(max_dist);
+  if (reduce == SHERD_REDUCE_MIN && n == 0) {
+    *out = double(window);
+    return SHERD_OK;
+  }
+  if (n == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> p, o;
+  if ((rc = upload(ctx, p, points, size_t(3) * n))) return rc;
+  if (reduce == SHERD_REDUCE_ALL) {
+    CK(o.alloc(n));
+    k_bounded_all<<<blocks_for(n, 128), 128, 0, ctx->stream>>>(mesh->view, p.p, n, pose_of(pose),
+                                                              window, o.p, ctx->d_status);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, o.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    return finish(ctx, "bounded_distance", n, true);
+  }
+  // The scan of cpu.rs:98-111 starts from the window and keeps the smaller
+  // of it and every distance found within the shrinking window.
+  DBuf<unsigned> best;
+  CK(best.alloc(1));
+  unsigned key0;
+  float w = window;
+  std::memcpy(&key0, &w, 4);
+  if (!(window > 0.0f)) key0 = 0u;  // a non-positive window finds nothing
+  CK(cudaMemcpyAsync(best.p, &key0, 4, cudaMemcpyHostToDevice, ctx->stream));
+  if (window > 0.0f) {
+    k_bounded_min<<<blocks_for(n, 128), 128, 0, ctx->stream>>>(mesh->view, p.p, n, pose_of(pose),
+                                                              best.p, ctx->d_status);
+    CK(cudaGetLastError());
+  }
+  unsigned key = 0;
+  CK(cudaMemcpyAsync(&key, best.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  rc = finish(ctx, "bounded_distance_min", n, true);
+  if (rc) return rc;
+  float f;
+  std::memcpy(&f, &key, 4);
+  *out = window > 0.0f ? double(f) : double(window);
+  return SHERD_OK;
+}
+
+int sherd_inside(sherd_ctx *ctx, const sherd_mesh *mesh, const double *points, uint32_t n,
+                 const double pose[16], sherd_inside_outcome *out) {
+  if (!ctx || !mesh || ((!points || !out) && n)) return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (!finite_pose(pose)) return fail(ctx, SHERD_E_INVALID, "pose is not finite");
+  if (n == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> p;
+  DBuf<sherd_inside_outcome> o;
+  if ((rc = upload(ctx, p, points, size_t(3) * n))) return rc;
+  CK(o.alloc(n));
+  k_inside<<<blocks_for(n, 128), 128, 0, ctx->stream>>>(mesh->view, p.p, n, pose_of(pose), o.p,
+                                                       ctx->d_status);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, o.p, sizeof(sherd_inside_outcome) * n, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  return finish(ctx, "inside", n, true);
+}
+
+// ---- preprocessing rays ------------------------------------------------------
+
+int sherd_face_geometry(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f, uint32_t nf,
+                        double *normals, double *areas, double *centroids) {
+  if (!ctx || ((!v && nv) || (!f && nf))) return fail(ctx, SHERD_E_INVALID, "null argument");
+  for (size_t i = 0; i < size_t(3) * nf; ++i)
+    if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
+  if (nf == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> dv, dn, da, dc;
+  DBuf<uint32_t> df;
+  if ((rc = upload(ctx, dv, v, size_t(3) * nv)) || (rc = upload(ctx, df, f, size_t(3) * nf))) return rc;
+  if (normals) CK(dn.alloc(size_t(3) * nf));
+  if (areas) CK(da.alloc(nf));
+  if (centroids) CK(dc.alloc(size_t(3) * nf));
+  k_face_geometry<<<blocks_for(nf), 256, 0, ctx->stream>>>(dv.p, df.p, nf, dn.p, da.p, dc.p);
+  CK(cudaGetLastError());
+  if (normals) CK(cudaMemcpyAsync(normals, dn.p, 24 * size_t(nf), cudaMemcpyDeviceToHost, ctx->stream));
+  if (areas) CK(cudaMemcpyAsync(areas, da.p, 8 * size_t(nf), cudaMemcpyDeviceToHost, ctx->stream));
+  if (centroids)
+    CK(cudaMemcpyAsync(centroids, dc.p, 24 * size_t(nf), cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, "face_geometry", nf, true);
+}
+
+namespace {
+
+// Sorts the valid and the looking-back distances and takes both histogram
+// modes on the device (thickness.rs:139-162).
+int thickness_modes(sherd_ctx *ctx, DBuf<float> &ok, DBuf<float> &far, DBuf<unsigned> &counts,
+                    float *t, float *mode, uint32_t *found) {
+  unsigned hc[2];
+  CK(cudaMemcpyAsync(hc, counts.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (hc[0] < 100) {
+    *found = 0;
+    return SHERD_OK;
+  }
+  DBuf<float> sorted;
+  DBuf<float> modes;
+  CK(sorted.alloc(std::max(hc[0], 1u)));
+  CK(modes.alloc(2));
+  size_t temp_bytes = 0;
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, ok.p, sorted.p, int(hc[0]), 0, 32,
+                                    ctx->stream));
+  DBuf<unsigned char> temp;
+  CK(temp.alloc(temp_bytes));
+  CK(cub::DeviceRadixSort::SortKeys(temp.p, temp_bytes, ok.p, sorted.p, int(hc[0]), 0, 32,
+                                    ctx->stream));
+  k_hist_mode<<<1, 1024, 0, ctx->stream>>>(sorted.p, hc[0], modes.p);
+  CK(cudaGetLastError());
+  if (hc[1] >= 100) {
+    CK(cub::DeviceRadixSort::SortKeys(temp.p, temp_bytes, far.p, sorted.p, int(hc[1]), 0, 32,
+                                      ctx->stream));
+    k_hist_mode<<<1, 1024, 0, ctx->stream>>>(sorted.p, hc[1], modes.p + 1);
+    CK(cudaGetLastError());
+  }
+  float hm[2];
+  CK(cudaMemcpyAsync(hm, modes.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *mode = hm[0];
+  *t = hc[1] >= 100 ? hm[1] : hm[0];
+  *found = 1;
+  return SHERD_OK;
+}
+
+}  // namespace
+
+int sherd_thickness(sherd_ctx *ctx, const sherd_mesh *mesh, const double *centroids,
+                    const double *normals, uint32_t nf, uint32_t max_rays, float *t,
+                    float *thick_mode, uint32_t *found, float *t_hit, uint32_t *prim) {
+  if (!ctx || !mesh || !centroids || !normals || !t || !thick_mode || !found)
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (nf != mesh->view.nf) return fail(ctx, SHERD_E_INVALID, "face count differs from the mesh");
+  *found = 0;
+  if (nf == 0) return SHERD_OK;
+  uint32_t n_req = max_rays ? max_rays : 1;
+  uint32_t stride = std::max<uint32_t>(1, (nf + n_req - 1) / n_req);
+  uint32_t n = (nf + stride - 1) / stride;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> dc, dn;
+  DBuf<float> th, ok, far;
+  DBuf<uint32_t> pr;
+  DBuf<unsigned> counts;
+  if ((rc = upload(ctx, dc, centroids, size_t(3) * nf)) || (rc = upload(ctx, dn, normals, size_t(3) * nf)))
+    return rc;
+  CK(th.alloc(n));
+  CK(pr.alloc(n));
+  CK(ok.alloc(n));
+  CK(far.alloc(n));
+  CK(counts.alloc(2));
+  CK(cudaMemsetAsync(counts.p, 0, 8, ctx->stream));
+  k_thickness_rays<<<blocks_for(n, 128), 128, 0, ctx->stream>>>(
+      mesh->view, dc.p, dn.p, nf, stride, n, th.p, pr.p, ok.p, far.p, counts.p, ctx->d_status);
+  CK(cudaGetLastError());
+  rc = thickness_modes(ctx, ok, far, counts, t, thick_mode, found);
+  if (rc) return rc;
+  if (t_hit) CK(cudaMemcpyAsync(t_hit, th.p, 4 * size_t(n), cudaMemcpyDeviceToHost, ctx->stream));
+  if (prim) CK(cudaMemcpyAsync(prim, pr.p, 4 * size_t(n), cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, "thickness", n, true);
+}
+
+int sherd_thickness_from_hits(sherd_ctx *ctx, const double *normals, uint32_t nf, const uint32_t *idx,
+                              const float *t_hit, const uint32_t *prim, uint32_t n, float *t,
+                              float *thick_mode, uint32_t *found) {
+  if (!ctx || !normals || !t || !thick_mode || !found || ((!idx || !t_hit || !prim) && n))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  for (uint32_t k = 0; k < n; ++k)
+    if (idx[k] >= nf) return fail(ctx, SHERD_E_INVALID, "ray face id beyond the mesh");
+  *found = 0;
+  if (n == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> dn;
+  DBuf<uint32_t> di, dp;
+  DBuf<float> dt, ok, far;
+  DBuf<unsigned> counts;
+  if ((rc = upload(ctx, dn, normals, size_t(3) * nf)) || (rc = upload(ctx, di, idx, n)) ||
+      (rc = upload(ctx, dt, t_hit, n)) || (rc = upload(ctx, dp, prim, n)))
+    return rc;
+  CK(ok.alloc(n));
+  CK(far.alloc(n));
+  CK(counts.alloc(2));
+  CK(cudaMemsetAsync(counts.p, 0, 8, ctx->stream));
+  k_thickness_filter<<<blocks_for(n), 256, 0, ctx->stream>>>(dn.p, nf, di.p, dt.p, dp.p, n, ok.p,
+                                                            far.p, counts.p);
+  CK(cudaGetLastError());
+  rc = thickness_modes(ctx, ok, far, counts, t, thick_mode, found);
+  if (rc) return rc;
+  return finish(ctx, "thickness_from_hits", n, true);
+}
+
+int sherd_cone_votes(sherd_ctx *ctx, const sherd_mesh *mesh, const double *centroids,
+                     const double *normals, const double *ns, const double *hit_normals,
+                     uint32_t nf, double thick, uint8_t *good) {
+  if (!ctx || !mesh || ((!centroids || !normals || !ns || !hit_normals || !good) && nf))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (nf != mesh->view.nf) return fail(ctx, SHERD_E_INVALID, "face count differs from the mesh");
+  if (nf == 0) return SHERD_OK;
+  // The cone's constants in f64 on the host, as segment.rs:330-355 computes
+  // them: 15 degrees through to_radians and the six azimuths 2 pi (k-1) / 6.
+  const double PI = 3.14159265358979323846;
+  ConeConsts cc;
+  double angle = 15.0 * (PI / 180.0);
+  cc.cos_a = std::cos(angle);
+  cc.sin_a = std::sin(angle);
+  for (int k = 1; k < 7; ++k) {
+    double phi = 2.0 * PI * double(k - 1) / 6.0;
+    cc.cp[k - 1] = std::cos(phi);
+    cc.sp[k - 1] = std::sin(phi);
+  }
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> dc, dn, dns, dh;
+  DBuf<uint8_t> dg;
+  if ((rc = upload(ctx, dc, centroids, size_t(3) * nf)) || (rc = upload(ctx, dn, normals, size_t(3) * nf)) ||
+      (rc = upload(ctx, dns, ns, size_t(3) * nf)) || (rc = upload(ctx, dh, hit_normals, size_t(3) * nf)))
+    return rc;
+  CK(dg.alloc(nf));
+  k_cone_votes<<<blocks_for(nf, 128), 128, 0, ctx->stream>>>(mesh->view, dc.p, dn.p, dns.p, dh.p, nf,
+                                                            thick, cc, dg.p, ctx->d_status);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(good, dg.p, nf, cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, "cone_votes", size_t(nf) * 7, true);
+}
+
+// ---- clouds ----------------------------------------------------------------
+
+int sherd_cloud_upload(sherd_ctx *ctx, const double *points, const double *normals, uint32_t np,
+                       sherd_cloud **out) {
+  if (!ctx || !out || (!points && np)) return fail(ctx, SHERD_E_INVALID, "null argument");
+  *out = nullptr;
+  if (np == 0) return fail(ctx, SHERD_E_EMPTY, "a cloud needs at least one point");
+  for (size_t i = 0; i < size_t(3) * np; ++i)
+    if (!std::isfinite(points[i])) return fail(ctx, SHERD_E_INVALID, "non-finite point");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CK(cudaSetDevice(ctx->device));
+  sherd_cloud *c = new sherd_cloud;
+  int rc = cloud_build(ctx, points, normals, np, c);
+  if (rc) {
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return SHERD_OK;
+}
+
+int sherd_cloud_free(sherd_cloud *cloud) {
+  if (!cloud) return SHERD_E_INVALID;
+  cudaSetDevice(cloud->ctx->device);
+  delete cloud;
+  return SHERD_OK;
+}
+
+uint32_t sherd_cloud_points(const sherd_cloud *cloud) { return cloud ? cloud->view.n : 0; }
+
+int sherd_nearest_within_sq(sherd_ctx *ctx, const sherd_cloud *cloud, const double *queries, uint32_t n,
+                            double r2, uint32_t *idx, double *d2) {
+  if (!ctx || !cloud || ((!queries || !idx || !d2) && n)) return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (n == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> q, o;
+  DBuf<uint32_t> i;
+  if ((rc = upload(ctx, q, queries, size_t(3) * n))) return rc;
+  CK(o.alloc(n));
+  CK(i.alloc(n));
+  k_nn_within<<<blocks_for(n, 128), 128, 0, ctx->stream>>>(cloud->view, q.p, n, r2, i.p, o.p,
+                                                          ctx->d_status);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(idx, i.p, 4 * size_t(n), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(d2, o.p, 8 * size_t(n), cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, "nearest_within_sq", n, true);
+}
+
+int sherd_nearest_below(sherd_ctx *ctx, const sherd_cloud *cloud, const double *queries, uint32_t n,
+                        double bound, uint32_t *idx, double *dist) {
+  if (!ctx || !cloud || ((!queries || !idx || !dist) && n)) return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (n == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> q, o;
+  DBuf<uint32_t> i;
+  if ((rc = upload(ctx, q, queries, size_t(3) * n))) return rc;
+  CK(o.alloc(n));
+  CK(i.alloc(n));
+  k_nn_below<<<blocks_for(n, 128), 128, 0, ctx->stream>>>(cloud->view, q.p, n, bound, i.p, o.p,
+                                                         ctx->d_status);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(idx, i.p, 4 * size_t(n), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(dist, o.p, 8 * size_t(n), cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, "nearest_below", n, true);
+}
+
+// ---- ICP -----------------------------------------------------------------------
+
+int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source, const sherd_cloud *target,
+                   const double *inits, uint32_t k, sherd_icp_options options,
+                   sherd_registration *out) {
+  if (!ctx || !target || ((!inits || !out) && k) || (!source && n_source))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (options.estimation != SHERD_POINT_TO_PLANE)
+    return fail(ctx, SHERD_E_INVALID, "only the point-to-plane rung runs on the device");
+  if (options.max_iteration < 0) return fail(ctx, SHERD_E_INVALID, "negative iteration cap");
+  for (uint32_t c = 0; c < k; ++c)
+    if (!finite_pose(inits + 16 * size_t(c))) return fail(ctx, SHERD_E_INVALID, "init pose is not finite");
+  if (k == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  sherd_cloud src;
+  DBuf<double> di;
+  DBuf<sherd_registration> dout;
+  if (n_source) {
+    if (has_nan(source, size_t(3) * n_source)) return fail(ctx, SHERD_E_INVALID, "non-finite source point");
+    rc = cloud_build(ctx, source, nullptr, n_source, &src);
+    if (rc) return rc;
+  }
+  if ((rc = upload(ctx, di, inits, size_t(16) * k))) return rc;
+  CK(dout.alloc(k));
+  CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  k_icp_rung<<<k, ICP_BLOCK, 0, ctx->stream>>>(n_source ? src.pts.p : nullptr, n_source, target->view,
+                                               di.p, options, dout.p, ctx->d_status);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, dout.p, sizeof(sherd_registration) * k, cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, "icp_rung", k, true);
+}
+
+// ---- verification ------------------------------------------------------------
+
+int sherd_surfaces_create(sherd_ctx *ctx, const sherd_mesh *fracture, const sherd_mesh *mesh,
+                          uint32_t watertight, double frac_area, const double *pf, uint32_t n_pf,
+                          const double *s, uint32_t n_s, const double *brk_p, const double *brk_ns,
+                          uint32_t n_brk, const double *margin_p, const double *margin_n,
+                          uint32_t n_margin, sherd_surfaces **out) {
+  if (!ctx || !fracture || !out || (!pf && n_pf) || (!s && n_s) || ((!brk_p || !brk_ns) && n_brk) ||
+      ((!margin_p || !margin_n) && n_margin))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CK(cudaSetDevice(ctx->device));
+  sherd_surfaces *x = new sherd_surfaces;
+  x->ctx = ctx;
+  x->fracture = fracture;
+  x->mesh = mesh;
+  auto up = [&](DBuf<double> &b, const double *h, uint32_t n) { return upload(ctx, b, h, size_t(3) * n); };
+  int rc = 0;
+  if ((rc = up(x->pf, pf, n_pf)) || (rc = up(x->s, s, n_s)) || (rc = up(x->brk_p, brk_p, n_brk)) ||
+      (rc = up(x->brk_ns, brk_ns, n_brk)) || (rc = up(x->margin_p, margin_p, n_margin)) ||
+      (rc = up(x->margin_n, margin_n, n_margin))) {
+    delete x;
+    return rc;
+  }
+  if (n_brk) {
+    if ((rc = cloud_build(ctx, brk_p, nullptr, n_brk, &x->brk_tree))) {
+      delete x;
+      return rc;
+    }
+    x->has_brk_tree = true;
+    x->brk_p_host.assign(brk_p, brk_p + size_t(3) * n_brk);
+  }
+  if (n_margin) {
+    if ((rc = cloud_build(ctx, margin_p, nullptr, n_margin, &x->margin_tree))) {
+      delete x;
+      return rc;
+    }
+    x->has_margin_tree = true;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  SurfView &v = x->view;
+  v.frac = fracture->view;
+  if (mesh) v.mesh = mesh->view;
+  v.has_mesh = mesh ? 1u : 0u;
+  v.watertight = watertight ? 1u : 0u;
+  v.frac_area = frac_area;
+  v.pf = x->pf.p;
+  v.n_pf = n_pf;
+  v.s = x->s.p;
+  v.n_s = n_s;
+  v.brk_p = x->brk_p.p;
+  v.brk_ns = x->brk_ns.p;
+  v.n_brk = n_brk;
+  v.brk_tree = x->brk_tree.view;
+  v.margin_p = x->margin_p.p;
+  v.margin_n = x->margin_n.p;
+  v.n_margin = n_margin;
+  v.margin_tree = x->margin_tree.view;
+  *out = x;
+  return SHERD_OK;
+}
+
+int sherd_surfaces_free(sherd_surfaces *s) {
+  if (!s) return SHERD_E_INVALID;
+  cudaSetDevice(s->ctx->device);
+  delete s;
+  return SHERD_OK;
+}
+
+void sherd_params_default(sherd_params *p) {
+  if (!p) return;
+  *p = sherd_params{0.25, 0.03, 0.005, 3.0, 0.8,
+                    0.15, 0.06, 0.01, 0.3, 0.12, 0.5, 0.06, 0.5, 0.04,
+                    2.3, 0.9, 0.15, 1.0, 0.45, 1.8, 4.0, 0.9, 0.6};
+}
+
+int sherd_scales_for_pair(const sherd_params *p, double t, double res, sherd_scales *out) {
+  if (!p || !out) return SHERD_E_INVALID;
+  auto f = [&](double k, double m) { return std::max(k * t, m * res); };
+  out->t = t;
+  out->res = res;
+  out->coarse = f(p->coarse_delta, p->coarse_res);
+  out->stage1 = f(p->stage1_delta, p->stage1_res);
+  out->tight = f(p->tight_delta, p->tight_res);
+  out->facing = f(p->facing_delta, p->facing_res);
+  out->gap = f(p->max_gap, p->gap_res);
+  out->seam = f(p->seam_delta, p->seam_res);
+  out->near = f(p->near_delta, p->near_res);
+  out->pen = f(p->pen_delta, p->pen_res);
+  out->nms = p->nms_delta * t;
+  out->icp = f(p->icp_delta, p->icp_res) / (p->icp_delta * t);
+  return SHERD_OK;
+}
+
+uint32_t sherd_accept(const sherd_scores *s, const sherd_params *p, const sherd_scales *sc) {
+  if (!s || !p || !sc) return 0;
+  return (s->tight >= p->min_tight && s->gap * sc->t <= sc->gap && s->pen <= p->max_pen &&
+          s->seam >= p->min_seam && s->cont_n >= p->min_cont_n)
+             ? 1u
+             : 0u;
+}
+
+namespace {
+
+int pair_view(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfaces *b, const sherd_scales *sc,
+              DBuf<uint32_t> &a_cell, PairView &v) {
+  v = PairView{};
+  v.a = a->view;
+  v.b = b->view;
+  v.sc = *sc;
+  int rc = seam_cells(ctx, a->brk_p_host, sc->t, a_cell, v.n_cells);
+  if (rc) return rc;
+  v.a_cell = a_cell.p;
+  v.scratch_floats = scratch_words(v);
+  return SHERD_OK;
+}
+
+}  // namespace
+
+int sherd_verify(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfaces *b, const double pose[16],
+                 const sherd_scales *sc, int full, sherd_scores *out) {
+  if (!ctx || !a || !b || !sc || !out) return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (!finite_pose(pose)) return fail(ctx, SHERD_E_INVALID, "pose is not finite");
+  if (!(sc->t > 0.0)) return fail(ctx, SHERD_E_INVALID, "scales need t > 0");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<uint32_t> cells;
+  PairView v;
+  if ((rc = pair_view(ctx, a, b, sc, cells, v))) return rc;
+  DBuf<PairView> dv;
+  DBuf<sherd_work_item> di;
+  DBuf<sherd_candidate> dc;
+  DBuf<uint32_t> order;
+  DBuf<unsigned> head, scratch;
+  sherd_work_item item{};
+  std::memcpy(item.init, pose, sizeof item.init);
+  sherd_candidate cand{};
+  std::memcpy(cand.rungs[3].transform, pose, sizeof cand.rungs[3].transform);
+  uint32_t zero = 0;
+  if ((rc = upload(ctx, dv, &v, 1)) || (rc = upload(ctx, di, &item, 1)) || (rc = upload(ctx, dc, &cand, 1)) ||
+      (rc = upload(ctx, order, &zero, 1)) || (rc = upload(ctx, head, &zero, 1)))
+    return rc;
+  CK(scratch.alloc(v.scratch_floats));
+  QueueCtl q{head.p, order.p, 1, nullptr, 0};
+  sherd_params p;
+  sherd_params_default(&p);
+  k_verify_items<<<1, VER_BLOCK, 0, ctx->stream>>>(dv.p, di.p, q, p, scratch.p, v.scratch_floats, dc.p,
+                                                  full, ctx->d_status);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&cand, dc.p, sizeof cand, cudaMemcpyDeviceToHost, ctx->stream));
+  rc = finish(ctx, "verify", 1, true);
+  if (rc) return rc;
+  *out = cand.scores;
+  return SHERD_OK;
+}
+
+// ---- the batched stage-2 path ---------------------------------------------------
+
+int sherd_pair_create(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfaces *b,
+                      const sherd_cloud *reg_target, const sherd_cloud *frac_target,
+                      const double *reg_source, uint32_t n_reg, const double *frac_source,
+                      uint32_t n_frac, const sherd_scales *sc, sherd_pair **out) {
+  if (!ctx || !a || !b || !reg_target || !frac_target || !sc || !out || (!reg_source && n_reg) ||
+      (!frac_source && n_frac))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  *out = nullptr;
+  if (!(sc->t > 0.0)) return fail(ctx, SHERD_E_INVALID, "scales need t > 0");
+  if (!reg_target->view.nrm || !frac_target->view.nrm)
+    return fail(ctx, SHERD_E_INVALID, "point-to-plane targets need normals");
+  if ((n_reg && has_nan(reg_source, size_t(3) * n_reg)) || (n_frac && has_nan(frac_source, size_t(3) * n_frac)))
+    return fail(ctx, SHERD_E_INVALID, "non-finite source point");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CK(cudaSetDevice(ctx->device));
+  sherd_pair *p = new sherd_pair;
+  p->ctx = ctx;
+  p->a = a;
+  p->b = b;
+  int rc = 0;
+  // The moving clouds are stored in Morton order (the LBVH builder's sorted
+  // points), so a warp's consecutive source points query nearby targets.
+  if (n_reg && (rc = cloud_build(ctx, reg_source, nullptr, n_reg, &p->reg_src))) {
+    delete p;
+    return rc;
+  }
+  if (n_frac && (rc = cloud_build(ctx, frac_source, nullptr, n_frac, &p->frac_src))) {
+    delete p;
+    return rc;
+  }
+  if ((rc = pair_view(ctx, a, b, sc, p->a_cell, p->view))) {
+    delete p;
+    return rc;
+  }
+  p->view.reg_tgt = reg_target->view;
+  p->view.frac_tgt = frac_target->view;
+  p->view.reg_src = n_reg ? p->reg_src.pts.p : nullptr;
+  p->view.n_reg = n_reg;
+  p->view.frac_src = n_frac ? p->frac_src.pts.p : nullptr;
+  p->view.n_frac = n_frac;
+  CK(cudaStreamSynchronize(ctx->stream));
+  *out = p;
+  return SHERD_OK;
+}
+
+int sherd_pair_free(sherd_pair *pair) {
+  if (!pair) return SHERD_E_INVALID;
+  cudaSetDevice(pair->ctx->device);
+  delete pair;
+  return SHERD_OK;
+}
+
+int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
+                              const sherd_work_item *items, uint32_t n_items, const sherd_params *p,
+                              int sched, sherd_candidate *out) {
+  if (!ctx || !p || ((!pairs) && n_pairs) || ((!items || !out) && n_items))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (sched != SHERD_SCHED_BATCHED && sched != SHERD_SCHED_PLAIN)
+    return fail(ctx, SHERD_E_INVALID, "unknown schedule");
+  for (uint32_t i = 0; i < n_pairs; ++i)
+    if (!pairs[i] || pairs[i]->ctx != ctx) return fail(ctx, SHERD_E_INVALID, "pair of another context");
+  // Cost per item, for the longest-first queue order: the ladder's point
+  // iterations and the verification's sample counts.
+  std::vector<double> pair_cost(n_pairs);
+  uint32_t max_scratch = 1;
+  for (uint32_t i = 0; i < n_pairs; ++i) {
+    const PairView &v = pairs[i]->view;
+    pair_cost[i] = 60.0 * (double(v.n_reg) + double(v.n_frac)) + 4.0 * (v.a.n_s + v.b.n_s) +
+                   double(v.a.n_pf + v.b.n_pf);
+    max_scratch = std::max(max_scratch, v.scratch_floats);
+  }
+  for (uint32_t i = 0; i < n_items; ++i) {
+    if (items[i].pair >= n_pairs) return fail(ctx, SHERD_E_INVALID, "work item names no pair");
+    if (!finite_pose(items[i].init)) return fail(ctx, SHERD_E_INVALID, "work item pose is not finite");
+  }
+  if (n_items == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  __atomic_store_n(ctx->abort_host, 0u, __ATOMIC_SEQ_CST);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  std::vector<PairView> views(n_pairs);
+  for (uint32_t i = 0; i < n_pairs; ++i) views[i] = pairs[i]->view;
+  std::vector<uint32_t> order(n_items);
+  for (uint32_t i = 0; i < n_items; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+    return pair_cost[items[x].pair] > pair_cost[items[y].pair];
+  });
+  DBuf<PairView> dv;
+  DBuf<sherd_work_item> di;
+  DBuf<sherd_candidate> dc;
+  DBuf<uint32_t> dorder;
+  DBuf<unsigned> heads, scratch;
+  if ((rc = upload(ctx, dv, views.data(), n_pairs)) || (rc = upload(ctx, di, items, n_items)) ||
+      (rc = upload(ctx, dorder, order.data(), n_items)))
+    return rc;
+  CK(dc.alloc(n_items));
+  CK(cudaMemsetAsync(dc.p, 0, sizeof(sherd_candidate) * n_items, ctx->stream));
+  CK(heads.alloc(2 * size_t(std::max<uint32_t>(n_pairs, 1))));
+  int occ_l = 0, occ_v = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, k_ladder, ICP_BLOCK, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_v, k_verify_items, VER_BLOCK, 0));
+  unsigned grid_l = unsigned(std::max(1, occ_l) * ctx->sm_count);
+  unsigned grid_v = unsigned(std::max(1, occ_v) * ctx->sm_count);
+  unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
+  CK(scratch.alloc(size_t(grid_v) * max_scratch));
+  CK(cudaMemsetAsync(heads.p, 0, sizeof(unsigned) * 2 * std::max<uint32_t>(n_pairs, 1), ctx->stream));
+  if (sched == SHERD_SCHED_BATCHED) {
+    QueueCtl ql{heads.p, dorder.p, n_items, ctx->abort_dev, budget};
+    QueueCtl qv{heads.p + 1, dorder.p, n_items, ctx->abort_dev, budget};
+    k_ladder<<<std::min<unsigned>(grid_l, n_items), ICP_BLOCK, 0, ctx->stream>>>(dv.p, di.p, ql, dc.p,
+                                                                              ctx->d_status);
+    CK(cudaGetLastError());
+    k_verify_items<<<std::min<unsigned>(grid_v, n_items), VER_BLOCK, 0, ctx->stream>>>(
+        dv.p, di.p, qv, *p, scratch.p, max_scratch, dc.p, 1, ctx->d_status);
+    CK(cudaGetLastError());
+  } else {
+    // One launch pair per pair, in pair order, synchronised between pairs.
+    std::vector<std::vector<uint32_t>> per(n_pairs);
+    for (uint32_t i = 0; i < n_items; ++i) per[items[i].pair].push_back(i);
+    size_t off = 0;
+    std::vector<uint32_t> flat;
+    std::vector<size_t> start(n_pairs);
+    for (uint32_t i = 0; i < n_pairs; ++i) {
+      start[i] = flat.size();
+      flat.insert(flat.end(), per[i].begin(), per[i].end());
+    }
+    (void)off;
+    CK(cudaMemcpyAsync(dorder.p, flat.data(), 4 * size_t(n_items), cudaMemcpyHostToDevice, ctx->stream));
+    for (uint32_t i = 0; i < n_pairs; ++i) {
+      uint32_t cnt = uint32_t(per[i].size());
+      if (!cnt) continue;
+      QueueCtl ql{heads.p + 2 * i, dorder.p + start[i], cnt, ctx->abort_dev, budget};
+      QueueCtl qv{heads.p + 2 * i + 1, dorder.p + start[i], cnt, ctx->abort_dev, budget};
+      k_ladder<<<cnt, ICP_BLOCK, 0, ctx->stream>>>(dv.p, di.p, ql, dc.p, ctx->d_status);
+      CK(cudaGetLastError());
+      k_verify_items<<<std::min<unsigned>(cnt, grid_v), VER_BLOCK, 0, ctx->stream>>>(
+          dv.p, di.p, qv, *p, scratch.p, max_scratch, dc.p, 1, ctx->d_status);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(ctx->stream));
+    }
+  }
+  CK(cudaMemcpyAsync(out, dc.p, sizeof(sherd_candidate) * n_items, cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, sched == SHERD_SCHED_BATCHED ? "ladder_verify_batched" : "ladder_verify_plain",
+                n_items, true);
+}
+
+}  // extern "C"

@@ -1,0 +1,384 @@
+// traverse.cuh — per-thread short-stack BVH traversal for the four queries of
+// the hot path. Every query is exact under one tie rule:
+//   first hit      smallest t, then lowest original face index
+//   crossings      every face the ray crosses (no pruning by distance)
+//   distance       smallest f32 point-to-triangle distance (a value, no id)
+//   nearest point  smallest f64 squared distance, then lowest original index
+// Pruning only ever drops a node whose padded box is provably beyond the best
+// answer so far (relative slack 4e-6 on top of the box padding), so the result
+// is the brute-force result the CPU oracle computes.
+#pragma once
+
+#include "lbvh.cuh"
+
+namespace sherd {
+
+struct Child2 {
+  float lo0[3], hi0[3], lo1[3], hi1[3];
+  int ref[2], cnt[2];
+};
+
+__device__ __forceinline__ Child2 load_node(const BNode *nodes, int i) {
+  const float4 *p = reinterpret_cast<const float4 *>(nodes + i);
+  float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+  int4 d = __ldg(reinterpret_cast<const int4 *>(p + 3));
+  Child2 n;
+  n.lo0[0] = a.x; n.lo0[1] = a.y; n.lo0[2] = a.z; n.hi0[0] = a.w;
+  n.hi0[1] = b.x; n.hi0[2] = b.y; n.lo1[0] = b.z; n.lo1[1] = b.w;
+  n.lo1[2] = c.x; n.hi1[0] = c.y; n.hi1[1] = c.z; n.hi1[2] = c.w;
+  n.ref[0] = d.x; n.ref[1] = d.y; n.cnt[0] = d.z; n.cnt[1] = d.w;
+  return n;
+}
+
+struct Ray {
+  float o[3], d[3], inv[3];
+  bool zero[3];
+};
+
+__device__ __forceinline__ Ray make_ray(F3 o, F3 d) {
+  Ray r;
+  r.o[0] = o.x; r.o[1] = o.y; r.o[2] = o.z;
+  r.d[0] = d.x; r.d[1] = d.y; r.d[2] = d.z;
+  for (int a = 0; a < 3; ++a) {
+    r.zero[a] = r.d[a] == 0.0f;
+    r.inv[a] = r.zero[a] ? 0.0f : 1.0f / r.d[a];
+  }
+  return r;
+}
+
+// Entry parameter of the ray into a padded box over [0, inf), or +inf.
+__device__ __forceinline__ float slab_enter(const Ray &r, const float *lo, const float *hi) {
+  float tmin = 0.0f, tmax = f_inf();
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (r.zero[a]) {
+      if (r.o[a] < lo[a] || r.o[a] > hi[a]) return f_inf();
+    } else {
+      float t0 = (lo[a] - r.o[a]) * r.inv[a], t1 = (hi[a] - r.o[a]) * r.inv[a];
+      tmin = fmaxf(tmin, fminf(t0, t1));
+      tmax = fminf(tmax, fmaxf(t0, t1));
+    }
+  }
+  return tmin <= tmax + 4e-6f * fabsf(tmax) ? tmin : f_inf();
+}
+
+__device__ __forceinline__ void tri_at(const MeshView &m, uint32_t s, F3 &a, F3 &b, F3 &c,
+                                       uint32_t &id) {
+  float4 x = __ldg(m.tri + 3 * s), y = __ldg(m.tri + 3 * s + 1), z = __ldg(m.tri + 3 * s + 2);
+  a = {x.x, x.y, x.z};
+  b = {y.x, y.y, y.z};
+  c = {z.x, z.y, z.z};
+  id = __float_as_uint(x.w);
+}
+
+// RayScene::first_hit (spatial/bvh.rs:84-90).
+__device__ void first_hit(const MeshView &m, F3 o, F3 d, float &best, uint32_t &best_id,
+                          uint32_t &status) {
+  best = f_inf();
+  best_id = MISS;
+  if (m.nf == 0) return;
+  Ray r = make_ray(o, d);
+  float dn = sqrtf(dot(d, d));
+  float pad_t = dn > 0.0f ? 4.0f * m.pad / dn : f_inf();
+  auto bound = [&]() { return best == f_inf() ? f_inf() : best + 4e-6f * best + pad_t; };
+  auto leaf = [&](int first, int count) {
+    for (int s = first; s < first + count; ++s) {
+      F3 a, b, c;
+      uint32_t id;
+      tri_at(m, s, a, b, c, id);
+      float t = moller_trumbore(o, d, a, b, c);
+      if (t < 0.0f) continue;
+      if (t < best || (t == best && id < best_id)) {
+        best = t;
+        best_id = id;
+      }
+    }
+  };
+  if (m.root_leaf) {
+    leaf(0, m.root_leaf);
+    return;
+  }
+  int stack_n[STACK];
+  float stack_t[STACK];
+  int sp = 0, node = 0;
+  uint32_t visits = 0;
+  for (;;) {
+    if (++visits > 2u * m.nf + 64u) {
+      status |= ST_STACK;
+      break;
+    }
+    Child2 n = load_node(m.nodes, node);
+    float te[2] = {slab_enter(r, n.lo0, n.hi0), slab_enter(r, n.lo1, n.hi1)};
+    int near_c = te[1] < te[0] ? 1 : 0;
+    int next = -1;
+    for (int q = 0; q < 2; ++q) {
+      int c = q == 0 ? near_c : 1 - near_c;
+      if (!(te[c] <= bound())) continue;
+      if (n.cnt[c]) {
+        leaf(n.ref[c], n.cnt[c]);
+      } else if (next < 0) {
+        next = n.ref[c];
+      } else if (sp < STACK) {
+        stack_n[sp] = n.ref[c];
+        stack_t[sp++] = te[c];
+      } else {
+        status |= ST_STACK;
+      }
+    }
+    if (next >= 0) {
+      node = next;
+      continue;
+    }
+    bool more = false;
+    while (sp > 0) {
+      --sp;
+      if (stack_t[sp] <= bound()) {
+        node = stack_n[sp];
+        more = true;
+        break;
+      }
+    }
+    if (!more) break;
+  }
+}
+
+// RayScene::crossings (spatial/bvh.rs:160-175) along +x, +y or +z: every face
+// the axis ray from p crosses. The box test is three comparisons per child.
+__device__ uint32_t crossings_axis(const MeshView &m, F3 p, int axis, uint32_t &status) {
+  if (m.nf == 0) return 0;
+  F3 d = {axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f};
+  float pc[3] = {p.x, p.y, p.z};
+  int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+  uint32_t hits = 0;
+  auto leaf = [&](int first, int count) {
+    for (int s = first; s < first + count; ++s) {
+      F3 a, b, c;
+      uint32_t id;
+      tri_at(m, s, a, b, c, id);
+      if (moller_trumbore(p, d, a, b, c) >= 0.0f) ++hits;
+    }
+  };
+  auto box_hit = [&](const float *lo, const float *hi) {
+    return pc[a1] >= lo[a1] && pc[a1] <= hi[a1] && pc[a2] >= lo[a2] && pc[a2] <= hi[a2] &&
+           hi[axis] >= pc[axis];
+  };
+  if (m.root_leaf) {
+    leaf(0, m.root_leaf);
+    return hits;
+  }
+  int stack_n[STACK];
+  int sp = 0, node = 0;
+  uint32_t visits = 0;
+  for (;;) {
+    if (++visits > 2u * m.nf + 64u) {
+      status |= ST_STACK;
+      break;
+    }
+    Child2 n = load_node(m.nodes, node);
+    bool h[2] = {box_hit(n.lo0, n.hi0), box_hit(n.lo1, n.hi1)};
+    int next = -1;
+    for (int c = 0; c < 2; ++c) {
+      if (!h[c]) continue;
+      if (n.cnt[c]) {
+        leaf(n.ref[c], n.cnt[c]);
+      } else if (next < 0) {
+        next = n.ref[c];
+      } else if (sp < STACK) {
+        stack_n[sp++] = n.ref[c];
+      } else {
+        status |= ST_STACK;
+      }
+    }
+    if (next >= 0) {
+      node = next;
+      continue;
+    }
+    if (sp == 0) break;
+    node = stack_n[--sp];
+  }
+  return hits;
+}
+
+// RayScene::inside (spatial/bvh.rs:146-157): the majority of three parities.
+__device__ __forceinline__ bool inside_mesh(const MeshView &m, F3 p, uint32_t &status) {
+  int votes = 0;
+  for (int a = 0; a < 3; ++a) votes += int(crossings_axis(m, p, a, status) & 1u);
+  return votes >= 2;
+}
+
+__device__ __forceinline__ float box_dist2(const float *lo, const float *hi, const float *p) {
+  float s = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float g = fmaxf(fmaxf(lo[a] - p[a], p[a] - hi[a]), 0.0f);
+    s += g * g;
+  }
+  return s;
+}
+
+// RayScene::bounded_distance (spatial/bvh.rs:123-131): the distance to the
+// nearest face when it is <= window (inclusive), else +inf. window = +inf is
+// RayScene::distance (bvh.rs:110-113).
+__device__ float mesh_distance(const MeshView &m, F3 p, float window, uint32_t &status) {
+  float best = f_inf();
+  if (m.nf == 0 || !(window > 0.0f)) return best;
+  float pc[3] = {p.x, p.y, p.z};
+  auto bound2 = [&]() {
+    float b = fminf(best, window);
+    if (b == f_inf()) return f_inf();
+    float s = b + 4e-6f * b + m.pad;
+    return s * s;
+  };
+  auto leaf = [&](int first, int count) {
+    for (int s = first; s < first + count; ++s) {
+      F3 a, b, c;
+      uint32_t id;
+      tri_at(m, s, a, b, c, id);
+      float dd = tri_distance(p, a, b, c);
+      if (dd <= window && dd < best) best = dd;
+    }
+  };
+  if (m.root_leaf) {
+    leaf(0, m.root_leaf);
+    return best;
+  }
+  int stack_n[STACK];
+  float stack_k[STACK];
+  int sp = 0, node = 0;
+  uint32_t visits = 0;
+  for (;;) {
+    if (++visits > 2u * m.nf + 64u) {
+      status |= ST_STACK;
+      break;
+    }
+    Child2 n = load_node(m.nodes, node);
+    float k[2] = {box_dist2(n.lo0, n.hi0, pc), box_dist2(n.lo1, n.hi1, pc)};
+    int near_c = k[1] < k[0] ? 1 : 0;
+    int next = -1;
+    for (int q = 0; q < 2; ++q) {
+      int c = q == 0 ? near_c : 1 - near_c;
+      if (!(k[c] <= bound2())) continue;
+      if (n.cnt[c]) {
+        leaf(n.ref[c], n.cnt[c]);
+      } else if (next < 0) {
+        next = n.ref[c];
+      } else if (sp < STACK) {
+        stack_n[sp] = n.ref[c];
+        stack_k[sp++] = k[c];
+      } else {
+        status |= ST_STACK;
+      }
+    }
+    if (next >= 0) {
+      node = next;
+      continue;
+    }
+    bool more = false;
+    while (sp > 0) {
+      --sp;
+      if (stack_k[sp] <= bound2()) {
+        node = stack_n[sp];
+        more = true;
+        break;
+      }
+    }
+    if (!more) break;
+  }
+  return best;
+}
+
+// PointTree::nearest_within_squared (spatial/kdtree.rs:202-217): the nearest
+// point with d2 <= r2, lowest original index on an exact tie. Returns the
+// sorted slot (or -1) and its squared distance; d2 = ((dx dx + dy dy) + dz dz).
+__device__ int nearest_within_sq(const CloudView &c, double qx, double qy, double qz, double r2,
+                                 double &best, uint32_t &status) {
+  best = r2;
+  int best_s = -1;
+  uint32_t best_i = MISS;
+  if (c.n == 0 || !(r2 >= 0.0)) return -1;
+  float qc[3] = {float(qx), float(qy), float(qz)};
+  auto bound2 = [&]() {
+    float b = __double2float_ru(best);
+    return b + 1e-5f * b + 1e-30f;
+  };
+  auto leaf = [&](int first, int count) {
+    for (int s = first; s < first + count; ++s) {
+      double4 p = ldg4(c.pts + s);
+      double dx = qx - p.x, dy = qy - p.y, dz = qz - p.z;
+      double d2 = (dx * dx + dy * dy) + dz * dz;
+      if (d2 > r2) continue;
+      uint32_t id = uint32_t(p.w);
+      if (best_s < 0 || d2 < best || (d2 == best && id < best_i)) {
+        best = d2;
+        best_s = s;
+        best_i = id;
+      }
+    }
+  };
+  if (c.root_leaf) {
+    leaf(0, c.root_leaf);
+    return best_s;
+  }
+  // Box distances are taken from the f32-rounded query; the padding of the
+  // boxes (>= the rounding of the query) keeps them lower bounds.
+  int stack_n[STACK];
+  float stack_k[STACK];
+  int sp = 0, node = 0;
+  uint32_t visits = 0;
+  for (;;) {
+    if (++visits > 2u * c.n + 64u) {
+      status |= ST_STACK;
+      break;
+    }
+    Child2 n = load_node(c.nodes, node);
+    float k[2] = {box_dist2(n.lo0, n.hi0, qc), box_dist2(n.lo1, n.hi1, qc)};
+    int near_c = k[1] < k[0] ? 1 : 0;
+    int next = -1;
+    for (int q = 0; q < 2; ++q) {
+      int ch = q == 0 ? near_c : 1 - near_c;
+      if (!(k[ch] <= bound2())) continue;
+      if (n.cnt[ch]) {
+        leaf(n.ref[ch], n.cnt[ch]);
+      } else if (next < 0) {
+        next = n.ref[ch];
+      } else if (sp < STACK) {
+        stack_n[sp] = n.ref[ch];
+        stack_k[sp++] = k[ch];
+      } else {
+        status |= ST_STACK;
+      }
+    }
+    if (next >= 0) {
+      node = next;
+      continue;
+    }
+    bool more = false;
+    while (sp > 0) {
+      --sp;
+      if (stack_k[sp] <= bound2()) {
+        node = stack_n[sp];
+        more = true;
+        break;
+      }
+    }
+    if (!more) break;
+  }
+  return best_s;
+}
+
+// PointTree::nearest_below (spatial/kdtree.rs:182-190): the unbounded nearest
+// point when sqrt(d2) < bound. Returns the sorted slot or -1.
+__device__ __forceinline__ int nearest_below(const CloudView &c, double qx, double qy, double qz,
+                                             double bound, double &dist, uint32_t &status) {
+  if (!(bound > 0.0)) return -1;
+  double widened = (bound * bound) * (1.0 + 4.0 * 2.220446049250313e-16);
+  double d2;
+  int s = nearest_within_sq(c, qx, qy, qz, widened, d2, status);
+  if (s < 0) return -1;
+  double d = sqrt(d2);
+  if (!(d < bound)) return -1;
+  dist = d;
+  return s;
+}
+
+}  // namespace sherd

@@ -1,0 +1,309 @@
+"""CUDA backend against the oracle on the reference's slab fixture (needs a B200).
+
+Contract: first hits, crossings, point-to-triangle distances, nearest neighbours, cone votes,
+thickness, every verification score and every verdict are bit-exact against the oracle under
+the shared tie rule; ICP poses (whose per-pass sums are reduced in a different order) agree
+within 1e-6 t of the oracle on every non-chaotic ladder, and within the reference's own D 10.2
+rows of the fixture.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from _slab import (CHAOTIC_SHARE, ROT_DEG, TRANS_T, VERIFY_TOL, oracle_pair, origin_t, piece,
+                   reference_scores, slab_params, trace_deg)
+
+pytestmark = pytest.mark.gpu
+
+SCORE_KEYS = ("tight_a", "tight_b", "tight", "gap_a", "gap_b", "gap", "contact_a", "contact_b",
+              "contact", "seam", "cont", "cont_n", "pen", "pen_depth")
+
+
+@pytest.fixture(scope="module")
+def gpu_slab(sherd, gpu_ctx, slab):
+    """Device meshes, surfaces, clouds and the pair of the slab, built once."""
+    out = {}
+    for name in ("pieceA", "pieceB"):
+        p = piece(slab, name)
+        mesh = gpu_ctx.mesh(p["V"], p["F"])
+        frac = mesh.subset(p["frac"])
+        surf = gpu_ctx.surfaces(frac, mesh, int(p["watertight"]), float(p["frac_area"]), p["Pf"],
+                                p["S"], p["brk_P"], p["brk_ns"], p["margin_p"], p["margin_n"])
+        out[name] = dict(mesh=mesh, frac=frac, surf=surf, arrays=p)
+    a, b = out["pieceA"], out["pieceB"]
+    reg_t = gpu_ctx.cloud(a["arrays"]["reg_p"], a["arrays"]["reg_n"])
+    frac_t = gpu_ctx.cloud(a["arrays"]["frac_p"], a["arrays"]["frac_n"])
+    scales = sherd.Scales(*[float(x) for x in slab["scales"]])
+    pair = gpu_ctx.pair(a["surf"], b["surf"], reg_t, frac_t, b["arrays"]["reg_p"],
+                        b["arrays"]["frac_p"], scales)
+    return dict(a=a, b=b, reg_t=reg_t, frac_t=frac_t, scales=scales, pair=pair)
+
+
+@pytest.fixture(scope="module")
+def cpu_slab(oracle, slab):
+    return oracle_pair(oracle, slab)
+
+
+def _rays(seed, n, lo, hi):
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(lo, hi, size=(n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return o, d.astype(np.float32)
+
+
+@pytest.mark.parametrize("name", ["pieceA", "pieceB"])
+def test_thickness_rays_are_bit_exact(sherd, gpu_ctx, oracle, slab, name):
+    p = piece(slab, name)
+    normals, _, cent = oracle.face_geometry(p["V0"], p["F"])
+    gn, ga, gc = gpu_ctx.face_geometry(p["V0"], p["F"])
+    assert np.array_equal(gn, normals) and np.array_equal(gc, cent)
+    mesh_c = oracle.Mesh(p["V0"], p["F"])
+    mesh_g = gpu_ctx.mesh(p["V0"], p["F"])
+    idx = oracle.face_indices(len(p["F"]))
+    t_c, prim_c = oracle.cast_inward_rays(mesh_c, cent, normals, idx)
+    res, t_g, prim_g = gpu_ctx.thickness(mesh_g, gc, gn, return_hits=True)
+    assert np.array_equal(prim_g, prim_c)
+    assert np.array_equal(t_g.view(np.uint32), t_c.view(np.uint32))
+    assert res == oracle.thickness_from_hits(normals, idx, t_c, prim_c)
+
+
+@pytest.mark.parametrize("name", ["pieceA", "pieceB"])
+def test_thickness_from_the_fixture_hits_on_the_device(gpu_ctx, oracle, slab, name):
+    p = piece(slab, name)
+    normals, _, _ = oracle.face_geometry(p["V0"], p["F"])
+    t, mode = gpu_ctx.thickness_from_hits(normals, p["thick_idx"], p["thick_t_hit"], p["thick_prim"])
+    assert t == p["thick_t"] and mode == p["thick_mode"]
+
+
+def test_random_first_hits_are_bit_exact(gpu_ctx, oracle, gpu_slab, cpu_slab):
+    p = gpu_slab["a"]["arrays"]
+    lo, hi = p["V"].min(0), p["V"].max(0)
+    o, d = _rays(7, 20000, lo - 5, hi + 5)
+    t_g, prim_g = gpu_ctx.first_hit(gpu_slab["a"]["mesh"], o, d)
+    t_c, prim_c = cpu_slab["a"]["mesh"].first_hit(o, d)
+    assert np.isfinite(t_g).sum() > 1000
+    assert np.array_equal(prim_g, prim_c)
+    assert np.array_equal(t_g.view(np.uint32), t_c.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["pieceA", "pieceB"])
+def test_cone_votes_are_bit_exact(gpu_ctx, oracle, slab, name):
+    p = piece(slab, name)
+    normals, _, cent = oracle.face_geometry(p["V"], p["F"])
+    good_c = oracle.cone_votes(oracle.Mesh(p["V"], p["F"]), cent, normals, p["seg_NS"], normals,
+                               float(p["thick_t"]))
+    good_g = gpu_ctx.cone_votes(gpu_ctx.mesh(p["V"], p["F"]), cent, normals, p["seg_NS"], normals,
+                                float(p["thick_t"]))
+    assert np.array_equal(good_g, good_c)
+
+
+@pytest.mark.parametrize("k", [1, 4, 0])
+def test_bounded_distance_is_bit_exact(sherd, gpu_ctx, gpu_slab, cpu_slab, slab, k):
+    pose = slab["s2_T_frac2"][k]
+    pts = gpu_slab["b"]["arrays"]["Pf"]
+    window = gpu_slab["scales"].facing
+    d_g = gpu_ctx.bounded_distance(gpu_slab["a"]["frac"], pts, pose, window)
+    d_c = cpu_slab["a"]["frac"].bounded_distance(pts, pose, window)
+    assert np.array_equal(d_g, d_c)
+    m_g = gpu_ctx.bounded_distance(gpu_slab["a"]["mesh"], pts, pose, 3.4e38, sherd.REDUCE_MIN)
+    m_c = cpu_slab["a"]["mesh"].bounded_distance(pts, pose, 3.4e38, 1)
+    assert np.array_equal(m_g, m_c)
+
+
+@pytest.mark.parametrize("k", [0, 1, 4])
+def test_inside_is_bit_exact(gpu_ctx, gpu_slab, cpu_slab, slab, k):
+    pose = slab["s2_T_frac2"][k]
+    pts = gpu_slab["b"]["arrays"]["S"]
+    d_g, in_g = gpu_ctx.inside(gpu_slab["a"]["mesh"], pts, pose)
+    d_c, in_c = cpu_slab["a"]["mesh"].inside(pts, pose)
+    assert np.array_equal(in_g, in_c)
+    assert np.array_equal(d_g.view(np.uint32), d_c.view(np.uint32))
+    if k == 0:
+        assert in_g.sum() > 0  # candidate 0 penetrates (the reference's pen = 0.0223)
+
+
+def test_nearest_neighbours_are_bit_exact(gpu_ctx, gpu_slab, cpu_slab, slab):
+    src = gpu_slab["b"]["arrays"]["reg_p"]
+    pose = slab["starts"][3]
+    q = src @ pose[:3, :3].T + pose[:3, 3]
+    sc = gpu_slab["scales"]
+    r = 0.2 * sc.t * sc.icp
+    i_g, d_g = gpu_slab["reg_t"].nearest_within_sq(q, r * r)
+    i_c, d_c = cpu_slab["reg_t"].nearest_within_sq(q, r * r)
+    assert (i_g != 0xFFFFFFFF).sum() > 100
+    assert np.array_equal(i_g, i_c) and np.array_equal(d_g, d_c)
+    j_g, e_g = gpu_slab["reg_t"].nearest_below(q, r)
+    j_c, e_c = cpu_slab["reg_t"].nearest_below(q, r)
+    assert np.array_equal(j_g, j_c) and np.array_equal(e_g, e_c)
+
+
+def test_nearest_neighbour_ties_go_to_the_lowest_index(gpu_ctx, oracle):
+    """kdtree.rs's mirrored-cloud ties (kdtree.rs:330-381): every query on x = 0 is equidistant
+    from a mirrored pair, and the lower index wins."""
+    rng = np.random.default_rng(3)
+    p = rng.uniform(-4, 4, size=(300, 3))
+    pts = np.empty((600, 3))
+    pts[0::2] = p
+    pts[1::2] = p * np.array([-1.0, 1.0, 1.0])
+    q = np.column_stack([np.zeros(400), rng.uniform(-4, 4, size=(400, 2))])
+    cg = gpu_ctx.cloud(pts)
+    cc = oracle.Cloud(pts)
+    i_g, d_g = cg.nearest_within_sq(q, 100.0)
+    i_c, d_c = cc.nearest_within_sq(q, 100.0)
+    assert np.array_equal(i_g, i_c) and np.array_equal(d_g, d_c)
+    assert np.all(i_g % 2 == 0)
+
+
+def test_icp_rungs_match_the_oracle(gpu_ctx, gpu_slab, cpu_slab, oracle, slab):
+    sc = gpu_slab["scales"]
+    src = gpu_slab["b"]["arrays"]["reg_p"]
+    starts = slab["starts"].reshape(-1, 16)
+    dist = 0.2 * sc.t * sc.icp
+    g = gpu_ctx.icp_rung(src, gpu_slab["reg_t"], starts, dist, 30)
+    c = oracle.icp_rung(src, cpu_slab["reg_t"], starts, dist, 30)
+    close = 0
+    for rg, rc in zip(g, c):
+        a, b = rg.pose(), np.array(rc.transform[:]).reshape(4, 4)
+        if origin_t(a, b, sc.t) < 1e-6 and trace_deg(a, b) < 1e-4:
+            close += 1
+            assert rg.correspondences == rc.correspondences
+    assert close >= 8, close
+
+
+def test_verification_is_bit_exact_against_the_oracle(sherd, gpu_ctx, gpu_slab, cpu_slab, oracle,
+                                                      slab):
+    params = slab_params(oracle, slab)
+    sparams = sherd.default_params()
+    for f in ("min_tight", "max_gap", "max_pen", "min_seam", "min_cont_n"):
+        setattr(sparams, f, getattr(params, f))
+    for k, pose in enumerate(slab["s2_T_frac2"]):
+        g = gpu_ctx.verify(gpu_slab["a"]["surf"], gpu_slab["b"]["surf"], pose, gpu_slab["scales"])
+        c = oracle.verify(cpu_slab["a"]["surf"], cpu_slab["b"]["surf"], pose, cpu_slab["scales"])
+        for key in SCORE_KEYS:
+            assert getattr(g, key) == getattr(c, key), (k, key, getattr(g, key), getattr(c, key))
+        assert sherd.accept(g, sparams, gpu_slab["scales"]) == bool(slab["s2_accepted"][k])
+        ref = reference_scores(slab, k)
+        for key, tol in VERIFY_TOL.items():
+            assert abs(getattr(g, key) - ref[key]) <= tol
+
+
+@pytest.mark.parametrize("sched", [0, 1])
+def test_batched_ladder_matches_oracle_and_reference(sherd, gpu_ctx, gpu_slab, cpu_slab, oracle,
+                                                     slab, sched):
+    params = slab_params(oracle, slab)
+    sparams = sherd.default_params()
+    for f in ("min_tight", "max_gap", "max_pen", "min_seam", "min_cont_n"):
+        setattr(sparams, f, getattr(params, f))
+    items = [(0, k, slab["starts"][k]) for k in range(len(slab["starts"]))]
+    cand_g = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items, sparams, sched)
+    witems = [oracle.WorkItem(0, k, (C.c_double * 16)(*slab["starts"][k].reshape(16)))
+              for k in range(len(items))]
+    cand_c, _ = oracle.ladder_verify_batch([cpu_slab["pair"]], witems, params)
+    t = gpu_slab["scales"].t
+    chaotic = []
+    for k in range(len(items)):
+        g, c = cand_g[k], cand_c[k]
+        assert g.status == 0 and g.start == k
+        assert g.accepted == c.accepted == int(slab["s2_accepted"][k])
+        for r, name in enumerate(("s2_T_reg1", "s2_T_reg2", "s2_T_frac1", "s2_T_frac2")):
+            mine = g.rungs[r].pose()
+            if trace_deg(mine, slab[name][k]) > ROT_DEG or origin_t(mine, slab[name][k], t) > TRANS_T:
+                chaotic.append(k)
+        a = g.rungs[3].pose()
+        b = np.array(c.rungs[3].transform[:]).reshape(4, 4)
+        if g.accepted:
+            assert origin_t(a, b, t) < 1e-4 and trace_deg(a, b) < np.degrees(1e-5)
+    assert len(set(chaotic)) <= CHAOTIC_SHARE * len(items)
+    assert not any(slab["s2_accepted"][k] for k in chaotic)
+
+
+def test_batched_path_is_deterministic(sherd, gpu_ctx, gpu_slab, slab):
+    items = [(0, k, slab["starts"][k]) for k in range(len(slab["starts"]))] * 3
+    p = sherd.default_params()
+    a = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items, p)
+    b = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items, p)
+    assert bytes(a) == bytes(b)
+
+
+def test_invalid_inputs_are_refused(sherd, gpu_ctx, gpu_slab):
+    bad = np.eye(4)
+    bad[0, 3] = np.nan
+    with pytest.raises(sherd.SherdError) as e:
+        gpu_ctx.bounded_distance(gpu_slab["a"]["mesh"], np.zeros((3, 3)), bad, 1.0)
+    assert e.value.code == -1
+    with pytest.raises(sherd.SherdError) as e:
+        gpu_ctx.mesh(np.zeros((3, 3)), np.zeros((0, 3)))
+    assert e.value.code == -6
+    with pytest.raises(sherd.SherdError):
+        gpu_ctx.cloud(np.zeros((0, 3)))
+    with pytest.raises(sherd.SherdError):
+        gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], [(3, 0, np.eye(4))], sherd.default_params())
+
+
+def test_empty_and_tiny_inputs(sherd, gpu_ctx, oracle):
+    tri_v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    tri_f = np.array([[0, 1, 2]], np.uint32)
+    m = gpu_ctx.mesh(tri_v, tri_f)
+    t, prim = gpu_ctx.first_hit(m, [[0.2, 0.2, 1.0]], [[0, 0, -1.0]])
+    assert prim[0] == 0 and t[0] == np.float32(1.0)
+    d = gpu_ctx.bounded_distance(m, np.zeros((0, 3)), np.eye(4), 1.0)
+    assert d.shape == (0,)
+    mn = gpu_ctx.bounded_distance(m, np.zeros((0, 3)), np.eye(4), 2.0, sherd.REDUCE_MIN)
+    assert mn[0] == 2.0
+    c = gpu_ctx.cloud([[1.0, 2.0, 3.0]])
+    i, d2 = c.nearest_within_sq([[1.0, 2.0, 3.5], [9.0, 9.0, 9.0]], 1.0)
+    assert list(i) == [0, 0xFFFFFFFF] and d2[0] == 0.25
+
+
+def test_box_mesh_known_answers(sherd, gpu_ctx):
+    """bvh.rs:255-279: first hits and misses on a box, from outside and inside."""
+    lo, hi = -1.0, 1.0
+    v = np.array([[lo, lo, lo], [hi, lo, lo], [hi, hi, lo], [lo, hi, lo], [lo, lo, hi], [hi, lo, hi],
+                  [hi, hi, hi], [lo, hi, hi]], np.float32)
+    f = np.array([[0, 2, 1], [0, 3, 2], [4, 5, 6], [4, 6, 7], [0, 1, 5], [0, 5, 4], [3, 7, 6],
+                  [3, 6, 2], [0, 4, 7], [0, 7, 3], [1, 2, 6], [1, 6, 5]], np.uint32)
+    m = gpu_ctx.mesh(v, f)
+    t, prim = gpu_ctx.first_hit(m, [[0, 0, 5], [0, 0, 0], [0, 0, 5]], [[0, 0, -1], [0, 0, -1], [0, 0, 1]])
+    assert abs(t[0] - 4.0) < 1e-5 and abs(t[1] - 1.0) < 1e-5 and prim[2] == 0xFFFFFFFF
+    d, inside = gpu_ctx.inside(m, [[0.1, 0.2, 0.3], [3.0, 0.0, 0.0]], np.eye(4))
+    assert list(inside) == [1, 0] and abs(d[0] - 0.7) < 1e-6
+
+
+def test_a_spent_time_budget_stops_the_batch_and_the_context_survives(sherd, gpu_ctx, gpu_slab,
+                                                                      slab):
+    items = [(0, k % 10, slab["starts"][k % 10]) for k in range(3000)]
+    gpu_ctx.set_timeout_ms(1)
+    try:
+        with pytest.raises(sherd.SherdError) as e:
+            gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items, sherd.default_params())
+        assert e.value.code == -3
+    finally:
+        gpu_ctx.set_timeout_ms(0)
+    out = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items[:10], sherd.default_params())
+    assert out[1].accepted == 1
+
+
+def test_abort_reaches_a_running_batch(sherd, gpu_ctx, gpu_slab, slab):
+    items = [(0, k % 10, slab["starts"][k % 10]) for k in range(20000)]
+
+    def later():
+        time.sleep(0.3)
+        gpu_ctx.abort()
+
+    th = threading.Thread(target=later)
+    th.start()
+    try:
+        with pytest.raises(sherd.SherdError) as e:
+            gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items, sherd.default_params())
+        assert e.value.code == -4
+    finally:
+        th.join()
+    out = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items[:10], sherd.default_params())
+    assert out[4].accepted == 1
