@@ -1,0 +1,339 @@
+"""Pair-pose verifications/s of the batched stage-2 path (4-rung point-to-plane ICP ladder +
+R 6 verification + R 6.5 verdict per (pair, start)) on a B200.
+
+Workload (default): the 40-fragment collection of three synthetic pots (t = 5, 8, 12), all
+780 pairs x 128 ladder starts = 99 840 verifications per step, generated seeded (synth.py).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config collection] [--impl cuda]
+
+Printed by rank 0: one JSON line with `value` (device throughput with every input resident in
+HBM, CUDA events around the batch's graph on the library's stream, max over ranks), `e2e`
+(the same metric through the host-buffer C-ABI call sherd_ladder_verify_batch, the work items
+copied in and the candidates copied out every step), the roofline of the dominant kernel,
+the clocks seen during the timed region and the oracle's CPU baseline on a bounded sample.
+`--impl reference` times the reference algorithm's CPU restatement (the oracle; the Rust
+reference cannot be built here) on all host cores instead.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "pair-pose verifications/s"
+UNIT = "verifications/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def _pkg(name=""):
+    return importlib.import_module("sherd-refit_b200" + (("." + name) if name else ""))
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _max_over_ranks(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(wl, seconds, params_fn):
+    """The oracle (reference algorithm, f64, all host threads) on a bounded, deterministic
+    sample of the workload's items: returns (verifications/s, threads, sample description)."""
+    oracle = importlib.import_module("oracle")
+    workload = _pkg("workload")
+    pairs, keep = oracle.collection(wl)
+    pair, start, inits = workload.item_arrays(wl)
+    n = len(pair)
+    params = oracle.default_params()
+    threads = oracle.lib().or_default_threads()
+
+    def run(k):
+        idx = np.linspace(0, n - 1, k).round().astype(np.int64)
+        items = oracle.work_items_from(pair[idx], start[idx], inits[idx])
+        t0 = time.perf_counter()
+        oracle.ladder_verify_items(pairs, items, params, 0)
+        return time.perf_counter() - t0
+
+    k = max(threads, 8)
+    dt = run(k)
+    while dt < 0.5 * seconds and k < 4096:
+        k = min(4096, int(k * max(2.0, 0.5 * seconds / max(dt, 1e-3))))
+        dt = run(k)
+    sample = (f"{k} of the {n} (pair, start) items, evenly spaced over the pair-major item "
+              f"list, on {threads} threads, {dt:.1f} s")
+    return k / dt, threads, sample
+
+
+def run_reference(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    synth = _pkg("synth")
+    wl = synth.make(args.config, args.seed)
+    oracle = importlib.import_module("oracle")
+    workload = _pkg("workload")
+    pairs, keep = oracle.collection(wl)
+    pair, start, inits = workload.item_arrays(wl)
+    n = len(pair)
+    params = oracle.default_params()
+    threads = oracle.lib().or_default_threads()
+    per_step = args.reference_items or max(threads * 2, 16)
+    rng = np.random.default_rng(args.seed)
+    times = []
+    for step in range(args.warmup + args.steps):
+        idx = np.sort(rng.choice(n, per_step, replace=False))
+        items = oracle.work_items_from(pair[idx], start[idx], inits[idx])
+        t0 = time.perf_counter()
+        oracle.ladder_verify_items(pairs, items, params, 0)
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(dt)
+    value = per_step * len(times) / sum(times)
+    sample = (f"{per_step} random (pair, start) items per step (seed {args.seed}) of the "
+              f"{n}-item workload, {threads} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(times)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": _config_dict(wl, args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("the reference's Rust CPU backend cannot be built in this image (no cargo); "
+                 "this is its C++ restatement (oracle/oracle.cpp), pinned to the reference's "
+                 "fixture to 1e-14 t, f64 point loops as the reference's Numerics::REFERENCE"),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _config_dict(wl, args, extra=None):
+    d = wl.describe()
+    cfg = {"workload": f"{args.config}: {d['fragments']} fragments, {d['pairs']} pairs x "
+                       f"{d['starts_per_pair']} starts = {d['items']} (pair, start) items",
+           **d, "sched": args.sched}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=("cuda", "reference"))
+    ap.add_argument("--config", default="collection")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--sched", default="batched", choices=("batched", "plain"))
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--reference-items", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    world, rank, local = _dist()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(local)
+    sherd = _pkg()
+    synth = _pkg("synth")
+    workload = _pkg("workload")
+    t_gen = time.perf_counter()
+    wl = synth.make(args.config, args.seed)
+    t_gen = time.perf_counter() - t_gen
+    ctx = sherd.Context(local)
+    params = sherd.default_params()
+    t_up = time.perf_counter()
+    dev = workload.to_device(ctx, wl, params)
+    t_up = time.perf_counter() - t_up
+    sched = sherd.SCHED_BATCHED if args.sched == "batched" else sherd.SCHED_PLAIN
+    batch = ctx.batch(dev.pairs, dev.items, params, sched)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(args.warmup):
+        batch.run()
+
+    sampler = ClockSampler(local)
+    _barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    ladder_ms, verify_ms, total_ms = [], [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        l, v, t = batch.run()
+        ladder_ms.append(l)
+        verify_ms.append(v)
+        total_ms.append(t)
+    torch.cuda.synchronize()
+    _barrier(world)
+    clocks = sampler.stop()
+    step_ms = _max_over_ranks(world, float(np.mean(total_ms)))
+    n_items = dev.n_items
+    value = world * n_items / (step_ms / 1000.0)
+
+    cands = sherd.candidates(batch.results())
+    icp_bytes, ver_bytes = workload.algorithmic_bytes(wl, cands, dev.n_src)
+    accepted = int(cands["accepted"].sum())
+    status_bad = int((cands["status"] != 0).sum())
+
+    # End to end through the host-buffer C-ABI call: work items in, candidates out.
+    e2e_ms = []
+    for k in range(args.e2e_steps + 1):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = ctx.ladder_verify_batch(dev.pairs, dev.items, params, sched)
+        t1 = time.perf_counter()
+        if k:
+            e2e_ms.append(1000 * (t1 - t0))
+    e2e_step = _max_over_ranks(world, float(np.mean(e2e_ms)))
+    h2d = n_items * sherd.WORK_ITEM.itemsize
+    d2h = n_items * sherd.CANDIDATE.itemsize
+    same = bytes(out) == bytes(batch.results())
+
+    peak, peak_kind = _peaks()
+    l_ms = float(np.mean(ladder_ms))
+    v_ms = float(np.mean(verify_ms))
+    dominant = "k_ladder" if l_ms >= v_ms else "k_verify_items"
+    bytes_dom = icp_bytes if dominant == "k_ladder" else ver_bytes
+    ms_dom = l_ms if dominant == "k_ladder" else v_ms
+    achieved = bytes_dom / (ms_dom / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "kernel": dominant,
+                "peak_source": peak_kind,
+                "per_unit": ("48 B per ICP point-iteration (16 B source point + 32 B matched "
+                             "target point and normal), over the passes each rung ran"
+                             if dominant == "k_ladder" else
+                             "24 B per verification query"),
+                "ladder_ms": l_ms, "verify_ms": v_ms,
+                "verify_gbs": ver_bytes / (v_ms / 1000.0) / 1e9 if v_ms > 0 else None}
+
+    if rank != 0:
+        ctx.close()
+        return
+    cpu = None
+    if not args.no_cpu:
+        v_cpu, threads, sample = cpu_baseline(wl, args.cpu_seconds, None)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, sherd-refit_b200/synth.py)",
+        "config": _config_dict(wl, args, {
+            "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MB write); the resident "
+                  "fragment data also exceeds L2",
+            "accepted": accepted, "item_errors": status_bad,
+            "generate_s": round(t_gen, 1), "upload_s": round(t_up, 1)}),
+        "e2e": {"value": world * n_items / (e2e_step / 1000.0), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "timer": "host wall clock around the synchronous C-ABI call",
+                "matches_resident_run": same},
+        "gpu_launches": 2 * args.steps,
+        "roofline": roofline,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

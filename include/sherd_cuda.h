@@ -131,6 +131,7 @@ typedef struct sherd_mesh sherd_mesh;         /* triangle LBVH, f32       */
 typedef struct sherd_cloud sherd_cloud;       /* point LBVH, f64 + normals */
 typedef struct sherd_surfaces sherd_surfaces; /* one fragment as R 6 reads it */
 typedef struct sherd_pair sherd_pair;         /* two fragments + ladder clouds */
+typedef struct sherd_batch sherd_batch;       /* a device-resident stage-2 batch */
 
 /* ---- context ----------------------------------------------------------- */
 
@@ -309,6 +310,24 @@ int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs,
                               uint32_t n_pairs, const sherd_work_item *items,
                               uint32_t n_items, const sherd_params *p, int sched,
                               sherd_candidate *out);
+
+/* A stage-2 batch made resident on the device: the pair views, work items,
+ * queue order, candidate records and per-CTA scratch are uploaded and sized
+ * once, and SHERD_SCHED_BATCHED captures the queue reset and the two
+ * persistent kernels (ladder, verification) as one CUDA graph. Running it
+ * again recomputes every candidate from the same resident inputs. This is the
+ * device-side form of sherd_ladder_verify_batch, for callers that keep their
+ * inputs on the GPU between calls. */
+int sherd_batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
+                       const sherd_work_item *items, uint32_t n_items,
+                       const sherd_params *p, int sched, sherd_batch **out);
+/* Launches the batch and waits for it; the device milliseconds of the ladder
+ * kernel, the verification kernel and both together are written to ms[0..2]
+ * (CUDA events on the context's stream). */
+int sherd_batch_run(sherd_batch *batch, float ms[3]);
+/* Copies the candidates of the last run to the host (n_items records). */
+int sherd_batch_results(sherd_batch *batch, sherd_candidate *out);
+int sherd_batch_free(sherd_batch *batch);
 
 #ifdef __cplusplus
 }

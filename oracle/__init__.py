@@ -354,3 +354,60 @@ def default_params() -> Params:
                   icp_delta=0.04, coarse_res=2.3, stage1_res=0.9, tight_res=0.15,
                   facing_res=1.0, gap_res=0.45, seam_res=1.8, near_res=4.0, pen_res=0.9,
                   icp_res=0.6)
+
+
+def collection(wl, params=None):
+    """The oracle's objects for a synthetic collection (the package's synth.Workload), built the
+    way the CUDA backend's workload.to_device builds its own: returns (pairs, keepalive)."""
+    params = params or default_params()
+    keep = []
+    surfaces, reg_t, frac_t = [], [], []
+    for fr in wl.fragments:
+        m = Mesh(fr.v, fr.f)
+        fm = m.subset(fr.frac)
+        s = Surfaces(fm, m, True, fr.frac_area, fr.pf, fr.s, fr.brk_p, fr.brk_ns, fr.margin_p,
+                     fr.margin_n)
+        keep += [m, fm]
+        surfaces.append(s)
+        reg_t.append(Cloud(fr.reg_p, fr.reg_n))
+        frac_t.append(Cloud(fr.pf, fr.pf_n))
+    pairs = []
+    for p in wl.pairs:
+        a, b = wl.fragments[p.a], wl.fragments[p.b]
+        sc = scales_for(params, min(a.t, b.t), max(a.res, b.res))
+        pairs.append(Pair(surfaces[p.a], surfaces[p.b], reg_t[p.a], frac_t[p.a], b.reg_p, b.pf, sc))
+    return pairs, (keep, surfaces, reg_t, frac_t)
+
+
+def scales_for(params: Params, t: float, res: float) -> Scales:
+    """Scales::for_pair (matching/scales.rs:72-88)."""
+    def f(k, m):
+        return max(k * t, m * res)
+    return Scales(t=t, res=res, coarse=f(params.coarse_delta, params.coarse_res),
+                  stage1=f(params.stage1_delta, params.stage1_res),
+                  tight=f(params.tight_delta, params.tight_res),
+                  facing=f(params.facing_delta, params.facing_res),
+                  gap=f(params.max_gap, params.gap_res), seam=f(params.seam_delta, params.seam_res),
+                  near=f(params.near_delta, params.near_res), pen=f(params.pen_delta, params.pen_res),
+                  nms=params.nms_delta * t,
+                  icp=f(params.icp_delta, params.icp_res) / (params.icp_delta * t))
+
+
+def work_items_from(pair, start, inits):
+    """A WorkItem array from aligned numpy arrays."""
+    n = len(pair)
+    arr = (WorkItem * max(n, 1))()
+    view = np.ctypeslib.as_array(arr)[:n]
+    view["pair"] = pair
+    view["start"] = start
+    view["init"] = np.asarray(inits, np.float64).reshape(n, 16)
+    return arr
+
+
+def ladder_verify_items(pairs, items, params: Params, threads=0):
+    """or_ladder_verify_batch over a prepared WorkItem array: (Candidate array, threads used)."""
+    arr = (C.c_void_p * len(pairs))(*[p.h for p in pairs])
+    out = (Candidate * len(items))()
+    used = lib().or_ladder_verify_batch(arr, len(pairs), C.cast(items, C.c_void_p), len(items),
+                                        C.byref(params), threads, C.cast(out, C.c_void_p))
+    return out, used

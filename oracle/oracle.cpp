@@ -285,11 +285,12 @@ struct Mesh {
     return id;
   }
 
-  // Entry parameter of the ray into the padded box, or +inf when it misses.
+  // Entry parameter of the ray into the padded box (twice the padding, so it
+  // also holds every face rectangle of crossings()), or +inf when it misses.
   double ray_box(const TriNode &n, const double *o, const double *invd) const {
     double t0 = 0.0, t1 = D_INF;
     for (int a = 0; a < 3; ++a) {
-      double l = double(n.lo[a]) - pad, h = double(n.hi[a]) + pad;
+      double l = double(n.lo[a]) - 2.0 * pad, h = double(n.hi[a]) + 2.0 * pad;
       if (std::isinf(invd[a])) {
         if (o[a] < l || o[a] > h) return D_INF;
         continue;
@@ -351,9 +352,39 @@ struct Mesh {
     *prim_out = bi;
   }
 
-  // RayScene::crossings (bvh.rs:160-175): every face the ray crosses.
+  // RayScene::crossings (bvh.rs:160-175) along a coordinate axis: the faces
+  // whose projected rectangle, padded outward by the mesh padding in f32 with
+  // directed rounding, holds the origin's projection and that Moller-Trumbore
+  // reports crossed (the rule the CUDA backend's axis grids implement).
   uint32_t crossings(V3f o, V3f d) const {
     if (nodes.empty()) return 0;
+    int axis = d.x != 0.0f ? 0 : (d.y != 0.0f ? 1 : 2);
+    int au = (axis + 1) % 3, av = (axis + 2) % 3;
+    float oc[3] = {o.x, o.y, o.z};
+    float padf = float(pad);
+    auto rd = [](float a, float b) {  // a - b rounded toward -inf
+      float r = a - b;
+      if (double(r) > double(a) - double(b)) r = std::nextafter(r, -F_INF);
+      return r;
+    };
+    auto ru = [](float a, float b) {  // a + b rounded toward +inf
+      float r = a + b;
+      if (double(r) < double(a) + double(b)) r = std::nextafter(r, F_INF);
+      return r;
+    };
+    auto in_rect = [&](uint32_t face) {
+      float lo_u = F_INF, hi_u = -F_INF, lo_v = F_INF, hi_v = -F_INF;
+      for (int k = 0; k < 3; ++k) {
+        V3f p = vert(face, k);
+        float c[3] = {p.x, p.y, p.z};
+        lo_u = std::min(lo_u, c[au]);
+        hi_u = std::max(hi_u, c[au]);
+        lo_v = std::min(lo_v, c[av]);
+        hi_v = std::max(hi_v, c[av]);
+      }
+      return !(oc[au] < rd(lo_u, padf) || oc[au] > ru(hi_u, padf) || oc[av] < rd(lo_v, padf) ||
+               oc[av] > ru(hi_v, padf));
+    };
     double od[3] = {o.x, o.y, o.z}, invd[3] = {1.0 / d.x, 1.0 / d.y, 1.0 / d.z};
     uint32_t hits = 0;
     int stack[128];
@@ -365,6 +396,7 @@ struct Mesh {
       if (n.left < 0) {
         for (uint32_t i = n.first; i < n.first + n.count; ++i) {
           uint32_t face = order[i];
+          if (!in_rect(face)) continue;
           if (moller_trumbore(o, d, vert(face, 0), vert(face, 1), vert(face, 2)) >= 0.0f) ++hits;
         }
       } else {

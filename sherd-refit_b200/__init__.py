@@ -10,11 +10,13 @@ verification and the batched persistent stage-2 path, plus the differentiable po
 from ._abi import (Candidate, IcpOptions, InsideOutcome, Params, Registration, Scales, Scores,
                    SherdError, WorkItem, REDUCE_ALL, REDUCE_MIN, SCHED_BATCHED, SCHED_PLAIN,
                    exported_symbols, lib)
-from .backend import (Cloud, Context, CudaExecutor, DistBatch, IcpBatch, InsideBatch, Mesh, Pair,
-                      Surfaces, accept, default_params, scales_for_pair, work_items)
+from .backend import (CANDIDATE, WORK_ITEM, Batch, Cloud, Context, CudaExecutor, DistBatch,
+                      IcpBatch, InsideBatch, Mesh, Pair, Surfaces, accept, candidates,
+                      default_params, scales_for_pair, work_item_array, work_items)
 
 __all__ = [
-    "Candidate", "Cloud", "Context", "CudaExecutor", "DistBatch", "IcpBatch", "IcpOptions",
+    "Batch", "CANDIDATE", "WORK_ITEM", "candidates", "work_item_array", "Candidate", "Cloud",
+    "Context", "CudaExecutor", "DistBatch", "IcpBatch", "IcpOptions",
     "InsideBatch", "InsideOutcome", "Mesh", "Pair", "Params", "Registration", "Scales", "Scores",
     "SherdError", "Surfaces", "WorkItem", "REDUCE_ALL", "REDUCE_MIN", "SCHED_BATCHED",
     "SCHED_PLAIN", "accept", "default_params", "exported_symbols", "lib", "scales_for_pair",

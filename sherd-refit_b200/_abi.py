@@ -143,6 +143,11 @@ _SIGNATURES = {
     "sherd_pair_free": (C.c_int, [VP]),
     "sherd_ladder_verify_batch": (C.c_int, [VP, VP, C.c_uint32, VP, C.c_uint32,
                                             C.POINTER(Params), C.c_int, VP]),
+    "sherd_batch_create": (C.c_int, [VP, VP, C.c_uint32, VP, C.c_uint32, C.POINTER(Params),
+                                     C.c_int, C.POINTER(VP)]),
+    "sherd_batch_run": (C.c_int, [VP, np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")]),
+    "sherd_batch_results": (C.c_int, [VP, VP]),
+    "sherd_batch_free": (C.c_int, [VP]),
 }
 
 

@@ -35,6 +35,19 @@ def _pose(t) -> np.ndarray:
     return _f64(t, (16,))
 
 
+class _Handle:
+    _free = ""
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                getattr(A.lib(), self._free)(h)
+            except Exception:
+                pass
+            self.h = None
+
+
 def default_params() -> A.Params:
     """Params::default (params.rs:141-190), the fields the C ABI reads."""
     p = A.Params()
@@ -205,6 +218,9 @@ class Context:
              reg_source, frac_source, scales: A.Scales) -> "Pair":
         return Pair(self, a, b, reg_target, frac_target, reg_source, frac_source, scales)
 
+    def batch(self, pairs, items, params: A.Params, sched=A.SCHED_BATCHED) -> "Batch":
+        return Batch(self, pairs, items, params, sched)
+
     def ladder_verify_batch(self, pairs, items, params: A.Params, sched=A.SCHED_BATCHED):
         """R 5.6 + R 6 + R 6.5 for every (pair, start); `items` is a ctypes WorkItem array or a
         list of (pair, start, init 4x4) tuples. Returns the ctypes Candidate array."""
@@ -219,27 +235,60 @@ class Context:
         return out
 
 
+WORK_ITEM = np.dtype(A.WorkItem)
+CANDIDATE = np.dtype(A.Candidate)
+
+
 def work_items(items) -> C.Array:
     """(pair index, start id, 4x4 init) tuples as the C ABI's work-item array."""
-    arr = (A.WorkItem * max(len(items), 1))()
-    for k, (p, s, t) in enumerate(items):
-        arr[k].pair = int(p)
-        arr[k].start = int(s)
-        arr[k].init[:] = [float(x) for x in _pose(t)]
+    pair = np.array([int(p) for p, _, _ in items], np.uint32)
+    start = np.array([int(s) for _, s, _ in items], np.uint32)
+    inits = np.array([_pose(t) for _, _, t in items], np.float64).reshape(-1, 16)
+    return work_item_array(pair, start, inits)
+
+
+def work_item_array(pair, start, inits) -> C.Array:
+    """The work-item array from three aligned numpy arrays (vectorised)."""
+    n = len(pair)
+    arr = (A.WorkItem * max(n, 1))()
+    view = np.ctypeslib.as_array(arr)[:n]
+    view["pair"] = pair
+    view["start"] = start
+    view["init"] = np.asarray(inits, np.float64).reshape(n, 16)
     return arr
 
 
-class _Handle:
-    _free = ""
+def candidates(arr) -> np.ndarray:
+    """A structured numpy view of a Candidate array (fields as in sherd_candidate)."""
+    return np.ctypeslib.as_array(arr)
 
-    def __del__(self):
-        h = getattr(self, "h", None)
-        if h:
-            try:
-                getattr(A.lib(), self._free)(h)
-            except Exception:
-                pass
-            self.h = None
+
+class Batch(_Handle):
+    """A device-resident stage-2 batch (sherd_batch_*): upload once, run many times."""
+    _free = "sherd_batch_free"
+
+    def __init__(self, ctx: Context, pairs, items, params: A.Params, sched=A.SCHED_BATCHED):
+        self.ctx = ctx
+        self.keep = list(pairs)
+        if not isinstance(items, C.Array):
+            items = work_items(items)
+        self.n = len(items)
+        arr = (C.c_void_p * max(len(pairs), 1))(*[p.h for p in pairs])
+        h = C.c_void_p()
+        check(ctx.h, A.lib().sherd_batch_create(ctx.h, arr, len(pairs), C.cast(items, C.c_void_p),
+                                               self.n, C.byref(params), int(sched), C.byref(h)))
+        self.h = h
+
+    def run(self):
+        """Runs the batch; returns (ladder ms, verification ms, total ms) of device time."""
+        ms = np.zeros(3, np.float32)
+        check(self.ctx.h, A.lib().sherd_batch_run(self.h, ms))
+        return tuple(float(x) for x in ms)
+
+    def results(self):
+        out = (A.Candidate * self.n)()
+        check(self.ctx.h, A.lib().sherd_batch_results(self.h, C.cast(out, C.c_void_p)))
+        return out
 
 
 class Mesh(_Handle):

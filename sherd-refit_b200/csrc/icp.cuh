@@ -20,7 +20,7 @@
 
 namespace sherd {
 
-constexpr int ICP_BLOCK = 256;
+constexpr int ICP_BLOCK = 128;
 constexpr int ICP_SUMS = 29;  // count, err2, jtj[21], jtr[6]
 
 struct IcpShared {
@@ -146,9 +146,11 @@ __device__ void plane_update(const double *s, bool has_normals, double u[16]) {
 }
 
 // One correspondence pass (icp::correspondences + icp::normal_equations) over
-// `src` under the pose sh.t; leaves the block totals in sh.sums.
+// `src` under the pose sh.t; leaves the block totals in sh.sums. `hint[i]`
+// carries each source point's last match (a target slot, or -1) from pass to
+// pass as the warm start of its search.
 __device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, double r2,
-                         bool valid, IcpShared &sh, uint32_t &status) {
+                         bool valid, IcpShared &sh, int *hint, uint32_t &status) {
   double acc[ICP_SUMS];
 #pragma unroll
   for (int k = 0; k < ICP_SUMS; ++k) acc[k] = 0.0;
@@ -161,7 +163,8 @@ __device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, 
       double x, y, z;
       apply_pose(t, p.x, p.y, p.z, x, y, z);
       double d2;
-      int s = nearest_within_sq(tgt, x, y, z, r2, d2, status);
+      int s = nearest_within_sq(tgt, x, y, z, r2, d2, status, hint[i]);
+      hint[i] = s;
       if (s < 0 || !(d2 < r2)) continue;
       acc[0] += 1.0;
       acc[1] += d2;
@@ -212,7 +215,7 @@ __device__ __forceinline__ void fit_rmse(const double *s, uint32_t ns, double &f
 // block calls it. On return sh.t holds the refined pose and thread 0 has
 // written *out.
 __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView &tgt,
-                               double distance, int max_iter, IcpShared &sh,
+                               double distance, int max_iter, IcpShared &sh, int *hint,
                                sherd_registration *out, uint32_t &status) {
   if (ns == 0 || tgt.n == 0) {
     if (threadIdx.x == 0) {
@@ -228,7 +231,8 @@ __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView 
   }
   bool valid = distance > 0.0;  // a NaN radius is not valid either
   double r2 = distance * distance;
-  icp_pass(src, ns, tgt, r2, valid, sh, status);
+  for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) hint[i] = -1;
+  icp_pass(src, ns, tgt, r2, valid, sh, hint, status);
   double fit, rmse;
   fit_rmse(sh.sums, ns, fit, rmse);
   uint32_t iterations = 0;
@@ -240,7 +244,7 @@ __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView 
       matmul4(u, sh.t, sh.t);
     }
     __syncthreads();
-    icp_pass(src, ns, tgt, r2, valid, sh, status);
+    icp_pass(src, ns, tgt, r2, valid, sh, hint, status);
     ++iterations;
     double nfit, nrmse;
     fit_rmse(sh.sums, ns, nfit, nrmse);

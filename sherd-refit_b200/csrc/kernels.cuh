@@ -268,16 +268,16 @@ __global__ void k_cone_votes(MeshView m, const double *centroids, const double *
 // ---- ICP -----------------------------------------------------------------------
 
 // Executor::icp_rung: one block per candidate.
-__global__ void __launch_bounds__(ICP_BLOCK) k_icp_rung(const double4 *src, uint32_t ns,
+__global__ void __launch_bounds__(ICP_BLOCK, 4) k_icp_rung(const double4 *src, uint32_t ns,
                                                         CloudView tgt, const double *inits,
-                                                        sherd_icp_options opt,
+                                                        sherd_icp_options opt, int *hints,
                                                         sherd_registration *out, uint32_t *status) {
   __shared__ IcpShared sh;
   uint32_t st = 0;
   if (threadIdx.x < 16) sh.t[threadIdx.x] = inits[16 * blockIdx.x + threadIdx.x];
   __syncthreads();
   icp_rung_block(src, ns, tgt, opt.max_correspondence_distance, opt.max_iteration, sh,
-                 out + blockIdx.x, st);
+                 hints + size_t(ns) * blockIdx.x, out + blockIdx.x, st);
   if (st) atomicOr(status, st);
 }
 
@@ -315,11 +315,13 @@ __device__ __forceinline__ bool take(const QueueCtl &q, unsigned long long start
 }
 
 // R 5.6's four point-to-plane rungs per (pair, start) (ladder.rs:142-161).
-__global__ void __launch_bounds__(ICP_BLOCK) k_ladder(const PairView *pairs,
+__global__ void __launch_bounds__(ICP_BLOCK, 4) k_ladder(const PairView *pairs,
                                                       const sherd_work_item *items, QueueCtl q,
+                                                      int *hints, size_t hint_stride,
                                                       sherd_candidate *out, uint32_t *status) {
   __shared__ IcpShared sh;
   uint32_t st = 0;
+  int *hint = hints + hint_stride * blockIdx.x;
   unsigned long long start = global_ns();
   unsigned it;
   while (take(q, start, it, st)) {
@@ -336,16 +338,17 @@ __global__ void __launch_bounds__(ICP_BLOCK) k_ladder(const PairView *pairs,
     for (int r = 0; r < 4; ++r) {
       double distance = k[r] * pr.sc.t * pr.sc.icp;
       if (r < 2)
-        icp_rung_block(pr.reg_src, pr.n_reg, pr.reg_tgt, distance, 30, sh, &c->rungs[r], st);
+        icp_rung_block(pr.reg_src, pr.n_reg, pr.reg_tgt, distance, 30, sh, hint, &c->rungs[r], st);
       else
-        icp_rung_block(pr.frac_src, pr.n_frac, pr.frac_tgt, distance, 30, sh, &c->rungs[r], st);
+        icp_rung_block(pr.frac_src, pr.n_frac, pr.frac_tgt, distance, 30, sh, hint, &c->rungs[r],
+                       st);
     }
   }
-  if (threadIdx.x == 0 && st) atomicOr(status, st);
+  if (st) atomicOr(status, st);
 }
 
 // R 6 + R 6.5 at each item's last rung pose (verify.rs:590-638).
-__global__ void __launch_bounds__(VER_BLOCK) k_verify_items(const PairView *pairs,
+__global__ void __launch_bounds__(VER_BLOCK, 3) k_verify_items(const PairView *pairs,
                                                             const sherd_work_item *items,
                                                             QueueCtl q, sherd_params p,
                                                             unsigned *scratch, size_t stride,

@@ -27,6 +27,17 @@ struct __align__(16) BNode {
   int4 d;    // ref0 ref1 cnt0 cnt1  (cnt > 0: leaf range at ref; cnt == 0: node ref)
 };
 
+// The crossing grid of one axis: the mesh projected onto the plane of the other
+// two axes (u, v) = ((a+1)%3, (a+2)%3), cut into square cells; each cell lists
+// (CSR) the sorted slots of every face whose padded projected rectangle
+// touches it. An axis ray from p can only cross faces in p's own cell.
+struct AxisGrid {
+  const uint32_t *start;  // nu * nv + 1 offsets
+  const uint32_t *slot;   // face slots
+  float lo_u, lo_v, inv_cell;
+  uint32_t nu, nv;
+};
+
 // What the traversal kernels take by value.
 struct MeshView {
   const BNode *nodes;
@@ -35,6 +46,7 @@ struct MeshView {
   uint32_t root_leaf;  // nf when the whole mesh is one leaf, else 0
   float pad;           // outward padding of every node box
   float lo[3], hi[3];  // exact vertex box (RayScene::aabb)
+  AxisGrid grid[3];    // crossing grids for the +x, +y, +z parity rays
 };
 
 struct CloudView {
@@ -305,6 +317,50 @@ __global__ void k_emit(const float *v, const uint32_t *f, const double *p, const
   nd.c = make_float4(bx[1].lo[2], bx[1].hi[0], bx[1].hi[1], bx[1].hi[2]);
   nd.d = make_int4(ref[0], ref[1], cnt[0], cnt[1]);
   nodes[i] = nd;
+}
+
+// ---- crossing grids ---------------------------------------------------------
+
+__device__ __forceinline__ void grid_rect(const float4 *tri, uint32_t s, int axis, const AxisGrid &g,
+                                          float pad, int &u0, int &u1, int &v0, int &v1) {
+  int au = (axis + 1) % 3, av = (axis + 2) % 3;
+  float umin = f_inf(), umax = -f_inf(), vmin = f_inf(), vmax = -f_inf();
+  for (int k = 0; k < 3; ++k) {
+    float4 p = tri[3 * s + k];
+    float c[3] = {p.x, p.y, p.z};
+    umin = fminf(umin, c[au]);
+    umax = fmaxf(umax, c[au]);
+    vmin = fminf(vmin, c[av]);
+    vmax = fmaxf(vmax, c[av]);
+  }
+  u0 = int(floorf((__fsub_rd(umin, pad) - g.lo_u) * g.inv_cell));
+  u1 = int(floorf((__fadd_ru(umax, pad) - g.lo_u) * g.inv_cell));
+  v0 = int(floorf((__fsub_rd(vmin, pad) - g.lo_v) * g.inv_cell));
+  v1 = int(floorf((__fadd_ru(vmax, pad) - g.lo_v) * g.inv_cell));
+  u0 = max(u0, 0);
+  v0 = max(v0, 0);
+  u1 = min(u1, int(g.nu) - 1);
+  v1 = min(v1, int(g.nv) - 1);
+}
+
+__global__ void k_grid_count(const float4 *tri, uint32_t nf, int axis, AxisGrid g, float pad,
+                             unsigned *count) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nf) return;
+  int u0, u1, v0, v1;
+  grid_rect(tri, s, axis, g, pad, u0, u1, v0, v1);
+  for (int u = u0; u <= u1; ++u)
+    for (int v = v0; v <= v1; ++v) atomicAdd(&count[size_t(u) * g.nv + v], 1u);
+}
+
+__global__ void k_grid_fill(const float4 *tri, uint32_t nf, int axis, AxisGrid g, float pad,
+                            unsigned *cursor, uint32_t *slot) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nf) return;
+  int u0, u1, v0, v1;
+  grid_rect(tri, s, axis, g, pad, u0, u1, v0, v1);
+  for (int u = u0; u <= u1; ++u)
+    for (int v = v0; v <= v1; ++v) slot[atomicAdd(&cursor[size_t(u) * g.nv + v], 1u)] = s;
 }
 
 __global__ void k_store_tris(const float *v, const uint32_t *f, const uint32_t *sorted, uint32_t nf,

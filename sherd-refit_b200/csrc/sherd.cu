@@ -8,6 +8,7 @@
 // result on the host; a CUDA failure is an error status, never a fallback.
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <array>
@@ -155,6 +156,7 @@ struct sherd_mesh {
   std::vector<uint32_t> hf;  // host copy of the faces
   DBuf<BNode> nodes;
   DBuf<float4> tri;
+  DBuf<uint32_t> gstart[3], gslot[3];
   MeshView view{};
 };
 
@@ -169,8 +171,8 @@ struct sherd_surfaces {
   sherd_ctx *ctx = nullptr;
   const sherd_mesh *fracture = nullptr, *mesh = nullptr;
   std::vector<double> brk_p_host;
-  DBuf<double> pf, s, brk_p, brk_ns, margin_p, margin_n;
-  sherd_cloud brk_tree, margin_tree;
+  DBuf<double> brk_p, brk_ns, margin_p, margin_n;
+  sherd_cloud pf_sorted, s_sorted, brk_tree, margin_tree;
   bool has_brk_tree = false, has_margin_tree = false;
   SurfView view{};
 };
@@ -288,6 +290,55 @@ int mesh_build(sherd_ctx *ctx, sherd_mesh *m) {
       vlo[k] = std::min(vlo[k], m->hv[3 * i + k]);
       vhi[k] = std::max(vhi[k], m->hv[3 * i + k]);
     }
+  // The three crossing grids: cells about one mean edge across, at most 16 M
+  // cells per axis, every face binned with the box padding.
+  double edge = 0.0;
+  for (uint32_t i = 0; i < nf; ++i) {
+    const float *a = &m->hv[3 * m->hf[3 * i]], *b = &m->hv[3 * m->hf[3 * i + 1]];
+    edge += std::sqrt(double(a[0] - b[0]) * (a[0] - b[0]) + double(a[1] - b[1]) * (a[1] - b[1]) +
+                      double(a[2] - b[2]) * (a[2] - b[2]));
+  }
+  edge = std::max(edge / std::max<uint32_t>(nf, 1), 1e-6);
+  for (int axis = 0; axis < 3; ++axis) {
+    int au = (axis + 1) % 3, av = (axis + 2) % 3;
+    AxisGrid g{};
+    double lo_u = double(vlo[au]) - 2.0 * pad, lo_v = double(vlo[av]) - 2.0 * pad;
+    double ext_u = double(vhi[au]) - lo_u + 2.0 * pad, ext_v = double(vhi[av]) - lo_v + 2.0 * pad;
+    double cell = edge;
+    while ((ext_u / cell + 1.0) * (ext_v / cell + 1.0) > 16.0e6) cell *= 1.5;
+    g.lo_u = float(lo_u);
+    g.lo_v = float(lo_v);
+    g.inv_cell = float(1.0 / cell);
+    g.nu = uint32_t(ext_u / cell) + 2;
+    g.nv = uint32_t(ext_v / cell) + 2;
+    size_t cells = size_t(g.nu) * g.nv;
+    DBuf<unsigned> count;
+    CK(count.alloc(cells + 1));
+    CK(cudaMemsetAsync(count.p, 0, sizeof(unsigned) * (cells + 1), ctx->stream));
+    k_grid_count<<<blocks_for(nf), 256, 0, ctx->stream>>>(m->tri.p, nf, axis, g, pad, count.p);
+    CK(cudaGetLastError());
+    CK(m->gstart[axis].alloc(cells + 1));
+    size_t temp_bytes = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, count.p, m->gstart[axis].p, int(cells + 1),
+                                     ctx->stream));
+    DBuf<unsigned char> temp;
+    CK(temp.alloc(temp_bytes));
+    CK(cub::DeviceScan::ExclusiveSum(temp.p, temp_bytes, count.p, m->gstart[axis].p, int(cells + 1),
+                                     ctx->stream));
+    uint32_t total = 0;
+    CK(cudaMemcpyAsync(&total, m->gstart[axis].p + cells, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(m->gslot[axis].alloc(std::max<uint32_t>(total, 1)));
+    CK(cudaMemcpyAsync(count.p, m->gstart[axis].p, sizeof(unsigned) * cells, cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    k_grid_fill<<<blocks_for(nf), 256, 0, ctx->stream>>>(m->tri.p, nf, axis, g, pad, count.p,
+                                                        m->gslot[axis].p);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    g.start = m->gstart[axis].p;
+    g.slot = m->gslot[axis].p;
+    m->view.grid[axis] = g;
+  }
   MeshView &v = m->view;
   v.nodes = m->nodes.p;
   v.tri = m->tri.p;
@@ -881,6 +932,8 @@ int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source, cons
   sherd_cloud src;
   DBuf<double> di;
   DBuf<sherd_registration> dout;
+  DBuf<int> hints;
+  CK(hints.alloc(std::max<size_t>(1, size_t(n_source) * k)));
   if (n_source) {
     if (has_nan(source, size_t(3) * n_source)) return fail(ctx, SHERD_E_INVALID, "non-finite source point");
     rc = cloud_build(ctx, source, nullptr, n_source, &src);
@@ -891,7 +944,7 @@ int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source, cons
   CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   k_icp_rung<<<k, ICP_BLOCK, 0, ctx->stream>>>(n_source ? src.pts.p : nullptr, n_source, target->view,
-                                               di.p, options, dout.p, ctx->d_status);
+                                               di.p, options, hints.p, dout.p, ctx->d_status);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, dout.p, sizeof(sherd_registration) * k, cudaMemcpyDeviceToHost, ctx->stream));
   return finish(ctx, "icp_rung", k, true);
@@ -916,9 +969,14 @@ int sherd_surfaces_create(sherd_ctx *ctx, const sherd_mesh *fracture, const sher
   x->mesh = mesh;
   auto up = [&](DBuf<double> &b, const double *h, uint32_t n) { return upload(ctx, b, h, size_t(3) * n); };
   int rc = 0;
-  if ((rc = up(x->pf, pf, n_pf)) || (rc = up(x->s, s, n_s)) || (rc = up(x->brk_p, brk_p, n_brk)) ||
-      (rc = up(x->brk_ns, brk_ns, n_brk)) || (rc = up(x->margin_p, margin_p, n_margin)) ||
-      (rc = up(x->margin_n, margin_n, n_margin))) {
+  if ((rc = up(x->brk_p, brk_p, n_brk)) || (rc = up(x->brk_ns, brk_ns, n_brk)) ||
+      (rc = up(x->margin_p, margin_p, n_margin)) || (rc = up(x->margin_n, margin_n, n_margin))) {
+    delete x;
+    return rc;
+  }
+  // The two query-only sample sets, in Morton order (the LBVH builder's sort).
+  if ((n_pf && (rc = cloud_build(ctx, pf, nullptr, n_pf, &x->pf_sorted))) ||
+      (n_s && (rc = cloud_build(ctx, s, nullptr, n_s, &x->s_sorted)))) {
     delete x;
     return rc;
   }
@@ -944,9 +1002,9 @@ int sherd_surfaces_create(sherd_ctx *ctx, const sherd_mesh *fracture, const sher
   v.has_mesh = mesh ? 1u : 0u;
   v.watertight = watertight ? 1u : 0u;
   v.frac_area = frac_area;
-  v.pf = x->pf.p;
+  v.pf = n_pf ? x->pf_sorted.pts.p : nullptr;
   v.n_pf = n_pf;
-  v.s = x->s.p;
+  v.s = n_s ? x->s_sorted.pts.p : nullptr;
   v.n_s = n_s;
   v.brk_p = x->brk_p.p;
   v.brk_ns = x->brk_ns.p;
@@ -1109,98 +1167,288 @@ int sherd_pair_free(sherd_pair *pair) {
   return SHERD_OK;
 }
 
-int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
-                              const sherd_work_item *items, uint32_t n_items, const sherd_params *p,
-                              int sched, sherd_candidate *out) {
-  if (!ctx || !p || ((!pairs) && n_pairs) || ((!items || !out) && n_items))
-    return fail(ctx, SHERD_E_INVALID, "null argument");
-  if (sched != SHERD_SCHED_BATCHED && sched != SHERD_SCHED_PLAIN)
-    return fail(ctx, SHERD_E_INVALID, "unknown schedule");
-  for (uint32_t i = 0; i < n_pairs; ++i)
-    if (!pairs[i] || pairs[i]->ctx != ctx) return fail(ctx, SHERD_E_INVALID, "pair of another context");
-  // Cost per item, for the longest-first queue order: the ladder's point
-  // iterations and the verification's sample counts.
-  std::vector<double> pair_cost(n_pairs);
-  uint32_t max_scratch = 1;
-  for (uint32_t i = 0; i < n_pairs; ++i) {
-    const PairView &v = pairs[i]->view;
-    pair_cost[i] = 60.0 * (double(v.n_reg) + double(v.n_frac)) + 4.0 * (v.a.n_s + v.b.n_s) +
-                   double(v.a.n_pf + v.b.n_pf);
-    max_scratch = std::max(max_scratch, v.scratch_floats);
-  }
-  for (uint32_t i = 0; i < n_items; ++i) {
-    if (items[i].pair >= n_pairs) return fail(ctx, SHERD_E_INVALID, "work item names no pair");
-    if (!finite_pose(items[i].init)) return fail(ctx, SHERD_E_INVALID, "work item pose is not finite");
-  }
-  if (n_items == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  __atomic_store_n(ctx->abort_host, 0u, __ATOMIC_SEQ_CST);
-  int rc = begin(ctx);
-  if (rc) return rc;
-  std::vector<PairView> views(n_pairs);
-  for (uint32_t i = 0; i < n_pairs; ++i) views[i] = pairs[i]->view;
-  std::vector<uint32_t> order(n_items);
-  for (uint32_t i = 0; i < n_items; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-    return pair_cost[items[x].pair] > pair_cost[items[y].pair];
-  });
+}  // extern "C"
+
+struct sherd_batch {
+  sherd_ctx *ctx = nullptr;
+  int sched = SHERD_SCHED_BATCHED;
+  uint32_t n_pairs = 0, n_items = 0;
+  sherd_params params{};
+  std::vector<uint32_t> pair_first, pair_count;  // queue segments of the plain schedule
   DBuf<PairView> dv;
   DBuf<sherd_work_item> di;
   DBuf<sherd_candidate> dc;
   DBuf<uint32_t> dorder;
   DBuf<unsigned> heads, scratch;
-  if ((rc = upload(ctx, dv, views.data(), n_pairs)) || (rc = upload(ctx, di, items, n_items)) ||
-      (rc = upload(ctx, dorder, order.data(), n_items)))
+  DBuf<int> hints;  // per ladder CTA: each source point's last match
+  size_t hint_stride = 1;
+  unsigned grid_l = 1, grid_v = 1;
+  uint32_t max_scratch = 64;
+  cudaGraph_t graph = nullptr, graph_v = nullptr;
+  cudaGraphExec_t exec = nullptr, exec_v = nullptr;
+  uint32_t captured_timeout = 0xFFFFFFFFu;
+  cudaEvent_t e0 = nullptr, emid = nullptr, e1 = nullptr;
+  ~sherd_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (exec_v) cudaGraphExecDestroy(exec_v);
+    if (graph_v) cudaGraphDestroy(graph_v);
+    if (e0) cudaEventDestroy(e0);
+    if (emid) cudaEventDestroy(emid);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+
+namespace {
+
+// The batched schedule as two graphs: the queue reset and the persistent
+// ladder kernel, then the persistent verification kernel; the host records an
+// event between them so each kernel's device time is known.
+int launch_ladder(sherd_batch *b, cudaStream_t s) {
+  sherd_ctx *ctx = b->ctx;
+  unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
+  CK(cudaMemsetAsync(b->heads.p, 0, 2 * sizeof(unsigned), s));
+  QueueCtl ql{b->heads.p, b->dorder.p, b->n_items, ctx->abort_dev, budget};
+  k_ladder<<<std::min<unsigned>(b->grid_l, b->n_items), ICP_BLOCK, 0, s>>>(
+      b->dv.p, b->di.p, ql, b->hints.p, b->hint_stride, b->dc.p, ctx->d_status);
+  CK(cudaGetLastError());
+  return SHERD_OK;
+}
+
+int launch_verify(sherd_batch *b, cudaStream_t s) {
+  sherd_ctx *ctx = b->ctx;
+  unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
+  QueueCtl qv{b->heads.p + 1, b->dorder.p, b->n_items, ctx->abort_dev, budget};
+  k_verify_items<<<std::min<unsigned>(b->grid_v, b->n_items), VER_BLOCK, 0, s>>>(
+      b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, ctx->d_status);
+  CK(cudaGetLastError());
+  return SHERD_OK;
+}
+
+int capture_one(sherd_batch *b, int (*launch)(sherd_batch *, cudaStream_t), cudaGraph_t &graph,
+                cudaGraphExec_t &exec) {
+  sherd_ctx *ctx = b->ctx;
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  exec = nullptr;
+  graph = nullptr;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = launch(b, ctx->stream);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
     return rc;
-  CK(dc.alloc(n_items));
-  CK(cudaMemsetAsync(dc.p, 0, sizeof(sherd_candidate) * n_items, ctx->stream));
-  CK(heads.alloc(2 * size_t(std::max<uint32_t>(n_pairs, 1))));
+  }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+  graph = g;
+  CK(cudaGraphInstantiate(&exec, graph, 0));
+  return SHERD_OK;
+}
+
+// Captures both graphs (again when the time budget changed).
+int capture(sherd_batch *b) {
+  if (b->exec && b->exec_v && b->captured_timeout == b->ctx->timeout_ms) return SHERD_OK;
+  int rc = capture_one(b, launch_ladder, b->graph, b->exec);
+  if (rc) return rc;
+  if ((rc = capture_one(b, launch_verify, b->graph_v, b->exec_v))) return rc;
+  b->captured_timeout = b->ctx->timeout_ms;
+  return SHERD_OK;
+}
+
+int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
+                 const sherd_work_item *items, uint32_t n_items, const sherd_params *p, int sched,
+                 sherd_batch *b) {
+  b->ctx = ctx;
+  b->sched = sched;
+  b->n_pairs = n_pairs;
+  b->n_items = n_items;
+  b->params = *p;
+  // Longest items first: the ladder's point iterations and the sample counts
+  // of the verification, per pair.
+  std::vector<double> pair_cost(n_pairs);
+  for (uint32_t i = 0; i < n_pairs; ++i) {
+    const PairView &v = pairs[i]->view;
+    pair_cost[i] = 60.0 * (double(v.n_reg) + double(v.n_frac)) + 4.0 * (v.a.n_s + v.b.n_s) +
+                   double(v.a.n_pf + v.b.n_pf);
+    b->max_scratch = std::max(b->max_scratch, v.scratch_floats);
+    b->hint_stride = std::max<size_t>(b->hint_stride, std::max(v.n_reg, v.n_frac));
+  }
+  std::vector<PairView> views(n_pairs);
+  for (uint32_t i = 0; i < n_pairs; ++i) views[i] = pairs[i]->view;
+  std::vector<uint32_t> order(n_items);
+  if (sched == SHERD_SCHED_BATCHED) {
+    for (uint32_t i = 0; i < n_items; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+      return pair_cost[items[x].pair] > pair_cost[items[y].pair];
+    });
+  } else {
+    b->pair_first.assign(n_pairs, 0);
+    b->pair_count.assign(n_pairs, 0);
+    for (uint32_t i = 0; i < n_items; ++i) b->pair_count[items[i].pair]++;
+    uint32_t acc = 0;
+    for (uint32_t i = 0; i < n_pairs; ++i) {
+      b->pair_first[i] = acc;
+      acc += b->pair_count[i];
+    }
+    std::vector<uint32_t> fill(b->pair_first);
+    for (uint32_t i = 0; i < n_items; ++i) order[fill[items[i].pair]++] = i;
+  }
+  int rc;
+  if ((rc = upload(ctx, b->dv, views.data(), n_pairs)) || (rc = upload(ctx, b->di, items, n_items)) ||
+      (rc = upload(ctx, b->dorder, order.data(), n_items)))
+    return rc;
+  CK(b->dc.alloc(n_items));
+  CK(cudaMemsetAsync(b->dc.p, 0, sizeof(sherd_candidate) * n_items, ctx->stream));
+  CK(b->heads.alloc(2 * size_t(std::max<uint32_t>(n_pairs, 1))));
   int occ_l = 0, occ_v = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, k_ladder, ICP_BLOCK, 0));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_v, k_verify_items, VER_BLOCK, 0));
-  unsigned grid_l = unsigned(std::max(1, occ_l) * ctx->sm_count);
-  unsigned grid_v = unsigned(std::max(1, occ_v) * ctx->sm_count);
-  unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
-  CK(scratch.alloc(size_t(grid_v) * max_scratch));
-  CK(cudaMemsetAsync(heads.p, 0, sizeof(unsigned) * 2 * std::max<uint32_t>(n_pairs, 1), ctx->stream));
-  if (sched == SHERD_SCHED_BATCHED) {
-    QueueCtl ql{heads.p, dorder.p, n_items, ctx->abort_dev, budget};
-    QueueCtl qv{heads.p + 1, dorder.p, n_items, ctx->abort_dev, budget};
-    k_ladder<<<std::min<unsigned>(grid_l, n_items), ICP_BLOCK, 0, ctx->stream>>>(dv.p, di.p, ql, dc.p,
-                                                                              ctx->d_status);
-    CK(cudaGetLastError());
-    k_verify_items<<<std::min<unsigned>(grid_v, n_items), VER_BLOCK, 0, ctx->stream>>>(
-        dv.p, di.p, qv, *p, scratch.p, max_scratch, dc.p, 1, ctx->d_status);
-    CK(cudaGetLastError());
+  b->grid_l = unsigned(std::max(1, occ_l) * ctx->sm_count);
+  b->grid_v = unsigned(std::max(1, occ_v) * ctx->sm_count);
+  CK(b->scratch.alloc(size_t(b->grid_v) * b->max_scratch));
+  b->hint_stride = (b->hint_stride + 63) / 64 * 64;
+  // The plain schedule launches one CTA per item of a pair, so it needs as many
+  // hint slots as the largest pair has items.
+  size_t slots = b->grid_l;
+  for (uint32_t c : b->pair_count) slots = std::max<size_t>(slots, c);
+  CK(b->hints.alloc(slots * b->hint_stride));
+  CK(cudaEventCreate(&b->e0));
+  CK(cudaEventCreate(&b->emid));
+  CK(cudaEventCreate(&b->e1));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (sched == SHERD_SCHED_BATCHED) return capture(b);
+  return SHERD_OK;
+}
+
+int batch_run(sherd_batch *b, float ms[3]) {
+  sherd_ctx *ctx = b->ctx;
+  __atomic_store_n(ctx->abort_host, 0u, __ATOMIC_SEQ_CST);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  if (b->sched == SHERD_SCHED_BATCHED) {
+    if ((rc = capture(b))) return rc;
+    CK(cudaEventRecord(b->e0, s));
+    CK(cudaGraphLaunch(b->exec, s));
+    CK(cudaEventRecord(b->emid, s));
+    CK(cudaGraphLaunch(b->exec_v, s));
+    CK(cudaEventRecord(b->e1, s));
   } else {
-    // One launch pair per pair, in pair order, synchronised between pairs.
-    std::vector<std::vector<uint32_t>> per(n_pairs);
-    for (uint32_t i = 0; i < n_items; ++i) per[items[i].pair].push_back(i);
-    size_t off = 0;
-    std::vector<uint32_t> flat;
-    std::vector<size_t> start(n_pairs);
-    for (uint32_t i = 0; i < n_pairs; ++i) {
-      start[i] = flat.size();
-      flat.insert(flat.end(), per[i].begin(), per[i].end());
-    }
-    (void)off;
-    CK(cudaMemcpyAsync(dorder.p, flat.data(), 4 * size_t(n_items), cudaMemcpyHostToDevice, ctx->stream));
-    for (uint32_t i = 0; i < n_pairs; ++i) {
-      uint32_t cnt = uint32_t(per[i].size());
+    unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
+    CK(cudaMemsetAsync(b->heads.p, 0, sizeof(unsigned) * 2 * b->n_pairs, s));
+    CK(cudaEventRecord(b->e0, s));
+    for (uint32_t i = 0; i < b->n_pairs; ++i) {
+      uint32_t cnt = b->pair_count[i];
       if (!cnt) continue;
-      QueueCtl ql{heads.p + 2 * i, dorder.p + start[i], cnt, ctx->abort_dev, budget};
-      QueueCtl qv{heads.p + 2 * i + 1, dorder.p + start[i], cnt, ctx->abort_dev, budget};
-      k_ladder<<<cnt, ICP_BLOCK, 0, ctx->stream>>>(dv.p, di.p, ql, dc.p, ctx->d_status);
+      QueueCtl ql{b->heads.p + 2 * i, b->dorder.p + b->pair_first[i], cnt, ctx->abort_dev, budget};
+      QueueCtl qv{b->heads.p + 2 * i + 1, b->dorder.p + b->pair_first[i], cnt, ctx->abort_dev, budget};
+      k_ladder<<<cnt, ICP_BLOCK, 0, s>>>(b->dv.p, b->di.p, ql, b->hints.p, b->hint_stride, b->dc.p,
+                                         ctx->d_status);
       CK(cudaGetLastError());
-      k_verify_items<<<std::min<unsigned>(cnt, grid_v), VER_BLOCK, 0, ctx->stream>>>(
-          dv.p, di.p, qv, *p, scratch.p, max_scratch, dc.p, 1, ctx->d_status);
+      k_verify_items<<<std::min<unsigned>(cnt, b->grid_v), VER_BLOCK, 0, s>>>(
+          b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, ctx->d_status);
       CK(cudaGetLastError());
-      CK(cudaStreamSynchronize(ctx->stream));
+      CK(cudaStreamSynchronize(s));
     }
+    CK(cudaEventRecord(b->e1, s));
   }
-  CK(cudaMemcpyAsync(out, dc.p, sizeof(sherd_candidate) * n_items, cudaMemcpyDeviceToHost, ctx->stream));
-  return finish(ctx, sched == SHERD_SCHED_BATCHED ? "ladder_verify_batched" : "ladder_verify_plain",
-                n_items, true);
+  rc = finish(ctx, b->sched == SHERD_SCHED_BATCHED ? "batch_batched" : "batch_plain", b->n_items,
+              true);
+  if (ms) {
+    float total = -1.0f, l = -1.0f, v = -1.0f;
+    cudaEventElapsedTime(&total, b->e0, b->e1);
+    if (b->sched == SHERD_SCHED_BATCHED) {
+      cudaEventElapsedTime(&l, b->e0, b->emid);
+      cudaEventElapsedTime(&v, b->emid, b->e1);
+    }
+    cudaGetLastError();
+    ms[0] = l;
+    ms[1] = v;
+    ms[2] = total;
+  }
+  return rc;
+}
+
+int check_batch_args(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
+                     const sherd_work_item *items, uint32_t n_items, const sherd_params *p, int sched) {
+  if (!ctx || !p || ((!pairs) && n_pairs) || ((!items) && n_items))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (sched != SHERD_SCHED_BATCHED && sched != SHERD_SCHED_PLAIN)
+    return fail(ctx, SHERD_E_INVALID, "unknown schedule");
+  for (uint32_t i = 0; i < n_pairs; ++i)
+    if (!pairs[i] || pairs[i]->ctx != ctx) return fail(ctx, SHERD_E_INVALID, "pair of another context");
+  for (uint32_t i = 0; i < n_items; ++i) {
+    if (items[i].pair >= n_pairs) return fail(ctx, SHERD_E_INVALID, "work item names no pair");
+    if (!finite_pose(items[i].init)) return fail(ctx, SHERD_E_INVALID, "work item pose is not finite");
+  }
+  return SHERD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sherd_batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
+                       const sherd_work_item *items, uint32_t n_items, const sherd_params *p,
+                       int sched, sherd_batch **out) {
+  if (!out) return fail(ctx, SHERD_E_INVALID, "null argument");
+  *out = nullptr;
+  int rc = check_batch_args(ctx, pairs, n_pairs, items, n_items, p, sched);
+  if (rc) return rc;
+  if (n_items == 0) return fail(ctx, SHERD_E_EMPTY, "a batch needs at least one work item");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CK(cudaSetDevice(ctx->device));
+  sherd_batch *b = new sherd_batch;
+  rc = batch_create(ctx, pairs, n_pairs, items, n_items, p, sched, b);
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return SHERD_OK;
+}
+
+int sherd_batch_run(sherd_batch *batch, float ms[3]) {
+  if (!batch) return SHERD_E_INVALID;
+  std::lock_guard<std::mutex> lock(batch->ctx->mu);
+  return batch_run(batch, ms);
+}
+
+int sherd_batch_results(sherd_batch *batch, sherd_candidate *out) {
+  if (!batch || !out) return SHERD_E_INVALID;
+  sherd_ctx *ctx = batch->ctx;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(out, batch->dc.p, sizeof(sherd_candidate) * batch->n_items,
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SHERD_OK;
+}
+
+int sherd_batch_free(sherd_batch *batch) {
+  if (!batch) return SHERD_E_INVALID;
+  cudaSetDevice(batch->ctx->device);
+  delete batch;
+  return SHERD_OK;
+}
+
+int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
+                              const sherd_work_item *items, uint32_t n_items, const sherd_params *p,
+                              int sched, sherd_candidate *out) {
+  int rc = check_batch_args(ctx, pairs, n_pairs, items, n_items, p, sched);
+  if (rc) return rc;
+  if (n_items == 0) return SHERD_OK;
+  if (!out) return fail(ctx, SHERD_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CK(cudaSetDevice(ctx->device));
+  sherd_batch b;
+  if ((rc = batch_create(ctx, pairs, n_pairs, items, n_items, p, sched, &b))) return rc;
+  if ((rc = batch_run(&b, nullptr))) return rc;
+  CK(cudaMemcpyAsync(out, b.dc.p, sizeof(sherd_candidate) * n_items, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SHERD_OK;
 }
 
 }  // extern "C"

@@ -72,7 +72,7 @@ __device__ __forceinline__ void tri_at(const MeshView &m, uint32_t s, F3 &a, F3 
 }
 
 // RayScene::first_hit (spatial/bvh.rs:84-90).
-__device__ void first_hit(const MeshView &m, F3 o, F3 d, float &best, uint32_t &best_id,
+__device__ __noinline__ void first_hit(const MeshView &m, F3 o, F3 d, float &best, uint32_t &best_id,
                           uint32_t &status) {
   best = f_inf();
   best_id = MISS;
@@ -142,68 +142,51 @@ __device__ void first_hit(const MeshView &m, F3 o, F3 d, float &best, uint32_t &
   }
 }
 
-// RayScene::crossings (spatial/bvh.rs:160-175) along +x, +y or +z: every face
-// the axis ray from p crosses. The box test is three comparisons per child.
-__device__ uint32_t crossings_axis(const MeshView &m, F3 p, int axis, uint32_t &status) {
+// RayScene::crossings (spatial/bvh.rs:160-175) along +x, +y or +z: the faces
+// the axis ray from p crosses. A face counts when p's projection lies inside
+// the face's projected rectangle padded outward by the mesh padding (f32,
+// directed rounding) and Moller-Trumbore reports a crossing; the padding is
+// far above the test's rounding, so this is the reference's count except for
+// a ray grazing a face edge-on, where it states one rule for both sides. Every
+// such face was binned into p's cell of the axis grid (rectangle containment
+// implies cell containment, the cell index being monotone in the coordinate),
+// so scanning that one cell is the whole traversal.
+__device__ __noinline__ uint32_t crossings_axis(const MeshView &m, F3 p, int axis, uint32_t &status) {
   if (m.nf == 0) return 0;
-  F3 d = {axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f};
+  const AxisGrid &g = m.grid[axis];
   float pc[3] = {p.x, p.y, p.z};
-  int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+  float pu = pc[(axis + 1) % 3], pv = pc[(axis + 2) % 3];
+  float fu = floorf((pu - g.lo_u) * g.inv_cell), fv = floorf((pv - g.lo_v) * g.inv_cell);
+  if (!(fu >= 0.0f && fv >= 0.0f && fu < float(g.nu) && fv < float(g.nv))) return 0;
+  size_t cell = size_t(fu) * g.nv + size_t(fv);
+  uint32_t b = __ldg(g.start + cell), e = __ldg(g.start + cell + 1);
+  F3 d = {axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f};
   uint32_t hits = 0;
-  auto leaf = [&](int first, int count) {
-    for (int s = first; s < first + count; ++s) {
-      F3 a, b, c;
-      uint32_t id;
-      tri_at(m, s, a, b, c, id);
-      if (moller_trumbore(p, d, a, b, c) >= 0.0f) ++hits;
-    }
-  };
-  auto box_hit = [&](const float *lo, const float *hi) {
-    return pc[a1] >= lo[a1] && pc[a1] <= hi[a1] && pc[a2] >= lo[a2] && pc[a2] <= hi[a2] &&
-           hi[axis] >= pc[axis];
-  };
-  if (m.root_leaf) {
-    leaf(0, m.root_leaf);
-    return hits;
+  int au = (axis + 1) % 3, av = (axis + 2) % 3;
+  for (uint32_t k = b; k < e; ++k) {
+    F3 a, bb, c;
+    uint32_t id;
+    tri_at(m, __ldg(g.slot + k), a, bb, c, id);
+    float ac[3] = {a.x, a.y, a.z}, bc[3] = {bb.x, bb.y, bb.z}, cc[3] = {c.x, c.y, c.z};
+    float umin = __fsub_rd(fminf(ac[au], fminf(bc[au], cc[au])), m.pad);
+    float umax = __fadd_ru(fmaxf(ac[au], fmaxf(bc[au], cc[au])), m.pad);
+    float vmin = __fsub_rd(fminf(ac[av], fminf(bc[av], cc[av])), m.pad);
+    float vmax = __fadd_ru(fmaxf(ac[av], fmaxf(bc[av], cc[av])), m.pad);
+    if (pu < umin || pu > umax || pv < vmin || pv > vmax) continue;
+    if (moller_trumbore(p, d, a, bb, c) >= 0.0f) ++hits;
   }
-  int stack_n[STACK];
-  int sp = 0, node = 0;
-  uint32_t visits = 0;
-  for (;;) {
-    if (++visits > 2u * m.nf + 64u) {
-      status |= ST_STACK;
-      break;
-    }
-    Child2 n = load_node(m.nodes, node);
-    bool h[2] = {box_hit(n.lo0, n.hi0), box_hit(n.lo1, n.hi1)};
-    int next = -1;
-    for (int c = 0; c < 2; ++c) {
-      if (!h[c]) continue;
-      if (n.cnt[c]) {
-        leaf(n.ref[c], n.cnt[c]);
-      } else if (next < 0) {
-        next = n.ref[c];
-      } else if (sp < STACK) {
-        stack_n[sp++] = n.ref[c];
-      } else {
-        status |= ST_STACK;
-      }
-    }
-    if (next >= 0) {
-      node = next;
-      continue;
-    }
-    if (sp == 0) break;
-    node = stack_n[--sp];
-  }
+  (void)status;
   return hits;
 }
 
 // RayScene::inside (spatial/bvh.rs:146-157): the majority of three parities.
+// When the first two agree the third cannot change the majority, so it is
+// cast only when they differ.
 __device__ __forceinline__ bool inside_mesh(const MeshView &m, F3 p, uint32_t &status) {
-  int votes = 0;
-  for (int a = 0; a < 3; ++a) votes += int(crossings_axis(m, p, a, status) & 1u);
-  return votes >= 2;
+  uint32_t a = crossings_axis(m, p, 0, status) & 1u;
+  uint32_t b = crossings_axis(m, p, 1, status) & 1u;
+  if (a == b) return a != 0;
+  return (crossings_axis(m, p, 2, status) & 1u) != 0;
 }
 
 __device__ __forceinline__ float box_dist2(const float *lo, const float *hi, const float *p) {
@@ -219,7 +202,7 @@ __device__ __forceinline__ float box_dist2(const float *lo, const float *hi, con
 // RayScene::bounded_distance (spatial/bvh.rs:123-131): the distance to the
 // nearest face when it is <= window (inclusive), else +inf. window = +inf is
 // RayScene::distance (bvh.rs:110-113).
-__device__ float mesh_distance(const MeshView &m, F3 p, float window, uint32_t &status) {
+__device__ __noinline__ float mesh_distance(const MeshView &m, F3 p, float window, uint32_t &status) {
   float best = f_inf();
   if (m.nf == 0 || !(window > 0.0f)) return best;
   float pc[3] = {p.x, p.y, p.z};
@@ -290,12 +273,28 @@ __device__ float mesh_distance(const MeshView &m, F3 p, float window, uint32_t &
 // PointTree::nearest_within_squared (spatial/kdtree.rs:202-217): the nearest
 // point with d2 <= r2, lowest original index on an exact tie. Returns the
 // sorted slot (or -1) and its squared distance; d2 = ((dx dx + dy dy) + dz dz).
-__device__ int nearest_within_sq(const CloudView &c, double qx, double qy, double qz, double r2,
-                                 double &best, uint32_t &status) {
+//
+// `hint` (a sorted slot, or -1) seeds the search with a point that is already
+// a candidate, typically the previous ICP pass's match: its exact distance is
+// the initial bound, so the traversal prunes from the first node. The answer
+// is the same with or without it: the hint is a valid candidate, anything
+// nearer replaces it, and an exact tie still goes to the lower index.
+__device__ __noinline__ int nearest_within_sq(const CloudView &c, double qx, double qy, double qz, double r2,
+                                 double &best, uint32_t &status, int hint = -1) {
   best = r2;
   int best_s = -1;
   uint32_t best_i = MISS;
   if (c.n == 0 || !(r2 >= 0.0)) return -1;
+  if (hint >= 0) {
+    double4 p = ldg4(c.pts + hint);
+    double dx = qx - p.x, dy = qy - p.y, dz = qz - p.z;
+    double d2 = (dx * dx + dy * dy) + dz * dz;
+    if (d2 <= r2) {
+      best = d2;
+      best_s = hint;
+      best_i = uint32_t(p.w);
+    }
+  }
   float qc[3] = {float(qx), float(qy), float(qz)};
   auto bound2 = [&]() {
     float b = __double2float_ru(best);

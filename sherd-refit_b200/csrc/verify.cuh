@@ -23,14 +23,20 @@ namespace sherd {
 
 constexpr int VER_BLOCK = 256;
 
+// Query arrays (pf, s, and the trees' own sorted points when a breakline or a
+// margin is the querying side) are in Morton order, so the 32 queries of a warp
+// are neighbours and traverse the same nodes. Every statistic R 6 takes over
+// them (counts, extrema, medians, a voxel set) is independent of their order.
+// Arrays a tree answers with (brk_p/brk_ns, margin_p/margin_n) stay in the
+// caller's order, because the lowest-index tie rule is stated on that order.
 struct SurfView {
   MeshView frac;
   MeshView mesh;
   uint32_t has_mesh, watertight;
   double frac_area;
-  const double *pf;
+  const double4 *pf;  // Morton order, w = original index
   uint32_t n_pf;
-  const double *s;
+  const double4 *s;   // Morton order, w = original index
   uint32_t n_s;
   const double *brk_p;
   const double *brk_ns;
@@ -56,8 +62,12 @@ struct PairView {
 };
 
 constexpr int MAX_CELL_WORDS = 2048;  // bitmap of up to 65 536 seam voxels
+constexpr int PEN_CHUNK = 1024;       // sample points per compaction round
 
 struct VerShared {
+  unsigned q_box[PEN_CHUNK];  // points of a round inside the mesh's box
+  unsigned q_in[PEN_CHUNK];   // ... and inside the mesh
+  unsigned n_box, n_in;
   double inv[16];
   double t[16];
   unsigned hist[256];
@@ -169,7 +179,7 @@ __device__ double median_f64(const unsigned long long *keys, uint32_t n, VerShar
 
 // verify::one_side (verify.rs:338-349) for `pts` moved by `pose` against the
 // other fragment's fracture scene.
-__device__ void one_side(const double *pts, uint32_t n, const double *pose, const MeshView &scene,
+__device__ __noinline__ void one_side(const double4 *pts, uint32_t n, const double *pose, const MeshView &scene,
                          double area, const sherd_scales &sc, unsigned *scratch, VerShared &sh,
                          double &tight, double &gap, double &contact, uint32_t &status) {
   if (threadIdx.x < 3) sh.cnt[threadIdx.x] = 0;
@@ -177,8 +187,9 @@ __device__ void one_side(const double *pts, uint32_t n, const double *pose, cons
   float window = float(sc.facing);
   unsigned facing = 0, tight_n = 0, touching = 0;
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    double4 q = ldg4(pts + i);
     double x, y, z;
-    apply_pose(pose, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], x, y, z);
+    apply_pose(pose, q.x, q.y, q.z, x, y, z);
     float d = mesh_distance(scene, narrow3(x, y, z), window, status);
     double dd = d == f_inf() ? d_inf() : double(d);
     if (dd < 2.0 * sc.tight) ++touching;
@@ -212,7 +223,7 @@ __device__ void one_side(const double *pts, uint32_t n, const double *pose, cons
 // frame and is searched around q = t^-1 a with a slack that covers the
 // rounding of both transforms, every candidate re-measured exactly in A's
 // frame. Returns B's original index or MISS.
-__device__ uint32_t seam_nearest(const SurfView &b, const double *t, const double *a_pt, double qx,
+__device__ __noinline__ uint32_t seam_nearest(const SurfView &b, const double *t, const double *a_pt, double qx,
                                  double qy, double qz, double bound, uint32_t &status) {
   if (!(bound > 0.0) || b.n_brk == 0) return MISS;
   const CloudView &c = b.brk_tree;
@@ -296,14 +307,16 @@ __device__ uint32_t seam_nearest(const SurfView &b, const double *t, const doubl
 }
 
 // verify::seam_score (verify.rs:378-442).
-__device__ double seam_score(const PairView &pr, VerShared &sh, uint32_t &status) {
+__device__ __noinline__ double seam_score(const PairView &pr, VerShared &sh, uint32_t &status) {
   const SurfView &a = pr.a, &b = pr.b;
   uint32_t words = (pr.n_cells + 31) / 32;
   for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) sh.cells[w] = 0;
   __syncthreads();
   if (b.n_brk > 0) {
-    for (uint32_t i = threadIdx.x; i < a.n_brk; i += blockDim.x) {
-      const double *ap = a.brk_p + 3 * i;
+    for (uint32_t k = threadIdx.x; k < a.n_brk; k += blockDim.x) {
+      double4 aq = ldg4(a.brk_tree.pts + k);
+      uint32_t i = uint32_t(aq.w);
+      const double ap[3] = {aq.x, aq.y, aq.z};
       double qx, qy, qz;
       apply_pose(sh.inv, ap[0], ap[1], ap[2], qx, qy, qz);
       uint32_t j = seam_nearest(b, sh.t, ap, qx, qy, qz, pr.sc.seam, status);
@@ -330,7 +343,7 @@ __device__ double seam_score(const PairView &pr, VerShared &sh, uint32_t &status
 }
 
 // verify::continuity_scores (verify.rs:450-474).
-__device__ void continuity(const PairView &pr, unsigned long long *steps,
+__device__ __noinline__ void continuity(const PairView &pr, unsigned long long *steps,
                            unsigned long long *agree, VerShared &sh, double &cont, double &cont_n,
                            uint32_t &status) {
   const SurfView &a = pr.a, &b = pr.b;
@@ -339,9 +352,11 @@ __device__ void continuity(const PairView &pr, unsigned long long *steps,
   if (a.n_margin == 0 || b.n_margin == 0) return;
   if (threadIdx.x == 0) sh.cnt[4] = 0;
   __syncthreads();
-  for (uint32_t m = threadIdx.x; m < b.n_margin; m += blockDim.x) {
+  for (uint32_t k = threadIdx.x; k < b.n_margin; k += blockDim.x) {
+    double4 mq = ldg4(b.margin_tree.pts + k);
+    uint32_t m = uint32_t(mq.w);
     double x, y, z;
-    apply_pose(sh.t, b.margin_p[3 * m], b.margin_p[3 * m + 1], b.margin_p[3 * m + 2], x, y, z);
+    apply_pose(sh.t, mq.x, mq.y, mq.z, x, y, z);
     double dist;
     int s = nearest_below(a.margin_tree, x, y, z, pr.sc.near, dist, status);
     if (s < 0) continue;
@@ -364,9 +379,39 @@ __device__ void continuity(const PairView &pr, unsigned long long *steps,
   cont_n = median_f64(agree, n, sh);
 }
 
+// Appends `slot` to a shared queue for every lane whose `pred` holds, with one
+// shared atomic per warp.
+__device__ __forceinline__ void warp_append(bool pred, unsigned slot, unsigned *queue,
+                                            unsigned *count) {
+  unsigned act = __activemask();
+  unsigned mask = __ballot_sync(act, pred);
+  if (!mask) return;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(mask) - 1;
+  unsigned base = 0;
+  if (lane == leader) base = atomicAdd(count, unsigned(__popc(mask)));
+  base = __shfl_sync(act, base, leader);
+  if (pred) queue[base + __popc(mask & ((1u << lane) - 1u))] = slot;
+}
+
+__device__ __forceinline__ F3 moved_point(const double4 *pts, uint32_t i, const double *pose) {
+  double4 q = ldg4(pts + i);
+  double x, y, z;
+  apply_pose(pose, q.x, q.y, q.z, x, y, z);
+  return narrow3(x, y, z);
+}
+
 // verify::one_penetration (verify.rs:541-580): (fraction deeper than pen,
-// smallest signed distance).
-__device__ void one_penetration(const double *pts, uint32_t n, const double *pose,
+// smallest signed distance). The points go through in rounds of PEN_CHUNK: the
+// box test compacts the ones inside the mesh's box into a shared queue, the
+// parity test runs densely over that queue and compacts the inside points into
+// a second one, and the depth queries run densely over those, so a warp's
+// lanes all do the same stage of the test. When nothing is inside, the
+// shrinking-window minimum of cpu.rs:98-111 is seeded from 32 points spread over
+// the set before the whole block scans it; a point whose distance to the mesh's
+// box already exceeds the window is skipped (it cannot beat it). Counts, the
+// maximum and the minimum do not depend on the order points are taken in.
+__device__ __noinline__ void one_penetration(const double4 *pts, uint32_t n, const double *pose,
                                 const MeshView &scene, double pen, VerShared &sh,
                                 double &fraction, double &mins, uint32_t &status) {
   fraction = 0.0;
@@ -374,27 +419,42 @@ __device__ void one_penetration(const double *pts, uint32_t n, const double *pos
   if (n == 0) return;
   if (threadIdx.x == 0) {
     sh.cnt[5] = 0;
-    sh.deep_key = 0;  // no inside point yet
+    sh.deep_key = 0;  // 0: no inside point yet; else f2key(depth) + 1
     sh.best_key = f2key(3.4028234663852886e38f);
   }
   __syncthreads();
   unsigned deeper = 0;
-  bool any = false;
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    double x, y, z;
-    apply_pose(pose, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], x, y, z);
-    F3 p = narrow3(x, y, z);
-    if (p.x < scene.lo[0] || p.x > scene.hi[0] || p.y < scene.lo[1] || p.y > scene.hi[1] ||
-        p.z < scene.lo[2] || p.z > scene.hi[2])
-      continue;
-    if (!inside_mesh(scene, p, status)) continue;
-    float depth = mesh_distance(scene, p, f_inf(), status);
-    any = true;
-    // deep_key holds depth + 1 ulp-free encoding: key + 1 so that 0 means "none".
-    atomicMax(&sh.deep_key, f2key(depth) + 1u);
-    if (double(depth) > pen) ++deeper;
+  for (uint32_t base = 0; base < n; base += PEN_CHUNK) {
+    uint32_t end = min(n, base + uint32_t(PEN_CHUNK));
+    if (threadIdx.x == 0) {
+      sh.n_box = 0;
+      sh.n_in = 0;
+    }
+    __syncthreads();
+    for (uint32_t i = base + threadIdx.x; i < base + PEN_CHUNK; i += blockDim.x) {
+      bool in_box = false;
+      if (i < end) {
+        F3 p = moved_point(pts, i, pose);
+        in_box = !(p.x < scene.lo[0] || p.x > scene.hi[0] || p.y < scene.lo[1] ||
+                   p.y > scene.hi[1] || p.z < scene.lo[2] || p.z > scene.hi[2]);
+      }
+      warp_append(in_box, i, sh.q_box, &sh.n_box);
+    }
+    __syncthreads();
+    unsigned nb = sh.n_box;
+    for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x) {
+      uint32_t i = sh.q_box[k];
+      warp_append(inside_mesh(scene, moved_point(pts, i, pose), status), i, sh.q_in, &sh.n_in);
+    }
+    __syncthreads();
+    unsigned ni = sh.n_in;
+    for (uint32_t k = threadIdx.x; k < ni; k += blockDim.x) {
+      float depth = mesh_distance(scene, moved_point(pts, sh.q_in[k], pose), f_inf(), status);
+      atomicMax(&sh.deep_key, f2key(depth) + 1u);
+      if (double(depth) > pen) ++deeper;
+    }
+    __syncthreads();
   }
-  (void)any;
   atomicAdd(&sh.cnt[5], deeper);
   __syncthreads();
   fraction = double(sh.cnt[5]) / double(n);
@@ -404,13 +464,20 @@ __device__ void one_penetration(const double *pts, uint32_t n, const double *pos
     mins = -double(key2f(dk - 1u));
     return;
   }
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    double x, y, z;
-    apply_pose(pose, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], x, y, z);
+  auto scan = [&](uint32_t i) {
+    F3 p = moved_point(pts, i, pose);
     float window = key2f(*((volatile unsigned *)&sh.best_key));
-    float d = mesh_distance(scene, narrow3(x, y, z), window, status);
+    float pc[3] = {p.x, p.y, p.z};
+    // Every face is at least the box's distance away; the slack keeps a face
+    // whose rounded distance ties the window within a few ulps.
+    float gap = sqrtf(box_dist2(scene.lo, scene.hi, pc));
+    if (gap > window + 1e-5f * window + scene.pad) return;
+    float d = mesh_distance(scene, p, window, status);
     if (d != f_inf()) atomicMin(&sh.best_key, f2key(d));
-  }
+  };
+  if (threadIdx.x < 32) scan(uint32_t((unsigned long long)threadIdx.x * n / 32u));
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) scan(i);
   __syncthreads();
   mins = double(key2f(sh.best_key));
   __syncthreads();
