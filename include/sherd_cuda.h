@@ -259,6 +259,30 @@ int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source,
                    const sherd_cloud *target, const double *inits, uint32_t k,
                    sherd_icp_options options, sherd_registration *out);
 
+/* For callers that cannot allocate device memory during a run: a worker held
+ * to a fixed device-memory budget set up front, or code that must not call
+ * cudaMalloc/cudaFree while other streams are in flight (both can block or
+ * synchronise the whole device). No counterpart in the reference.
+ *
+ * The same rung as sherd_icp_rung, with every buffer already on the device:
+ * `source` holds n_source points as 4 doubles each (x, y, z, unused; 16-byte
+ * aligned), `inits` k row-major 4x4 poses, `out` room for k registrations.
+ * The per-point working memory (each source point's last match) lives in one
+ * array inside this library, sized at SHERD_NOALLOC_CAPACITY entries and held
+ * by every GPU that loads the library until the process exits; a call with
+ * k * n_source above it is refused with SHERD_E_INVALID. The call allocates
+ * nothing, waits for its own work, and leaves the array holding the last
+ * call's contents (each rung resets the part it uses before reading it). All
+ * calls share the one array, so two calls that overlap on the GPU (from two
+ * contexts, or two host threads on different contexts of one device) race.
+ * The first call on each device looks the array's device address up
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture on the device. */
+#define SHERD_NOALLOC_CAPACITY (1u << 20)
+int sherd_icp_rung_noalloc(sherd_ctx *ctx, const double *source, uint32_t n_source,
+                           const sherd_cloud *target, const double *inits, uint32_t k,
+                           sherd_icp_options options, sherd_registration *out);
+
 /* ---- verification (matching/verify.rs) ---------------------------------- */
 
 /* Surfaces (verify.rs:223-299): one fragment as R 6 reads it. `fracture` is

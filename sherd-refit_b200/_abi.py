@@ -18,6 +18,7 @@ OK, E_INVALID, E_OOM, E_TIMEOUT, E_ABORTED, E_DEVICE, E_EMPTY = 0, -1, -2, -3, -
 REDUCE_ALL, REDUCE_MIN = 0, 1
 POINT_TO_POINT, POINT_TO_PLANE = 0, 1
 SCHED_BATCHED, SCHED_PLAIN = 0, 1
+NOALLOC_CAPACITY = 1 << 20
 
 F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 F64P = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -129,6 +130,7 @@ _SIGNATURES = {
     "sherd_nearest_within_sq": (C.c_int, [VP, VP, F64P, C.c_uint32, C.c_double, U32P, F64P]),
     "sherd_nearest_below": (C.c_int, [VP, VP, F64P, C.c_uint32, C.c_double, U32P, F64P]),
     "sherd_icp_rung": (C.c_int, [VP, VP, C.c_uint32, VP, F64P, C.c_uint32, IcpOptions, VP]),
+    "sherd_icp_rung_noalloc": (C.c_int, [VP, VP, C.c_uint32, VP, VP, C.c_uint32, IcpOptions, VP]),
     "sherd_surfaces_create": (C.c_int, [VP, VP, VP, C.c_uint32, C.c_double, VP, C.c_uint32, VP,
                                         C.c_uint32, VP, VP, C.c_uint32, VP, VP, C.c_uint32,
                                         C.POINTER(VP)]),

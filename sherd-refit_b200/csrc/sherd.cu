@@ -48,9 +48,34 @@ struct sherd_ctx {
   std::map<std::string, MethodStats> stats;
 };
 
+// Working memory of sherd_icp_rung_noalloc: each source point's last match, for
+// every candidate of one call. A file-scope device array, so that entry point
+// never allocates; every GPU that loads the library holds it until exit.
+static __device__ __align__(256) int g_noalloc_hints[SHERD_NOALLOC_CAPACITY];
+
 namespace {
 
 thread_local std::map<const sherd_ctx *, std::string> t_errors;
+
+// The device address of g_noalloc_hints, looked up once per device with that
+// device current (host code cannot use the symbol itself as an address).
+std::mutex g_symbol_mu;
+std::map<int, int *> g_noalloc_address;
+
+cudaError_t noalloc_address(int device, int **out) {
+  std::lock_guard<std::mutex> lock(g_symbol_mu);
+  auto it = g_noalloc_address.find(device);
+  if (it != g_noalloc_address.end()) {
+    *out = it->second;
+    return cudaSuccess;
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_hints);
+  if (e != cudaSuccess) return e;
+  g_noalloc_address[device] = static_cast<int *>(p);
+  *out = static_cast<int *>(p);
+  return cudaSuccess;
+}
 
 int fail(const sherd_ctx *ctx, int code, const std::string &msg) {
   t_errors[ctx] = msg;
@@ -948,6 +973,35 @@ int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source, cons
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, dout.p, sizeof(sherd_registration) * k, cudaMemcpyDeviceToHost, ctx->stream));
   return finish(ctx, "icp_rung", k, true);
+}
+
+int sherd_icp_rung_noalloc(sherd_ctx *ctx, const double *source, uint32_t n_source,
+                           const sherd_cloud *target, const double *inits, uint32_t k,
+                           sherd_icp_options options, sherd_registration *out) {
+  if (!ctx || !target || ((!inits || !out) && k) || (!source && n_source))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (options.estimation != SHERD_POINT_TO_PLANE)
+    return fail(ctx, SHERD_E_INVALID, "only the point-to-plane rung runs on the device");
+  if (options.max_iteration < 0) return fail(ctx, SHERD_E_INVALID, "negative iteration cap");
+  if (uint64_t(k) * n_source > SHERD_NOALLOC_CAPACITY)
+    return fail(ctx, SHERD_E_INVALID,
+                "k * n_source exceeds SHERD_NOALLOC_CAPACITY (1048576): split the candidates "
+                "over several calls or use sherd_icp_rung");
+  if ((reinterpret_cast<uintptr_t>(source) & 15u) != 0)
+    return fail(ctx, SHERD_E_INVALID, "source must be 16-byte aligned (4 doubles per point)");
+  if (k == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);  // makes the context's device current
+  if (rc) return rc;
+  // The first call on a device looks the array's address up; that call should
+  // come before any stream capture on the device.
+  int *hints = nullptr;
+  CK(noalloc_address(ctx->device, &hints));
+  k_icp_rung<<<k, ICP_BLOCK, 0, ctx->stream>>>(reinterpret_cast<const double4 *>(source), n_source,
+                                               target->view, inits, options, hints, out,
+                                               ctx->d_status);
+  CK(cudaGetLastError());
+  return finish(ctx, "icp_rung_noalloc", k, true);
 }
 
 // ---- verification ------------------------------------------------------------
