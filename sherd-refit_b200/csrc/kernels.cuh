@@ -347,13 +347,15 @@ __global__ void __launch_bounds__(ICP_BLOCK, 4) k_ladder(const PairView *pairs,
   if (st) atomicOr(status, st);
 }
 
-// R 6 + R 6.5 at each item's last rung pose (verify.rs:590-638).
+// R 6 + R 6.5 at each item's last rung pose (verify.rs:590-638). With `inv`
+// set, the penetration half is left to the wavefront kernels below and the
+// inverse pose of every item is written for them.
 __global__ void __launch_bounds__(VER_BLOCK, 3) k_verify_items(const PairView *pairs,
                                                             const sherd_work_item *items,
                                                             QueueCtl q, sherd_params p,
                                                             unsigned *scratch, size_t stride,
                                                             sherd_candidate *out, int full,
-                                                            uint32_t *status) {
+                                                            double *inv, uint32_t *status) {
   __shared__ VerShared sh;
   uint32_t st = 0;
   unsigned long long start = global_ns();
@@ -372,9 +374,295 @@ __global__ void __launch_bounds__(VER_BLOCK, 3) k_verify_items(const PairView *p
       __syncthreads();
       continue;
     }
-    verify_block(pr, full != 0, p, mine, sh, &c->scores, &c->accepted, st);
+    verify_block(pr, full != 0, p, mine, sh, &c->scores, &c->accepted, st, inv == nullptr,
+                 inv ? inv + 16 * size_t(it) : nullptr);
   }
   if (st) atomicOr(status, st);
+}
+
+// ---- the penetration wavefront of the batched path ------------------------------
+//
+// R 6.4 for every (item, side) of a batch at once: side 0 is B's surface
+// samples moved by T against A's mesh, side 1 A's moved by T^-1 against B's.
+// The samples of all units are one flat list of 32-point chunks that warps
+// take from a global counter, so no block ever waits at a barrier for its
+// slowest lane. Each warp keeps two shared queues: the points of its chunks
+// that fall in the mesh's box, and the ones the parity test calls inside; a
+// queue is drained 32 entries at a time, so the parity and depth queries run
+// with every lane of the warp busy. A unit's count, deepest depth and minimum
+// distance are combined with global atomics, which makes them independent of
+// the order the points are taken in, as R 6.4's statistics are.
+
+struct PenState {
+  unsigned *deeper;    // per unit: points deeper than sc.pen
+  unsigned *deep;      // per unit: f2key(deepest depth) + 1, 0 when nothing is inside
+  unsigned *best;      // per unit: f2key(smallest distance) for the nothing-inside case
+  const uint32_t *chunk0;  // per unit: its first chunk in the flat list (n_units + 1)
+  uint32_t n_units, n_chunks;
+};
+
+struct PenUnit {
+  const double4 *pts;
+  uint32_t n;
+  const MeshView *mesh;
+  const double *pose;
+  double pen;
+  bool avail;
+};
+
+__device__ __forceinline__ PenUnit pen_unit(const PairView *pairs, const sherd_work_item *items,
+                                            const sherd_candidate *cands, const double *inv,
+                                            uint32_t u) {
+  uint32_t item = u >> 1, side = u & 1u;
+  const PairView &pr = pairs[items[item].pair];
+  PenUnit x;
+  x.avail = pr.a.has_mesh && pr.b.has_mesh && pr.a.watertight && pr.b.watertight;
+  x.pts = side ? pr.a.s : pr.b.s;
+  x.n = side ? pr.a.n_s : pr.b.n_s;
+  x.mesh = side ? &pr.b.mesh : &pr.a.mesh;
+  x.pose = side ? inv + 16 * size_t(item) : cands[item].rungs[3].transform;
+  x.pen = pr.sc.pen;
+  return x;
+}
+
+__device__ __forceinline__ uint32_t unit_of_chunk(const PenState &ps, uint32_t chunk) {
+  uint32_t lo = 0, hi = ps.n_units;  // last unit with chunk0[u] <= chunk
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(ps.chunk0 + mid) <= chunk) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+struct WarpQueue {
+  unsigned long long box[64];
+  unsigned long long in[64];
+  int n_box, n_in;
+};
+
+__device__ __forceinline__ void wq_push(unsigned long long *q, int *count, bool pred,
+                                        unsigned long long v) {
+  unsigned mask = __ballot_sync(0xffffffffu, pred);
+  int lane = threadIdx.x & 31;
+  int base = *count;
+  if (pred) q[base + __popc(mask & ((1u << lane) - 1u))] = v;
+  __syncwarp();
+  if (lane == 0) *count = base + __popc(mask);
+  __syncwarp();
+}
+
+// Pops up to 32 entries; returns whether this lane got one.
+__device__ __forceinline__ bool wq_pop(unsigned long long *q, int *count, unsigned long long &v) {
+  int lane = threadIdx.x & 31;
+  int n = *count;
+  int take = n < 32 ? n : 32;
+  bool got = lane < take;
+  if (got) v = q[n - take + lane];
+  __syncwarp();
+  if (lane == 0) *count = n - take;
+  __syncwarp();
+  return got;
+}
+
+// Takes the next chunk for the warp. The abort flag lives in host-mapped
+// memory, a round trip over the bus, so a warp polls it (and the time budget)
+// only every 128 chunks it takes.
+__device__ __forceinline__ bool take_chunk(unsigned *head, uint32_t n_chunks,
+                                           const uint32_t *abort_flag, unsigned long long budget,
+                                           unsigned long long start, uint32_t &taken,
+                                           uint32_t &chunk, uint32_t &st) {
+  uint32_t c = 0xFFFFFFFFu;
+  if ((threadIdx.x & 31) == 0) {
+    bool stop = false;
+    if ((taken++ & 127u) == 0u) {
+      if (abort_flag && *((volatile const uint32_t *)abort_flag)) {
+        st |= ST_ABORTED;
+        stop = true;
+      } else if (budget && global_ns() - start > budget) {
+        st |= ST_TIMEOUT;
+        stop = true;
+      }
+    }
+    if (!stop) c = atomicAdd(head, 1u);
+  }
+  chunk = __shfl_sync(0xffffffffu, c, 0);
+  return chunk < n_chunks;
+}
+
+__device__ __forceinline__ F3 unit_point(const PenUnit &x, uint32_t i) {
+  double4 q = ldg4(x.pts + i);
+  double a, b, c;
+  apply_pose(x.pose, q.x, q.y, q.z, a, b, c);
+  return {float(a), float(b), float(c)};
+}
+
+__global__ void k_pen_init(PenState ps) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < ps.n_units; u += gridDim.x * blockDim.x) {
+    ps.deeper[u] = 0;
+    ps.deep[u] = 0;
+    ps.best[u] = f2key(3.4028234663852886e38f);
+  }
+}
+
+// Box test, parity, depth: the first pass of one_penetration (verify.rs:541-568).
+__global__ void __launch_bounds__(256) k_pen_inside(const PairView *pairs, const sherd_work_item *items,
+                                                    const sherd_candidate *cands, const double *inv,
+                                                    PenState ps, unsigned *head,
+                                                    const uint32_t *abort_flag,
+                                                    unsigned long long budget, uint32_t *status) {
+  __shared__ WarpQueue wqs[8];
+  WarpQueue &q = wqs[threadIdx.x >> 5];
+  int lane = threadIdx.x & 31;
+  if (lane == 0) q.n_box = q.n_in = 0;
+  __syncwarp();
+  uint32_t st = 0;
+  unsigned long long start = global_ns();
+  auto depth_stage = [&](bool drain) {
+    while (q.n_in >= 32 || (drain && q.n_in > 0)) {
+      unsigned long long e;
+      if (wq_pop(q.in, &q.n_in, e)) {
+        uint32_t u = uint32_t(e >> 32), i = uint32_t(e);
+        PenUnit x = pen_unit(pairs, items, cands, inv, u);
+        float depth = mesh_distance(*x.mesh, unit_point(x, i), f_inf(), st);
+        atomicMax(&ps.deep[u], f2key(depth) + 1u);
+        if (double(depth) > x.pen) atomicAdd(&ps.deeper[u], 1u);
+      }
+    }
+  };
+  auto parity_stage = [&](bool drain) {
+    while (q.n_box >= 32 || (drain && q.n_box > 0)) {
+      unsigned long long e = 0;
+      bool got = wq_pop(q.box, &q.n_box, e);
+      bool inside = false;
+      if (got) {
+        uint32_t u = uint32_t(e >> 32), i = uint32_t(e);
+        PenUnit x = pen_unit(pairs, items, cands, inv, u);
+        inside = inside_mesh(*x.mesh, unit_point(x, i), st);
+      }
+      wq_push(q.in, &q.n_in, inside, e);
+      depth_stage(false);
+    }
+  };
+  uint32_t chunk, taken = 0;
+  while (take_chunk(head, ps.n_chunks, abort_flag, budget, start, taken, chunk, st)) {
+    uint32_t u = unit_of_chunk(ps, chunk);
+    PenUnit x = pen_unit(pairs, items, cands, inv, u);
+    uint32_t i = (chunk - ps.chunk0[u]) * 32u + lane;
+    bool in_box = false;
+    if (x.avail && i < x.n) {
+      F3 p = unit_point(x, i);
+      const MeshView &m = *x.mesh;
+      in_box = !(p.x < m.lo[0] || p.x > m.hi[0] || p.y < m.lo[1] || p.y > m.hi[1] ||
+                 p.z < m.lo[2] || p.z > m.hi[2]);
+    }
+    wq_push(q.box, &q.n_box, in_box, (unsigned long long)u << 32 | i);
+    parity_stage(false);
+  }
+  parity_stage(true);
+  depth_stage(true);
+  if (st) atomicOr(status, st);
+}
+
+// The nothing-inside case (verify.rs:569-579): 32 points spread over each such
+// unit seed its shrinking window with unbounded queries.
+__global__ void k_pen_seed(const PairView *pairs, const sherd_work_item *items,
+                           const sherd_candidate *cands, const double *inv, PenState ps,
+                           uint32_t *status) {
+  uint32_t st = 0;
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < ps.n_units; u += warps) {
+    PenUnit x = pen_unit(pairs, items, cands, inv, u);
+    if (!x.avail || x.n == 0 || ps.deep[u] != 0) continue;
+    if (lane < x.n) {
+      uint32_t i = uint32_t((unsigned long long)lane * x.n / 32u);
+      float window = key2f(*((volatile unsigned *)&ps.best[u]));
+      float d = mesh_distance(*x.mesh, unit_point(x, i), window, st);
+      if (d != f_inf()) atomicMin(&ps.best[u], f2key(d));
+    }
+  }
+  if (st) atomicOr(status, st);
+}
+
+// The shrinking-window scan over every point of the nothing-inside units; a
+// point farther from the mesh's box than the window cannot beat it.
+__global__ void __launch_bounds__(256) k_pen_min(const PairView *pairs, const sherd_work_item *items,
+                                                 const sherd_candidate *cands, const double *inv,
+                                                 PenState ps, unsigned *head,
+                                                 const uint32_t *abort_flag,
+                                                 unsigned long long budget, uint32_t *status) {
+  __shared__ WarpQueue wqs[8];
+  WarpQueue &q = wqs[threadIdx.x >> 5];
+  int lane = threadIdx.x & 31;
+  if (lane == 0) q.n_box = q.n_in = 0;
+  __syncwarp();
+  uint32_t st = 0;
+  unsigned long long start = global_ns();
+  auto query_stage = [&](bool drain) {
+    while (q.n_box >= 32 || (drain && q.n_box > 0)) {
+      unsigned long long e;
+      if (wq_pop(q.box, &q.n_box, e)) {
+        uint32_t u = uint32_t(e >> 32), i = uint32_t(e);
+        PenUnit x = pen_unit(pairs, items, cands, inv, u);
+        float window = key2f(*((volatile unsigned *)&ps.best[u]));
+        float d = mesh_distance(*x.mesh, unit_point(x, i), window, st);
+        if (d != f_inf()) atomicMin(&ps.best[u], f2key(d));
+      }
+    }
+  };
+  uint32_t chunk, taken = 0;
+  while (take_chunk(head, ps.n_chunks, abort_flag, budget, start, taken, chunk, st)) {
+    uint32_t u = unit_of_chunk(ps, chunk);
+    PenUnit x = pen_unit(pairs, items, cands, inv, u);
+    uint32_t i = (chunk - ps.chunk0[u]) * 32u + lane;
+    bool want = false;
+    if (x.avail && i < x.n && ps.deep[u] == 0) {
+      F3 p = unit_point(x, i);
+      float pc[3] = {p.x, p.y, p.z};
+      float window = key2f(*((volatile unsigned *)&ps.best[u]));
+      float gap = sqrtf(box_dist2(x.mesh->lo, x.mesh->hi, pc));
+      want = !(gap > window + 1e-5f * window + x.mesh->pad);
+    }
+    wq_push(q.box, &q.n_box, want, (unsigned long long)u << 32 | i);
+    query_stage(false);
+  }
+  query_stage(true);
+  if (st) atomicOr(status, st);
+}
+
+// penetration_scores (verify.rs:483-498) from the two units of each item, and
+// the verdict (verify.rs:632-638).
+__global__ void k_pen_finalize(const PairView *pairs, const sherd_work_item *items,
+                               sherd_candidate *cands, PenState ps, sherd_params p, uint32_t n_items) {
+  uint32_t it = blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= n_items) return;
+  const PairView &pr = pairs[items[it].pair];
+  sherd_candidate &c = cands[it];
+  if (c.status) return;
+  sherd_scores &s = c.scores;
+  bool avail = pr.a.has_mesh && pr.b.has_mesh && pr.a.watertight && pr.b.watertight;
+  if (avail) {
+    double frac[2], mins[2];
+    for (int side = 0; side < 2; ++side) {
+      uint32_t u = 2 * it + side;
+      uint32_t n = side ? pr.a.n_s : pr.b.n_s;
+      if (n == 0) {
+        frac[side] = 0.0;
+        mins[side] = 0.0;
+        continue;
+      }
+      frac[side] = double(ps.deeper[u]) / double(n);
+      mins[side] = ps.deep[u] ? -double(key2f(ps.deep[u] - 1u)) : double(key2f(ps.best[u]));
+    }
+    // side 0 is pen_b / min_b, side 1 pen_a / min_a
+    s.pen = fmax(frac[1], frac[0]);
+    s.pen_depth = fmax(-mins[1], -mins[0]) / pr.sc.t;
+  }
+  const sherd_scales &sc = pr.sc;
+  c.accepted = (s.tight >= p.min_tight && s.gap * sc.t <= sc.gap && s.pen <= p.max_pen &&
+                s.seam >= p.min_seam && s.cont_n >= p.min_cont_n)
+                   ? 1u
+                   : 0u;
 }
 
 }  // namespace sherd

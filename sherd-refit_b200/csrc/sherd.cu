@@ -1158,7 +1158,7 @@ int sherd_verify(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfaces *
   sherd_params p;
   sherd_params_default(&p);
   k_verify_items<<<1, VER_BLOCK, 0, ctx->stream>>>(dv.p, di.p, q, p, scratch.p, v.scratch_floats, dc.p,
-                                                  full, ctx->d_status);
+                                                  full, nullptr, ctx->d_status);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(&cand, dc.p, sizeof cand, cudaMemcpyDeviceToHost, ctx->stream));
   rc = finish(ctx, "verify", 1, true);
@@ -1236,6 +1236,13 @@ struct sherd_batch {
   DBuf<unsigned> heads, scratch;
   DBuf<int> hints;  // per ladder CTA: each source point's last match
   size_t hint_stride = 1;
+  // The penetration wavefront: per item the inverse pose, per (item, side)
+  // unit its counters and its first chunk.
+  DBuf<double> inv;
+  DBuf<unsigned> deeper, deep, best, pen_heads;
+  DBuf<uint32_t> chunk0;
+  uint32_t n_chunks = 0;
+  unsigned grid_p = 1, grid_m = 1;
   unsigned grid_l = 1, grid_v = 1;
   uint32_t max_scratch = 64;
   cudaGraph_t graph = nullptr, graph_v = nullptr;
@@ -1274,7 +1281,26 @@ int launch_verify(sherd_batch *b, cudaStream_t s) {
   unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
   QueueCtl qv{b->heads.p + 1, b->dorder.p, b->n_items, ctx->abort_dev, budget};
   k_verify_items<<<std::min<unsigned>(b->grid_v, b->n_items), VER_BLOCK, 0, s>>>(
-      b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, ctx->d_status);
+      b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, b->inv.p,
+      ctx->d_status);
+  CK(cudaGetLastError());
+  PenState ps{b->deeper.p, b->deep.p, b->best.p, b->chunk0.p, 2 * b->n_items, b->n_chunks};
+  CK(cudaMemsetAsync(b->pen_heads.p, 0, 2 * sizeof(unsigned), s));
+  k_pen_init<<<blocks_for(ps.n_units), 256, 0, s>>>(ps);
+  CK(cudaGetLastError());
+  if (b->n_chunks) {
+    k_pen_inside<<<b->grid_p, 256, 0, s>>>(b->dv.p, b->di.p, b->dc.p, b->inv.p, ps, b->pen_heads.p,
+                                         ctx->abort_dev, budget, ctx->d_status);
+    CK(cudaGetLastError());
+    k_pen_seed<<<blocks_for(size_t(ps.n_units) * 32), 256, 0, s>>>(b->dv.p, b->di.p, b->dc.p,
+                                                                  b->inv.p, ps, ctx->d_status);
+    CK(cudaGetLastError());
+    k_pen_min<<<b->grid_m, 256, 0, s>>>(b->dv.p, b->di.p, b->dc.p, b->inv.p, ps,
+                                      b->pen_heads.p + 1, ctx->abort_dev, budget, ctx->d_status);
+    CK(cudaGetLastError());
+  }
+  k_pen_finalize<<<blocks_for(b->n_items), 256, 0, s>>>(b->dv.p, b->di.p, b->dc.p, ps, b->params,
+                                                       b->n_items);
   CK(cudaGetLastError());
   return SHERD_OK;
 }
@@ -1361,6 +1387,34 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
   b->grid_l = unsigned(std::max(1, occ_l) * ctx->sm_count);
   b->grid_v = unsigned(std::max(1, occ_v) * ctx->sm_count);
   CK(b->scratch.alloc(size_t(b->grid_v) * b->max_scratch));
+  if (sched == SHERD_SCHED_BATCHED) {
+    // Unit 2i is item i's side 0 (B's samples in A's mesh), 2i+1 its side 1.
+    std::vector<uint32_t> chunk0(2 * size_t(n_items) + 1);
+    uint64_t acc = 0;
+    for (uint32_t i = 0; i < n_items; ++i) {
+      const PairView &v = views[items[i].pair];
+      bool avail = v.a.has_mesh && v.b.has_mesh && v.a.watertight && v.b.watertight;
+      uint32_t ns[2] = {v.b.n_s, v.a.n_s};
+      for (int side = 0; side < 2; ++side) {
+        chunk0[2 * size_t(i) + side] = uint32_t(acc);
+        if (avail) acc += (ns[side] + 31u) / 32u;
+      }
+    }
+    if (acc >= 0xFFFFFFFFull) return fail(ctx, SHERD_E_INVALID, "batch too large for one wavefront");
+    chunk0[2 * size_t(n_items)] = uint32_t(acc);
+    b->n_chunks = uint32_t(acc);
+    if ((rc = upload(ctx, b->chunk0, chunk0.data(), chunk0.size()))) return rc;
+    CK(b->inv.alloc(16 * size_t(n_items)));
+    CK(b->deeper.alloc(2 * size_t(n_items)));
+    CK(b->deep.alloc(2 * size_t(n_items)));
+    CK(b->best.alloc(2 * size_t(n_items)));
+    CK(b->pen_heads.alloc(2));
+    int occ_p = 0, occ_m = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k_pen_inside, 256, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_pen_min, 256, 0));
+    b->grid_p = unsigned(std::max(1, occ_p) * ctx->sm_count);
+    b->grid_m = unsigned(std::max(1, occ_m) * ctx->sm_count);
+  }
   b->hint_stride = (b->hint_stride + 63) / 64 * 64;
   // The plain schedule launches one CTA per item of a pair, so it needs as many
   // hint slots as the largest pair has items.
@@ -1401,7 +1455,8 @@ int batch_run(sherd_batch *b, float ms[3]) {
                                          ctx->d_status);
       CK(cudaGetLastError());
       k_verify_items<<<std::min<unsigned>(cnt, b->grid_v), VER_BLOCK, 0, s>>>(
-          b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, ctx->d_status);
+          b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, nullptr,
+          ctx->d_status);
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(s));
     }

@@ -485,11 +485,16 @@ __device__ __noinline__ void one_penetration(const double4 *pts, uint32_t n, con
 
 // verify::verify (verify.rs:590-626) + accept (verify.rs:632-638) at the pose
 // in sh.t. Every thread calls it; thread 0 writes *out.
+// `pen_here` false leaves the penetration scores to the batched path's
+// wavefront kernels (which read the inverse pose from `inv_out`) and the
+// verdict to its finalising kernel.
 __device__ void verify_block(const PairView &pr, bool full, const sherd_params &p,
                              unsigned *scratch, VerShared &sh, sherd_scores *out,
-                             uint32_t *accepted, uint32_t &status) {
+                             uint32_t *accepted, uint32_t &status, bool pen_here = true,
+                             double *inv_out = nullptr) {
   if (threadIdx.x == 0) pose_inverse(sh.t, sh.inv);
   __syncthreads();
+  if (inv_out && threadIdx.x < 16) inv_out[threadIdx.x] = sh.inv[threadIdx.x];
   const sherd_scales &sc = pr.sc;
   double ta, ga, ca, tb, gb, cb;
   one_side(pr.b.pf, pr.b.n_pf, sh.t, pr.a.frac, pr.b.frac_area, sc, scratch, sh, tb, gb, cb,
@@ -504,7 +509,7 @@ __device__ void verify_block(const PairView &pr, bool full, const sherd_params &
     continuity(pr, steps, steps + pr.b.n_margin, sh, cont, cont_n, status);
     if (!pr.a.has_mesh || !pr.b.has_mesh || !(pr.a.watertight && pr.b.watertight)) {
       unavailable = 1;
-    } else {
+    } else if (pen_here) {
       double pen_b, min_b, pen_a, min_a;
       one_penetration(pr.b.s, pr.b.n_s, sh.t, pr.a.mesh, sc.pen, sh, pen_b, min_b, status);
       one_penetration(pr.a.s, pr.a.n_s, sh.inv, pr.b.mesh, sc.pen, sh, pen_a, min_a, status);
@@ -535,7 +540,7 @@ __device__ void verify_block(const PairView &pr, bool full, const sherd_params &
     s.brk = 0.0;
     s.brk_best = 0.0;
     *out = s;
-    if (accepted)
+    if (accepted && pen_here)
       *accepted = (s.tight >= p.min_tight && s.gap * sc.t <= sc.gap && s.pen <= p.max_pen &&
                    s.seam >= p.min_seam && s.cont_n >= p.min_cont_n)
                       ? 1u
