@@ -250,23 +250,21 @@ def main():
     _barrier(world)
     torch.cuda.synchronize()
     sampler.start()
-    ladder_ms, verify_ms, total_ms = [], [], []
+    runs = []
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
-        l, v, t = batch.run()
-        ladder_ms.append(l)
-        verify_ms.append(v)
-        total_ms.append(t)
+        runs.append(batch.run())
     torch.cuda.synchronize()
     _barrier(world)
     clocks = sampler.stop()
-    step_ms = _max_over_ranks(world, float(np.mean(total_ms)))
+    stage_ms = {k: float(np.mean([r[k] for r in runs])) for k in runs[0]}
+    step_ms = _max_over_ranks(world, stage_ms["total"])
     n_items = dev.n_items
     value = world * n_items / (step_ms / 1000.0)
 
     cands = sherd.candidates(batch.results())
-    icp_bytes, ver_bytes = workload.algorithmic_bytes(wl, cands, dev.n_src)
+    sbytes = workload.stage_bytes(wl, cands, dev.n_src)
     accepted = int(cands["accepted"].sum())
     status_bad = int((cands["status"] != 0).sum())
 
@@ -286,21 +284,22 @@ def main():
     same = bytes(out) == bytes(batch.results())
 
     peak, peak_kind = _peaks()
-    l_ms = float(np.mean(ladder_ms))
-    v_ms = float(np.mean(verify_ms))
-    dominant = "k_ladder" if l_ms >= v_ms else "k_verify_items"
-    bytes_dom = icp_bytes if dominant == "k_ladder" else ver_bytes
-    ms_dom = l_ms if dominant == "k_ladder" else v_ms
-    achieved = bytes_dom / (ms_dom / 1000.0) / 1e9
+    kernel_of = {"ladder": "k_ladder", "verify": "k_verify_items", "pen_inside": "k_pen_inside",
+                 "pen_min": "k_pen_seed + k_pen_min", "finalize": "k_pen_init + k_pen_finalize"}
+    stages = {}
+    for k, name in kernel_of.items():
+        ms = stage_ms[k]
+        stages[k] = {"kernel": name, "ms": ms, "algorithmic_bytes": sbytes[k],
+                     "gbs": sbytes[k] / (ms / 1000.0) / 1e9 if ms > 0 else None}
+    dom = max(("ladder", "verify", "pen_inside", "pen_min"), key=lambda k: stage_ms[k])
+    achieved = stages[dom]["gbs"]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "kernel": dominant,
-                "peak_source": peak_kind,
+                "frac": achieved / peak, "traffic": None, "kernel": stages[dom]["kernel"],
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "per_unit": ("48 B per ICP point-iteration (16 B source point + 32 B matched "
-                             "target point and normal), over the passes each rung ran"
-                             if dominant == "k_ladder" else
-                             "24 B per verification query"),
-                "ladder_ms": l_ms, "verify_ms": v_ms,
-                "verify_gbs": ver_bytes / (v_ms / 1000.0) / 1e9 if v_ms > 0 else None}
+                             "target point and normal) over the passes each rung ran"
+                             if dom == "ladder" else "24 B per query point"),
+                "stages": stages}
 
     if rank != 0:
         ctx.close()
@@ -323,7 +322,7 @@ def main():
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "timer": "host wall clock around the synchronous C-ABI call",
                 "matches_resident_run": same},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": 7 * args.steps,
         "roofline": roofline,
         "clocks": clocks,
         "cpu_baseline": cpu,

@@ -345,10 +345,14 @@ int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs,
 int sherd_batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
                        const sherd_work_item *items, uint32_t n_items,
                        const sherd_params *p, int sched, sherd_batch **out);
-/* Launches the batch and waits for it; the device milliseconds of the ladder
- * kernel, the verification kernel and both together are written to ms[0..2]
- * (CUDA events on the context's stream). */
-int sherd_batch_run(sherd_batch *batch, float ms[3]);
+/* Launches the batch and waits for it. `ms` (nullable) receives the device
+ * milliseconds of each stage, CUDA events on the context's stream:
+ * [0] ladder, [1] fracture/seam/continuity verification, [2] penetration
+ * box/parity/depth pass, [3] penetration minimum pass, [4] finalising pass,
+ * [5] the whole run. Under SHERD_SCHED_PLAIN only [5] is measured (the
+ * others are -1). */
+#define SHERD_BATCH_TIMES 6
+int sherd_batch_run(sherd_batch *batch, float ms[SHERD_BATCH_TIMES]);
 /* Copies the candidates of the last run to the host (n_items records). */
 int sherd_batch_results(sherd_batch *batch, sherd_candidate *out);
 int sherd_batch_free(sherd_batch *batch);

@@ -279,11 +279,13 @@ class Batch(_Handle):
                                                self.n, C.byref(params), int(sched), C.byref(h)))
         self.h = h
 
-    def run(self):
-        """Runs the batch; returns (ladder ms, verification ms, total ms) of device time."""
-        ms = np.zeros(3, np.float32)
+    STAGES = ("ladder", "verify", "pen_inside", "pen_min", "finalize", "total")
+
+    def run(self) -> dict:
+        """Runs the batch; returns the device milliseconds of each stage and of the run."""
+        ms = np.zeros(len(self.STAGES), np.float32)
         check(self.ctx.h, A.lib().sherd_batch_run(self.h, ms))
-        return tuple(float(x) for x in ms)
+        return {k: float(x) for k, x in zip(self.STAGES, ms)}
 
     def results(self):
         out = (A.Candidate * self.n)()

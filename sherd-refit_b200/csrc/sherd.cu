@@ -1245,26 +1245,28 @@ struct sherd_batch {
   unsigned grid_p = 1, grid_m = 1;
   unsigned grid_l = 1, grid_v = 1;
   uint32_t max_scratch = 64;
-  cudaGraph_t graph = nullptr, graph_v = nullptr;
-  cudaGraphExec_t exec = nullptr, exec_v = nullptr;
+  static constexpr int STAGES = 5;  // ladder, verify, pen inside, pen min, finalize
+  cudaGraph_t graph[STAGES] = {};
+  cudaGraphExec_t exec[STAGES] = {};
   uint32_t captured_timeout = 0xFFFFFFFFu;
-  cudaEvent_t e0 = nullptr, emid = nullptr, e1 = nullptr;
+  cudaEvent_t ev[STAGES + 1] = {};
   ~sherd_batch() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    if (exec_v) cudaGraphExecDestroy(exec_v);
-    if (graph_v) cudaGraphDestroy(graph_v);
-    if (e0) cudaEventDestroy(e0);
-    if (emid) cudaEventDestroy(emid);
-    if (e1) cudaEventDestroy(e1);
+    for (int k = 0; k < STAGES; ++k) {
+      if (exec[k]) cudaGraphExecDestroy(exec[k]);
+      if (graph[k]) cudaGraphDestroy(graph[k]);
+    }
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
   }
 };
 
 namespace {
 
-// The batched schedule as two graphs: the queue reset and the persistent
-// ladder kernel, then the persistent verification kernel; the host records an
-// event between them so each kernel's device time is known.
+// The batched schedule as five graphs, one per stage, so that the host can put
+// an event between them and every stage's device time is known: the queue
+// reset and the persistent ladder kernel; the persistent fracture, seam and
+// continuity kernel; the penetration box/parity/depth wavefront; its minimum
+// pass; the finalising pass.
 int launch_ladder(sherd_batch *b, cudaStream_t s) {
   sherd_ctx *ctx = b->ctx;
   unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
@@ -1276,7 +1278,7 @@ int launch_ladder(sherd_batch *b, cudaStream_t s) {
   return SHERD_OK;
 }
 
-int launch_verify(sherd_batch *b, cudaStream_t s) {
+int launch_verify_items(sherd_batch *b, cudaStream_t s) {
   sherd_ctx *ctx = b->ctx;
   unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
   QueueCtl qv{b->heads.p + 1, b->dorder.p, b->n_items, ctx->abort_dev, budget};
@@ -1284,7 +1286,17 @@ int launch_verify(sherd_batch *b, cudaStream_t s) {
       b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, b->inv.p,
       ctx->d_status);
   CK(cudaGetLastError());
-  PenState ps{b->deeper.p, b->deep.p, b->best.p, b->chunk0.p, 2 * b->n_items, b->n_chunks};
+  return SHERD_OK;
+}
+
+PenState pen_state(sherd_batch *b) {
+  return PenState{b->deeper.p, b->deep.p, b->best.p, b->chunk0.p, 2 * b->n_items, b->n_chunks};
+}
+
+int launch_pen_inside(sherd_batch *b, cudaStream_t s) {
+  sherd_ctx *ctx = b->ctx;
+  unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
+  PenState ps = pen_state(b);
   CK(cudaMemsetAsync(b->pen_heads.p, 0, 2 * sizeof(unsigned), s));
   k_pen_init<<<blocks_for(ps.n_units), 256, 0, s>>>(ps);
   CK(cudaGetLastError());
@@ -1292,6 +1304,15 @@ int launch_verify(sherd_batch *b, cudaStream_t s) {
     k_pen_inside<<<b->grid_p, 256, 0, s>>>(b->dv.p, b->di.p, b->dc.p, b->inv.p, ps, b->pen_heads.p,
                                          ctx->abort_dev, budget, ctx->d_status);
     CK(cudaGetLastError());
+  }
+  return SHERD_OK;
+}
+
+int launch_pen_min(sherd_batch *b, cudaStream_t s) {
+  sherd_ctx *ctx = b->ctx;
+  unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
+  PenState ps = pen_state(b);
+  if (b->n_chunks) {
     k_pen_seed<<<blocks_for(size_t(ps.n_units) * 32), 256, 0, s>>>(b->dv.p, b->di.p, b->dc.p,
                                                                   b->inv.p, ps, ctx->d_status);
     CK(cudaGetLastError());
@@ -1299,8 +1320,13 @@ int launch_verify(sherd_batch *b, cudaStream_t s) {
                                       b->pen_heads.p + 1, ctx->abort_dev, budget, ctx->d_status);
     CK(cudaGetLastError());
   }
-  k_pen_finalize<<<blocks_for(b->n_items), 256, 0, s>>>(b->dv.p, b->di.p, b->dc.p, ps, b->params,
-                                                       b->n_items);
+  return SHERD_OK;
+}
+
+int launch_finalize(sherd_batch *b, cudaStream_t s) {
+  sherd_ctx *ctx = b->ctx;
+  k_pen_finalize<<<blocks_for(b->n_items), 256, 0, s>>>(b->dv.p, b->di.p, b->dc.p, pen_state(b),
+                                                       b->params, b->n_items);
   CK(cudaGetLastError());
   return SHERD_OK;
 }
@@ -1326,12 +1352,15 @@ int capture_one(sherd_batch *b, int (*launch)(sherd_batch *, cudaStream_t), cuda
   return SHERD_OK;
 }
 
-// Captures both graphs (again when the time budget changed).
+// Captures every stage's graph (again when the time budget changed).
 int capture(sherd_batch *b) {
-  if (b->exec && b->exec_v && b->captured_timeout == b->ctx->timeout_ms) return SHERD_OK;
-  int rc = capture_one(b, launch_ladder, b->graph, b->exec);
-  if (rc) return rc;
-  if ((rc = capture_one(b, launch_verify, b->graph_v, b->exec_v))) return rc;
+  if (b->exec[0] && b->captured_timeout == b->ctx->timeout_ms) return SHERD_OK;
+  int (*stage[sherd_batch::STAGES])(sherd_batch *, cudaStream_t) = {
+      launch_ladder, launch_verify_items, launch_pen_inside, launch_pen_min, launch_finalize};
+  for (int k = 0; k < sherd_batch::STAGES; ++k) {
+    int rc = capture_one(b, stage[k], b->graph[k], b->exec[k]);
+    if (rc) return rc;
+  }
   b->captured_timeout = b->ctx->timeout_ms;
   return SHERD_OK;
 }
@@ -1421,15 +1450,13 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
   size_t slots = b->grid_l;
   for (uint32_t c : b->pair_count) slots = std::max<size_t>(slots, c);
   CK(b->hints.alloc(slots * b->hint_stride));
-  CK(cudaEventCreate(&b->e0));
-  CK(cudaEventCreate(&b->emid));
-  CK(cudaEventCreate(&b->e1));
+  for (cudaEvent_t &e : b->ev) CK(cudaEventCreate(&e));
   CK(cudaStreamSynchronize(ctx->stream));
   if (sched == SHERD_SCHED_BATCHED) return capture(b);
   return SHERD_OK;
 }
 
-int batch_run(sherd_batch *b, float ms[3]) {
+int batch_run(sherd_batch *b, float *ms) {
   sherd_ctx *ctx = b->ctx;
   __atomic_store_n(ctx->abort_host, 0u, __ATOMIC_SEQ_CST);
   int rc = begin(ctx);
@@ -1437,15 +1464,15 @@ int batch_run(sherd_batch *b, float ms[3]) {
   cudaStream_t s = ctx->stream;
   if (b->sched == SHERD_SCHED_BATCHED) {
     if ((rc = capture(b))) return rc;
-    CK(cudaEventRecord(b->e0, s));
-    CK(cudaGraphLaunch(b->exec, s));
-    CK(cudaEventRecord(b->emid, s));
-    CK(cudaGraphLaunch(b->exec_v, s));
-    CK(cudaEventRecord(b->e1, s));
+    CK(cudaEventRecord(b->ev[0], s));
+    for (int k = 0; k < sherd_batch::STAGES; ++k) {
+      CK(cudaGraphLaunch(b->exec[k], s));
+      CK(cudaEventRecord(b->ev[k + 1], s));
+    }
   } else {
     unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
     CK(cudaMemsetAsync(b->heads.p, 0, sizeof(unsigned) * 2 * b->n_pairs, s));
-    CK(cudaEventRecord(b->e0, s));
+    CK(cudaEventRecord(b->ev[0], s));
     for (uint32_t i = 0; i < b->n_pairs; ++i) {
       uint32_t cnt = b->pair_count[i];
       if (!cnt) continue;
@@ -1460,21 +1487,17 @@ int batch_run(sherd_batch *b, float ms[3]) {
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(s));
     }
-    CK(cudaEventRecord(b->e1, s));
+    CK(cudaEventRecord(b->ev[sherd_batch::STAGES], s));
   }
   rc = finish(ctx, b->sched == SHERD_SCHED_BATCHED ? "batch_batched" : "batch_plain", b->n_items,
               true);
   if (ms) {
-    float total = -1.0f, l = -1.0f, v = -1.0f;
-    cudaEventElapsedTime(&total, b->e0, b->e1);
-    if (b->sched == SHERD_SCHED_BATCHED) {
-      cudaEventElapsedTime(&l, b->e0, b->emid);
-      cudaEventElapsedTime(&v, b->emid, b->e1);
-    }
+    for (int k = 0; k < SHERD_BATCH_TIMES; ++k) ms[k] = -1.0f;
+    cudaEventElapsedTime(&ms[SHERD_BATCH_TIMES - 1], b->ev[0], b->ev[sherd_batch::STAGES]);
+    if (b->sched == SHERD_SCHED_BATCHED)
+      for (int k = 0; k < sherd_batch::STAGES; ++k)
+        cudaEventElapsedTime(&ms[k], b->ev[k], b->ev[k + 1]);
     cudaGetLastError();
-    ms[0] = l;
-    ms[1] = v;
-    ms[2] = total;
   }
   return rc;
 }
@@ -1518,7 +1541,7 @@ int sherd_batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pair
   return SHERD_OK;
 }
 
-int sherd_batch_run(sherd_batch *batch, float ms[3]) {
+int sherd_batch_run(sherd_batch *batch, float ms[SHERD_BATCH_TIMES]) {
   if (!batch) return SHERD_E_INVALID;
   std::lock_guard<std::mutex> lock(batch->ctx->mu);
   return batch_run(batch, ms);

@@ -75,6 +75,26 @@ def to_device(ctx: Context, wl, params: A.Params | None = None) -> DeviceCollect
                             n_src)
 
 
+def stage_bytes(wl, cands, n_src):
+    """Compulsory bytes of each stage of the batched path over the units in `cands`:
+    ladder: 48 B per ICP point-iteration (16 B source point, 32 B matched target point and
+    normal) over the passes each rung ran (iterations + 1); verify: 24 B per query of
+    |Pf_A| + |Pf_B| + |brk_A| + |Pm_B|; pen_inside: 24 B per surface sample |S_A| + |S_B|;
+    pen_min: 24 B per surface sample of the items whose two sides had nothing inside
+    (pen_depth <= 0; a lower bound of the points that pass scans)."""
+    pair = cands["pair"].astype(np.int64)
+    passes = cands["rungs"]["iterations"].astype(np.int64) + 1
+    src = np.stack([n_src[pair, 0], n_src[pair, 0], n_src[pair, 1], n_src[pair, 1]], axis=1)
+    fr = wl.fragments
+    ver = np.array([len(fr[p.a].pf) + len(fr[p.b].pf) + len(fr[p.a].brk_p) + len(fr[p.b].margin_p)
+                    for p in wl.pairs], np.float64)
+    surf = np.array([len(fr[p.a].s) + len(fr[p.b].s) for p in wl.pairs], np.float64)
+    none_inside = cands["scores"]["pen_depth"] <= 0.0
+    return {"ladder": float(np.sum(passes * src) * 48), "verify": float(np.sum(ver[pair]) * 24),
+            "pen_inside": float(np.sum(surf[pair]) * 24),
+            "pen_min": float(np.sum(surf[pair][none_inside]) * 24), "finalize": 0.0}
+
+
 def algorithmic_bytes(wl, cands, n_src):
     """Compulsory bytes of the verification units in `cands` (structured Candidate array):
     ICP: 48 B per point-iteration (16 B source point, 32 B matched target point + normal) over
