@@ -80,6 +80,24 @@ __device__ __forceinline__ float moller_trumbore(F3 o, F3 d, F3 v0, F3 v1, F3 v2
   return t > EPS ? t : -1.0f;
 }
 
+// moller_trumbore with the two edges already formed (e1 = v1 - v0 and
+// e2 = v2 - v0 in f32, the same values the test computes itself).
+__device__ __forceinline__ float moller_trumbore_edges(F3 o, F3 d, F3 v0, F3 e1, F3 e2) {
+  const float EPS = 1e-9f;
+  F3 pvec = cross(d, e2);
+  float det = dot(e1, pvec);
+  if (fabsf(det) < EPS) return -1.0f;
+  float inv = 1.0f / det;
+  F3 tvec = sub(o, v0);
+  float u = inv * dot(tvec, pvec);
+  if (!(u >= 0.0f && u <= 1.0f)) return -1.0f;
+  F3 qvec = cross(tvec, e1);
+  float v = inv * dot(d, qvec);
+  if (v < 0.0f || u + v > 1.0f) return -1.0f;
+  float t = inv * dot(e2, qvec);
+  return t > EPS ? t : -1.0f;
+}
+
 // Point-to-triangle distance: the Voronoi-region closest point of Ericson,
 // "Real-Time Collision Detection" 5.1.5, in f32 (the reference's scene is f32).
 __device__ __forceinline__ float tri_distance(F3 p, F3 a, F3 b, F3 c) {

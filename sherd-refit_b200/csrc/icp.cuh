@@ -50,6 +50,7 @@ __device__ bool solve_ldlt(const double a[6][6], const double b[6], double x[6])
   double m[6][6];
   for (int k = 0; k < 6; ++k)
     for (int l = 0; l < 6; ++l) m[k][l] = a[perm[k]][perm[l]];
+#pragma unroll 1
   for (int k = 0; k < 6; ++k) {
     if (k > 0) {
       double temp[6];
@@ -123,8 +124,10 @@ __device__ void matmul4(const double *a, const double *b, double *o) {
 }
 
 // The point-to-plane update from the pass sums (icp.rs:408-440): identity when
-// there is no correspondence, no normal or no finite solution.
-__device__ void plane_update(const double *s, bool has_normals, double u[16]) {
+// there is no correspondence, no normal or no finite solution. Run by one
+// thread per pass and kept out of line, so that its 6x6 working arrays do not
+// count against the registers of the point loops.
+__device__ __noinline__ void plane_update(const double *s, bool has_normals, double u[16]) {
   for (int i = 0; i < 16; ++i) u[i] = (i % 5 == 0) ? 1.0 : 0.0;
   if (s[0] == 0.0 || !has_normals) return;
   double a[6][6], rhs[6], x[6];
@@ -145,31 +148,41 @@ __device__ void plane_update(const double *s, bool has_normals, double u[16]) {
   }
 }
 
-// One correspondence pass (icp::correspondences + icp::normal_equations) over
-// `src` under the pose sh.t; leaves the block totals in sh.sums. `hint[i]`
-// carries each source point's last match (a target slot, or -1) from pass to
-// pass as the warm start of its search.
-__device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, double r2,
-                         bool valid, IcpShared &sh, int *hint, uint32_t &status) {
-  double acc[ICP_SUMS];
+// T <- U T for the update of the pass sums in sh (thread 0 only).
+__device__ __noinline__ void plane_step(IcpShared &sh, bool has_normals) {
+  double u[16];
+  plane_update(sh.sums, has_normals, u);
+  matmul4(u, sh.t, sh.t);
+}
+
+// Sums B..E-1 of one pass (count, err2, the 21 lower-triangle terms of J^T J
+// and the 6 of J^T r, in that order) over the correspondences found in hint[],
+// reduced over the warp into sh.red[warp][B..E). The squared distance is
+// re-formed exactly as the search formed it.
+template <int B, int E>
+__device__ __forceinline__ void icp_accumulate(const double4 *src, uint32_t ns, const CloudView &tgt,
+                                               const double *t, double r2, bool valid,
+                                               const int *hint, IcpShared &sh) {
+  double acc[E - B];
 #pragma unroll
-  for (int k = 0; k < ICP_SUMS; ++k) acc[k] = 0.0;
-  double t[12];
-#pragma unroll
-  for (int k = 0; k < 12; ++k) t[k] = sh.t[k];
+  for (int k = 0; k < E - B; ++k) acc[k] = 0.0;
   if (valid) {
     for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) {
+      int s = hint[i];
+      if (s < 0) continue;
       double4 p = src[i];
       double x, y, z;
       apply_pose(t, p.x, p.y, p.z, x, y, z);
-      double d2;
-      int s = nearest_within_sq(tgt, x, y, z, r2, d2, status, hint[i]);
-      hint[i] = s;
-      if (s < 0 || !(d2 < r2)) continue;
-      acc[0] += 1.0;
-      acc[1] += d2;
+      double4 q = tgt.pts[s];
+      double dx = x - q.x, dy = y - q.y, dz = z - q.z;
+      double d2 = (dx * dx + dy * dy) + dz * dz;
+      if (!(d2 < r2)) continue;
+      double v[ICP_SUMS];
+      v[0] = 1.0;
+      v[1] = d2;
+#pragma unroll
+      for (int m = 2; m < ICP_SUMS; ++m) v[m] = 0.0;
       if (tgt.nrm) {
-        double4 q = tgt.pts[s];
         double4 n = tgt.nrm[s];
         double row[6] = {y * n.z - z * n.y, z * n.x - x * n.z, x * n.y - y * n.x, n.x, n.y, n.z};
         double r = (x - q.x) * n.x + (y - q.y) * n.y + (z - q.z) * n.z;
@@ -177,20 +190,49 @@ __device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, 
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
 #pragma unroll
-          for (int l = 0; l <= k; ++l) acc[m++] += row[k] * row[l];
+          for (int l = 0; l <= k; ++l) v[m++] = row[k] * row[l];
         }
 #pragma unroll
-        for (int k = 0; k < 6; ++k) acc[23 + k] += row[k] * r;
+        for (int k = 0; k < 6; ++k) v[23 + k] = row[k] * r;
       }
+#pragma unroll
+      for (int k = 0; k < E - B; ++k) acc[k] += v[B + k];
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < ICP_SUMS; ++k) {
-    double v = acc[k];
-    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) sh.red[warp][k] = v;
+  for (int k = 0; k < E - B; ++k) {
+    double x = acc[k];
+    for (int o = 16; o; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh.red[warp][B + k] = x;
   }
+}
+
+// One correspondence pass (icp::correspondences + icp::normal_equations) over
+// `src` under the pose sh.t; leaves the block totals in sh.sums. `hint[i]`
+// carries each source point's last match (a target slot, or -1) from pass to
+// pass as the warm start of its search.
+__device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, double r2,
+                         bool valid, IcpShared &sh, int *hint, uint32_t &status) {
+  double t[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) t[k] = sh.t[k];
+  // Two kinds of loops over the moving points, so that the 29 accumulators are
+  // never live across the nearest-neighbour search: the first finds every
+  // point's match (kept in hint[i], which also warm-starts the next pass), the
+  // others re-form the moved point and add each correspondence into half of
+  // the sums; every thread adds its points into each sum in the same order.
+  if (valid) {
+    for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) {
+      double4 p = src[i];
+      double x, y, z;
+      apply_pose(t, p.x, p.y, p.z, x, y, z);
+      double d2;
+      hint[i] = nearest_within_sq(tgt, x, y, z, r2, d2, status, hint[i]);
+    }
+  }
+  icp_accumulate<0, 15>(src, ns, tgt, t, r2, valid, hint, sh);
+  icp_accumulate<15, ICP_SUMS>(src, ns, tgt, t, r2, valid, hint, sh);
   __syncthreads();
   if (threadIdx.x < ICP_SUMS) {
     double v = sh.red[0][threadIdx.x];
@@ -238,11 +280,7 @@ __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView 
   uint32_t iterations = 0;
   bool converged = false;
   for (int it = 0; it < max_iter; ++it) {
-    if (threadIdx.x == 0) {
-      double u[16];
-      plane_update(sh.sums, tgt.nrm != nullptr, u);
-      matmul4(u, sh.t, sh.t);
-    }
+    if (threadIdx.x == 0) plane_step(sh, tgt.nrm != nullptr);
     __syncthreads();
     icp_pass(src, ns, tgt, r2, valid, sh, hint, status);
     ++iterations;

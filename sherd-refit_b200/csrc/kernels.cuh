@@ -315,7 +315,7 @@ __device__ __forceinline__ bool take(const QueueCtl &q, unsigned long long start
 }
 
 // R 5.6's four point-to-plane rungs per (pair, start) (ladder.rs:142-161).
-__global__ void __launch_bounds__(ICP_BLOCK, 4) k_ladder(const PairView *pairs,
+__global__ void __launch_bounds__(ICP_BLOCK, 6) k_ladder(const PairView *pairs,
                                                       const sherd_work_item *items, QueueCtl q,
                                                       int *hints, size_t hint_stride,
                                                       sherd_candidate *out, uint32_t *status) {

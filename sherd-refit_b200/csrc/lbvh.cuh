@@ -32,8 +32,9 @@ struct __align__(16) BNode {
 // (CSR) the sorted slots of every face whose padded projected rectangle
 // touches it. An axis ray from p can only cross faces in p's own cell.
 struct AxisGrid {
-  const uint32_t *start;  // nu * nv + 1 offsets
-  const uint32_t *slot;   // face slots
+  const uint32_t *start;  // nu * nv + 1 offsets into the entry arrays
+  const float4 *rect;     // per entry: the face's padded projected rectangle (u0, u1, v0, v1)
+  const float4 *tri;      // per entry, 3 float4: v0, e1 = v1 - v0, e2 = v2 - v0 (f32)
   float lo_u, lo_v, inv_cell;
   uint32_t nu, nv;
 };
@@ -353,14 +354,32 @@ __global__ void k_grid_count(const float4 *tri, uint32_t nf, int axis, AxisGrid 
     for (int v = v0; v <= v1; ++v) atomicAdd(&count[size_t(u) * g.nv + v], 1u);
 }
 
+// Writes every face's entries: its padded projected rectangle and its vertex
+// and edges, so the parity test reads one contiguous run per cell.
 __global__ void k_grid_fill(const float4 *tri, uint32_t nf, int axis, AxisGrid g, float pad,
-                            unsigned *cursor, uint32_t *slot) {
+                            unsigned *cursor, float4 *rect, float4 *edge) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nf) return;
   int u0, u1, v0, v1;
   grid_rect(tri, s, axis, g, pad, u0, u1, v0, v1);
+  int au = (axis + 1) % 3, av = (axis + 2) % 3;
+  float4 a = tri[3 * s], b = tri[3 * s + 1], c = tri[3 * s + 2];
+  float ac[3] = {a.x, a.y, a.z}, bc[3] = {b.x, b.y, b.z}, cc[3] = {c.x, c.y, c.z};
+  float4 r = make_float4(__fsub_rd(fminf(ac[au], fminf(bc[au], cc[au])), pad),
+                         __fadd_ru(fmaxf(ac[au], fmaxf(bc[au], cc[au])), pad),
+                         __fsub_rd(fminf(ac[av], fminf(bc[av], cc[av])), pad),
+                         __fadd_ru(fmaxf(ac[av], fmaxf(bc[av], cc[av])), pad));
+  float4 t0 = make_float4(a.x, a.y, a.z, 0.0f);
+  float4 t1 = make_float4(b.x - a.x, b.y - a.y, b.z - a.z, 0.0f);
+  float4 t2 = make_float4(c.x - a.x, c.y - a.y, c.z - a.z, 0.0f);
   for (int u = u0; u <= u1; ++u)
-    for (int v = v0; v <= v1; ++v) slot[atomicAdd(&cursor[size_t(u) * g.nv + v], 1u)] = s;
+    for (int v = v0; v <= v1; ++v) {
+      unsigned k = atomicAdd(&cursor[size_t(u) * g.nv + v], 1u);
+      rect[k] = r;
+      edge[3 * size_t(k)] = t0;
+      edge[3 * size_t(k) + 1] = t1;
+      edge[3 * size_t(k) + 2] = t2;
+    }
 }
 
 __global__ void k_store_tris(const float *v, const uint32_t *f, const uint32_t *sorted, uint32_t nf,

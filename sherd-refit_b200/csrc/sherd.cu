@@ -181,7 +181,8 @@ struct sherd_mesh {
   std::vector<uint32_t> hf;  // host copy of the faces
   DBuf<BNode> nodes;
   DBuf<float4> tri;
-  DBuf<uint32_t> gstart[3], gslot[3];
+  DBuf<uint32_t> gstart[3];
+  DBuf<float4> grect[3], gtri[3];
   MeshView view{};
 };
 
@@ -353,15 +354,17 @@ int mesh_build(sherd_ctx *ctx, sherd_mesh *m) {
     uint32_t total = 0;
     CK(cudaMemcpyAsync(&total, m->gstart[axis].p + cells, 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    CK(m->gslot[axis].alloc(std::max<uint32_t>(total, 1)));
+    CK(m->grect[axis].alloc(std::max<uint32_t>(total, 1)));
+    CK(m->gtri[axis].alloc(3 * size_t(std::max<uint32_t>(total, 1))));
     CK(cudaMemcpyAsync(count.p, m->gstart[axis].p, sizeof(unsigned) * cells, cudaMemcpyDeviceToDevice,
                        ctx->stream));
     k_grid_fill<<<blocks_for(nf), 256, 0, ctx->stream>>>(m->tri.p, nf, axis, g, pad, count.p,
-                                                        m->gslot[axis].p);
+                                                        m->grect[axis].p, m->gtri[axis].p);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
     g.start = m->gstart[axis].p;
-    g.slot = m->gslot[axis].p;
+    g.rect = m->grect[axis].p;
+    g.tri = m->gtri[axis].p;
     m->view.grid[axis] = g;
   }
   MeshView &v = m->view;

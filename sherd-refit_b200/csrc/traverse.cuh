@@ -162,18 +162,14 @@ __device__ __noinline__ uint32_t crossings_axis(const MeshView &m, F3 p, int axi
   uint32_t b = __ldg(g.start + cell), e = __ldg(g.start + cell + 1);
   F3 d = {axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f};
   uint32_t hits = 0;
-  int au = (axis + 1) % 3, av = (axis + 2) % 3;
   for (uint32_t k = b; k < e; ++k) {
-    F3 a, bb, c;
-    uint32_t id;
-    tri_at(m, __ldg(g.slot + k), a, bb, c, id);
-    float ac[3] = {a.x, a.y, a.z}, bc[3] = {bb.x, bb.y, bb.z}, cc[3] = {c.x, c.y, c.z};
-    float umin = __fsub_rd(fminf(ac[au], fminf(bc[au], cc[au])), m.pad);
-    float umax = __fadd_ru(fmaxf(ac[au], fmaxf(bc[au], cc[au])), m.pad);
-    float vmin = __fsub_rd(fminf(ac[av], fminf(bc[av], cc[av])), m.pad);
-    float vmax = __fadd_ru(fmaxf(ac[av], fmaxf(bc[av], cc[av])), m.pad);
-    if (pu < umin || pu > umax || pv < vmin || pv > vmax) continue;
-    if (moller_trumbore(p, d, a, bb, c) >= 0.0f) ++hits;
+    float4 r = __ldg(g.rect + k);
+    if (pu < r.x || pu > r.y || pv < r.z || pv > r.w) continue;
+    float4 t0 = __ldg(g.tri + 3 * size_t(k)), t1 = __ldg(g.tri + 3 * size_t(k) + 1),
+           t2 = __ldg(g.tri + 3 * size_t(k) + 2);
+    if (moller_trumbore_edges(p, d, {t0.x, t0.y, t0.z}, {t1.x, t1.y, t1.z}, {t2.x, t2.y, t2.z}) >=
+        0.0f)
+      ++hits;
   }
   (void)status;
   return hits;
