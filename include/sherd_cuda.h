@@ -137,7 +137,8 @@ typedef struct sherd_batch sherd_batch;       /* a device-resident stage-2 batch
 
 /* Opens device `device` (cudaSetDevice) and creates a context with its own
  * stream. Replaces the reference's backend resolution of a GPU executor
- * (crates/sherd-backend/src/lib.rs:377-484): it fails instead of falling back. */
+ * (crates/sherd-backend/src/lib.rs:203-318): it fails instead of falling back,
+ * as `--backend gpu` does (lib.rs:233-237). */
 int sherd_open(int device, sherd_ctx **out);
 int sherd_close(sherd_ctx *ctx);
 /* Message of the calling thread's last failure on this context ("" if none). */
@@ -327,9 +328,11 @@ int sherd_pair_free(sherd_pair *pair);
 /* R 5.6 + R 6 + R 6.5 for every (pair, start): the four point-to-plane rungs
  * (0.2 t, 0.08 t on pc_reg; 0.08 t, 0.04 t on pc_frac; 30 iterations each,
  * ladder.rs:51-61, 142-161), the full verification at the last pose and the
- * verdict. SHERD_SCHED_BATCHED runs every item in persistent kernels fed by a
- * device work queue, captured as one CUDA graph; SHERD_SCHED_PLAIN launches
- * the same kernels once per pair and synchronises between pairs. */
+ * verdict. SHERD_SCHED_BATCHED runs every item in persistent kernels fed by
+ * device work queues, one captured CUDA graph per stage (ladder, fracture/seam/
+ * continuity scores, penetration inside tests, penetration minimum distances,
+ * verdicts); SHERD_SCHED_PLAIN launches the ladder and verification kernels
+ * once per pair and synchronises between pairs. */
 int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs,
                               uint32_t n_pairs, const sherd_work_item *items,
                               uint32_t n_items, const sherd_params *p, int sched,
@@ -337,8 +340,8 @@ int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs,
 
 /* A stage-2 batch made resident on the device: the pair views, work items,
  * queue order, candidate records and per-CTA scratch are uploaded and sized
- * once, and SHERD_SCHED_BATCHED captures the queue reset and the two
- * persistent kernels (ladder, verification) as one CUDA graph. Running it
+ * once, and SHERD_SCHED_BATCHED captures each stage (queue resets and its
+ * persistent kernels) as a CUDA graph, five in all. Running it
  * again recomputes every candidate from the same resident inputs. This is the
  * device-side form of sherd_ladder_verify_batch, for callers that keep their
  * inputs on the GPU between calls. */
