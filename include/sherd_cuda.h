@@ -360,6 +360,39 @@ int sherd_batch_run(sherd_batch *batch, float ms[SHERD_BATCH_TIMES]);
 int sherd_batch_results(sherd_batch *batch, sherd_candidate *out);
 int sherd_batch_free(sherd_batch *batch);
 
+/* ---- differentiation: the adjoint of two group-alignment objectives ----- */
+
+/* Options of sherd_adjoint. No counterpart in the reference: the objectives
+ * are built from R 6's tight fraction (verify.rs:338-349) and the ICP's
+ * point-to-plane residual (icp.rs:361-392, 599-640). */
+typedef struct sherd_adjoint_options {
+    double radius_k; /* correspondence radius in units of t * Scales::icp (0.04: the last rung) */
+    double width_k;  /* sigmoid width w in units of t (0.01)                               */
+    double window_k; /* distances beyond facing + window_k * w are left out (30)           */
+} sherd_adjoint_options;
+#define SHERD_ADJOINT_VALUES 5
+
+/* For every group pose g and edge e (a pair: A fixed, B moving, its Scales):
+ * values[(g * n_edges + e) * 5 + k], k =
+ *   0  E   = 1/2 sum r^2, r = (T x - q) . n over B's fracture samples x whose
+ *          nearest A fracture sample q is strictly within the radius;
+ *   1  T_B = sum sigmoid((tight - d) / w), 2 F_B = sum sigmoid((facing - d) / w)
+ *          over B's fracture samples moved by T, d = sqrt(dist^2 + (w/10)^2)
+ *          their softened distance to A's fracture faces; T_B / F_B is R 6's
+ *          tight fraction, smoothed;
+ *   3  T_A, 4 F_A the same for A's samples moved by T^-1 against B's faces;
+ * and grads[((g * n_edges + e) * 5 + k) * 6 + j] = d values[k] / d xi_j, xi =
+ * (w, v) the left twist of the pose that moves the points, expressed in the
+ * fixed fragment's frame: T -> exp(xi^) T for k = 0, 1, 2 (A's frame) and
+ * T^-1 -> exp(xi^) T^-1 for k = 3, 4 (B's frame). For k = 0 it is the ICP's
+ * J^T r (icp.rs:616-624). Matches and nearest faces are held fixed (exact
+ * gradients of a piecewise-smooth objective); the distance to the assigned
+ * face is f64. `poses` and `inverses` are n_poses * n_edges row-major 4x4 T
+ * and T^-1. Nothing is stored between calls. */
+int sherd_adjoint(sherd_ctx *ctx, sherd_pair *const *edges, uint32_t n_edges,
+                  const double *poses, const double *inverses, uint32_t n_poses,
+                  const sherd_adjoint_options *opt, double *values, double *grads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,10 @@ class Candidate(C.Structure):
                 ("status", C.c_uint32), ("rungs", Registration * 4), ("scores", Scores)]
 
 
+class AdjointOptions(C.Structure):
+    _fields_ = [("radius_k", C.c_double), ("width_k", C.c_double), ("window_k", C.c_double)]
+
+
 class InsideOutcome(C.Structure):
     _fields_ = [("depth", C.c_float), ("inside", C.c_uint32)]
 
@@ -123,6 +127,9 @@ def lib() -> C.CDLL:
         "or_tri_distance": (C.c_float, [F32P, F32P, F32P, F32P]),
         "or_moller_trumbore": (C.c_float, [F32P, F32P, F32P, F32P, F32P]),
         "or_default_threads": (C.c_int, []),
+        "or_adjoint": (None, [vp, F64P, F64P, C.POINTER(AdjointOptions), C.c_int, I32P, F64P,
+                              F64P]),
+        "or_normal_equations": (None, [F64P, C.c_uint32, vp, F64P, C.c_double, F64P, F64P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -282,6 +289,33 @@ class Pair:
         if getattr(self, "h", None):
             lib().or_pair_free(self.h)
             self.h = None
+
+
+def adjoint(pair: Pair, t, t_inv, opts: AdjointOptions, assign=None):
+    """The group-alignment objectives of one pair at pose t (B into A) and t_inv: values (5,)
+    = E, T_B, F_B, T_A, F_A and their twist gradients (5, 6). Returns (values, grads, assign);
+    passing `assign` back holds the matches and faces fixed (for finite differences)."""
+    a_pf = pair.keep[0].arrays[0]
+    b_pf = pair.keep[1].arrays[0]
+    n = len(pair.fs) + len(b_pf) + len(a_pf)
+    frozen = assign is not None
+    assign = np.ascontiguousarray(assign, np.int32) if frozen else np.empty(n, np.int32)
+    assert len(assign) == n
+    values = np.empty(5)
+    grads = np.empty((5, 6))
+    lib().or_adjoint(pair.h, f64(t).reshape(16), f64(t_inv).reshape(16), C.byref(opts),
+                     int(frozen), assign, values, grads)
+    return values, grads, assign
+
+
+def normal_equations(source, target: Cloud, pose, distance):
+    """icp::correspondences + normal_equations at `pose`: (J^T J (6, 6), J^T r (6,))."""
+    src = f64(source).reshape(-1, 3)
+    jtj = np.empty((6, 6))
+    jtr = np.empty(6)
+    lib().or_normal_equations(src, len(src), target.h, f64(pose).reshape(16), float(distance),
+                              jtj, jtr)
+    return jtj, jtr
 
 
 def ladder_verify_batch(pairs, items, params: Params, threads=0):

@@ -443,6 +443,38 @@ struct Mesh {
     }
     return best;
   }
+
+  // distance() that also names the face: the nearest face within the window,
+  // an exact f32 tie going to the lowest face id; MISS-like 0xFFFFFFFF when
+  // nothing is within the window.
+  float nearest_face(V3f p, float window, uint32_t *face_out) const {
+    *face_out = 0xFFFFFFFFu;
+    if (nodes.empty() || !(window > 0.0f)) return F_INF;
+    float best = F_INF;
+    float pf[3] = {p.x, p.y, p.z};
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+      const TriNode &n = nodes[stack[--sp]];
+      double bound = std::min(double(best), double(window));
+      if (box_dist(n, pf) > bound + pad) continue;
+      if (n.left < 0) {
+        for (uint32_t i = n.first; i < n.first + n.count; ++i) {
+          uint32_t face = order[i];
+          float dd = tri_distance(p, vert(face, 0), vert(face, 1), vert(face, 2));
+          if (dd <= window && (dd < best || (dd == best && face < *face_out))) {
+            best = dd;
+            *face_out = face;
+          }
+        }
+      } else {
+        stack[sp++] = n.left;
+        stack[sp++] = n.right;
+      }
+    }
+    return best;
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -673,11 +705,15 @@ void correspondences(const std::vector<double> &moved, const Cloud &tgt, double 
 
 // icp::point_to_plane (icp.rs:408-440) with normal_equations (icp.rs:599-640)
 // under Assembly::World and Precision::F64.
-void point_to_plane(const std::vector<double> &moved, const Cloud &tgt,
-                    const std::vector<Corr> &corr, double u[16]) {
-  for (int i = 0; i < 16; ++i) u[i] = (i % 5 == 0) ? 1.0 : 0.0;
-  if (corr.empty() || tgt.n.size() != tgt.p.size()) return;
-  double jtj[6][6] = {}, jtr[6] = {};
+// icp::normal_equations (icp.rs:599-640) under Assembly::World and
+// Precision::F64: J^T J (lower triangle) and J^T r, rows (p x n, n), in
+// correspondence order.
+void normal_equations(const std::vector<double> &moved, const Cloud &tgt,
+                      const std::vector<Corr> &corr, double jtj[6][6], double jtr[6]) {
+  for (int k = 0; k < 6; ++k) {
+    jtr[k] = 0.0;
+    for (int l = 0; l < 6; ++l) jtj[k][l] = 0.0;
+  }
   for (const Corr &c : corr) {
     const double *p = &moved[3 * c.i], *q = &tgt.p[3 * c.j], *n = &tgt.n[3 * c.j];
     double pc[3] = {p[0] - 0.0, p[1] - 0.0, p[2] - 0.0};
@@ -689,6 +725,14 @@ void point_to_plane(const std::vector<double> &moved, const Cloud &tgt,
       jtr[k] = jtr[k] + row[k] * r;
     }
   }
+}
+
+void point_to_plane(const std::vector<double> &moved, const Cloud &tgt,
+                    const std::vector<Corr> &corr, double u[16]) {
+  for (int i = 0; i < 16; ++i) u[i] = (i % 5 == 0) ? 1.0 : 0.0;
+  if (corr.empty() || tgt.n.size() != tgt.p.size()) return;
+  double jtj[6][6], jtr[6];
+  normal_equations(moved, tgt, corr, jtj, jtr);
   double a[6][6];
   for (int k = 0; k < 6; ++k)
     for (int l = 0; l <= k; ++l) {
@@ -973,6 +1017,104 @@ uint32_t accept(const sherd_scores &s, const sherd_params &p, const sherd_scales
           s.seam >= p.min_seam && s.cont_n >= p.min_cont_n)
              ? 1u
              : 0u;
+}
+
+// ---------------------------------------------------------------------------
+// The adjoint of the group-alignment objectives (no reference function: the
+// values are R 6's tight fraction, smoothed, and the ICP's point-to-plane
+// residual; the gradients are taken with the assignment held fixed)
+// ---------------------------------------------------------------------------
+
+// Ericson, Real-Time Collision Detection, sec. 5.1.5, in f64.
+void closest_on_triangle(const double *p, const double *a, const double *b, const double *c,
+                         double *q) {
+  auto dot3 = [](const double *u, const double *v) { return (u[0] * v[0] + u[1] * v[1]) + u[2] * v[2]; };
+  auto put = [&](const double *o, const double *e1, double s1, const double *e2, double s2) {
+    for (int k = 0; k < 3; ++k) q[k] = (o[k] + e1[k] * s1) + e2[k] * s2;
+  };
+  const double z[3] = {0.0, 0.0, 0.0};
+  double ab[3], ac[3], ap[3], bp[3], cp[3];
+  for (int k = 0; k < 3; ++k) {
+    ab[k] = b[k] - a[k];
+    ac[k] = c[k] - a[k];
+    ap[k] = p[k] - a[k];
+    bp[k] = p[k] - b[k];
+    cp[k] = p[k] - c[k];
+  }
+  double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+  if (d1 <= 0.0 && d2 <= 0.0) return put(a, z, 0.0, z, 0.0);
+  double d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+  if (d3 >= 0.0 && d4 <= d3) return put(b, z, 0.0, z, 0.0);
+  double vc = d1 * d4 - d3 * d2;
+  if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) return put(a, ab, d1 / (d1 - d3), z, 0.0);
+  double d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+  if (d6 >= 0.0 && d5 <= d6) return put(c, z, 0.0, z, 0.0);
+  double vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) return put(a, ac, d2 / (d2 - d6), z, 0.0);
+  double va = d3 * d6 - d5 * d4;
+  double e43 = d4 - d3, e56 = d5 - d6;
+  if (va <= 0.0 && e43 >= 0.0 && e56 >= 0.0) {
+    double bc[3] = {c[0] - b[0], c[1] - b[1], c[2] - b[2]};
+    return put(b, bc, e43 / (e43 + e56), z, 0.0);
+  }
+  double den = (va + vb) + vc;
+  put(a, ab, vb / den, ac, vc / den);
+}
+
+void add_twist(double *acc, const double *p, const double *g) {
+  acc[0] += p[1] * g[2] - p[2] * g[1];
+  acc[1] += p[2] * g[0] - p[0] * g[2];
+  acc[2] += p[0] * g[1] - p[1] * g[0];
+  acc[3] += g[0];
+  acc[4] += g[1];
+  acc[5] += g[2];
+}
+
+struct AdjointSide {
+  const std::vector<double> *pts;  // the moving fragment's fracture samples (its own frame)
+  const Mesh *scene;               // the fixed fragment's fracture faces
+};
+
+// The two smoothed counts of one side and their twist gradients; `assign`
+// (per point, a face id or -1) is filled, or read when `frozen`.
+void adjoint_side(const AdjointSide &side, const double *m, const sherd_scales &sc, double w,
+                  double window_k, bool frozen, int32_t *assign, double *val2, double *grad12) {
+  float window = float(sc.facing + window_k * w);
+  size_t n = side.pts->size() / 3;
+  for (size_t i = 0; i < n; ++i) {
+    double p[3];
+    apply(m, &(*side.pts)[3 * i], p);
+    uint32_t face;
+    if (frozen) {
+      if (assign[i] < 0) continue;
+      face = uint32_t(assign[i]);
+    } else {
+      side.scene->nearest_face(narrow(p), window, &face);
+      assign[i] = face == 0xFFFFFFFFu ? -1 : int32_t(face);
+      if (face == 0xFFFFFFFFu) continue;
+    }
+    double v[3][3];
+    for (int k = 0; k < 3; ++k) {
+      V3f x = side.scene->vert(face, k);
+      v[k][0] = x.x;
+      v[k][1] = x.y;
+      v[k][2] = x.z;
+    }
+    double q[3];
+    closest_on_triangle(p, v[0], v[1], v[2], q);
+    double dv[3] = {p[0] - q[0], p[1] - q[1], p[2] - q[2]};
+    // The softened distance sqrt(|p - c|^2 + (w/10)^2): smooth where a sample crosses.
+    double d = std::sqrt(((dv[0] * dv[0] + dv[1] * dv[1]) + dv[2] * dv[2]) + 0.01 * w * w);
+    double st = 1.0 / (1.0 + std::exp(-((sc.tight - d) / w)));
+    double sf = 1.0 / (1.0 + std::exp(-((sc.facing - d) / w)));
+    val2[0] += st;
+    val2[1] += sf;
+    double kt = -st * (1.0 - st) / (w * d), kf = -sf * (1.0 - sf) / (w * d);
+    double gt[3] = {kt * dv[0], kt * dv[1], kt * dv[2]};
+    double gf[3] = {kf * dv[0], kf * dv[1], kf * dv[2]};
+    add_twist(grad12, p, gt);
+    add_twist(grad12 + 6, p, gf);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1438,5 +1580,66 @@ float or_moller_trumbore(const float *o, const float *d, const float *a, const f
 }
 
 int or_default_threads(void) { return default_threads(); }
+
+// The adjoint of the group-alignment objectives for one pair at pose t (B's
+// frame into A's) and t_inv: values[5] = E, T_B, F_B, T_A, F_A and grads[30],
+// six twist components per value (the CUDA backend's sherd_adjoint). The
+// assignment (per B fracture source point its target index, per B and A
+// fracture sample its face id, -1 for none) is written, or read when frozen.
+void or_adjoint(const void *pair, const double *t, const double *t_inv,
+                const sherd_adjoint_options *o, int frozen, int32_t *assign, double *values,
+                double *grads) {
+  const Pair &pr = *static_cast<const Pair *>(pair);
+  std::fill(values, values + 5, 0.0);
+  std::fill(grads, grads + 30, 0.0);
+  const sherd_scales &sc = pr.sc;
+  size_t nf = pr.frac_source.size() / 3, nb = pr.b->pf.size() / 3;
+  double r = o->radius_k * sc.t * sc.icp, r2 = r * r;
+  const Cloud &tgt = *pr.frac_target;
+  for (size_t i = 0; i < nf; ++i) {
+    double p[3];
+    apply(t, &pr.frac_source[3 * i], p);
+    uint32_t j;
+    if (frozen) {
+      if (assign[i] < 0) continue;
+      j = uint32_t(assign[i]);
+    } else {
+      double d2;
+      if (!tgt.nearest_within_sq(p, r2, &j, &d2) || !(d2 < r2)) {
+        assign[i] = -1;
+        continue;
+      }
+      assign[i] = int32_t(j);
+    }
+    const double *q = &tgt.p[3 * j], *n = &tgt.n[3 * j];
+    double res = ((p[0] - q[0]) * n[0] + (p[1] - q[1]) * n[1]) + (p[2] - q[2]) * n[2];
+    values[0] += 0.5 * res * res;
+    double g[3] = {res * n[0], res * n[1], res * n[2]};
+    add_twist(grads, p, g);
+  }
+  double w = o->width_k * sc.t;
+  adjoint_side({&pr.b->pf, pr.a->fracture}, t, sc, w, o->window_k,
+               frozen != 0, assign + nf, values + 1, grads + 6);
+  adjoint_side({&pr.a->pf, pr.b->fracture}, t_inv, sc, w, o->window_k, frozen != 0,
+               assign + nf + nb, values + 3, grads + 18);
+}
+
+// icp::correspondences + icp::normal_equations at `pose` (icp.rs:361-392,
+// 599-640): J^T J (36, symmetric) and J^T r of the point-to-plane system.
+void or_normal_equations(const double *src, uint32_t ns, const void *target, const double *pose,
+                         double distance, double *jtj36, double *jtr6) {
+  const Cloud &tgt = *static_cast<const Cloud *>(target);
+  std::vector<double> moved(src, src + size_t(3) * ns);
+  transform_points(moved, pose);
+  std::vector<Corr> corr;
+  double fit, rmse;
+  correspondences(moved, tgt, distance, corr, &fit, &rmse);
+  double jtj[6][6], jtr[6];
+  normal_equations(moved, tgt, corr, jtj, jtr);
+  for (int k = 0; k < 6; ++k) {
+    jtr6[k] = jtr[k];
+    for (int l = 0; l <= k; ++l) jtj36[6 * k + l] = jtj36[6 * l + k] = jtj[k][l];
+  }
+}
 
 }  // extern "C"

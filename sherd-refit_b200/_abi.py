@@ -96,6 +96,12 @@ class Candidate(C.Structure):
                 ("status", C.c_uint32), ("rungs", Registration * 4), ("scores", Scores)]
 
 
+class AdjointOptions(C.Structure):
+    _fields_ = [("radius_k", C.c_double), ("width_k", C.c_double), ("window_k", C.c_double)]
+
+
+ADJOINT_VALUES = 5
+
 _lib = None
 
 _SIGNATURES = {
@@ -150,6 +156,8 @@ _SIGNATURES = {
     "sherd_batch_run": (C.c_int, [VP, np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")]),
     "sherd_batch_results": (C.c_int, [VP, VP]),
     "sherd_batch_free": (C.c_int, [VP]),
+    "sherd_adjoint": (C.c_int, [VP, VP, C.c_uint32, F64P, F64P, C.c_uint32,
+                                C.POINTER(AdjointOptions), F64P, F64P]),
 }
 
 

@@ -234,6 +234,26 @@ class Context:
                                                        C.cast(out, C.c_void_p)))
         return out
 
+    # -- differentiation ------------------------------------------------------------------------
+    def adjoint(self, edges, poses, inverses, opts: A.AdjointOptions):
+        """The group-alignment objectives of every (pose, edge): `poses` and `inverses` are
+        (P, E, 4, 4) arrays of T (B's frame into A's) and T^-1 for the E pairs in `edges`.
+        Returns values (P, E, 5) = E, T_B, F_B, T_A, F_A and their twist gradients (P, E, 5, 6):
+        the first three in A's frame (T -> exp(xi^) T), the last two in B's (T^-1 ->
+        exp(xi^) T^-1)."""
+        n_e = len(edges)
+        poses = np.ascontiguousarray(poses, np.float64).reshape(-1, n_e, 16)
+        inverses = np.ascontiguousarray(inverses, np.float64).reshape(-1, n_e, 16)
+        if poses.shape != inverses.shape:
+            raise A.SherdError(A.E_INVALID, "poses and inverses differ in shape")
+        n_p = poses.shape[0]
+        values = np.empty((n_p, n_e, A.ADJOINT_VALUES))
+        grads = np.empty((n_p, n_e, A.ADJOINT_VALUES, 6))
+        arr = (C.c_void_p * max(n_e, 1))(*[e.h for e in edges])
+        check(self.h, A.lib().sherd_adjoint(self.h, arr, n_e, poses, inverses, n_p, C.byref(opts),
+                                            values, grads))
+        return values, grads
+
 
 WORK_ITEM = np.dtype(A.WorkItem)
 CANDIDATE = np.dtype(A.Candidate)

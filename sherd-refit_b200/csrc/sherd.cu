@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "adjoint.cuh"
 
 using namespace sherd;
 
@@ -1584,6 +1585,50 @@ int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return SHERD_OK;
+}
+
+// ---- differentiation ----------------------------------------------------------
+
+int sherd_adjoint(sherd_ctx *ctx, sherd_pair *const *edges, uint32_t n_edges, const double *poses,
+                  const double *inverses, uint32_t n_poses, const sherd_adjoint_options *opt,
+                  double *values, double *grads) {
+  if (!ctx || !opt) return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (n_edges == 0 || n_poses == 0) return SHERD_OK;
+  if (!edges || !poses || !inverses || !values || !grads)
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (!(opt->radius_k > 0.0) || !(opt->width_k > 0.0) || !(opt->window_k >= 0.0) ||
+      !std::isfinite(opt->radius_k) || !std::isfinite(opt->width_k) || !std::isfinite(opt->window_k))
+    return fail(ctx, SHERD_E_INVALID, "adjoint options must be finite and positive");
+  size_t n_pe = size_t(n_poses) * n_edges;
+  if (n_pe * 3 > size_t(1u << 31) - 1) return fail(ctx, SHERD_E_INVALID, "too many (pose, edge) units");
+  for (size_t i = 0; i < n_pe; ++i)
+    if (!finite_pose(poses + 16 * i) || !finite_pose(inverses + 16 * i))
+      return fail(ctx, SHERD_E_INVALID, "pose is not finite");
+  std::vector<PairView> views(n_edges);
+  for (uint32_t e = 0; e < n_edges; ++e) {
+    if (!edges[e] || edges[e]->ctx != ctx) return fail(ctx, SHERD_E_INVALID, "edge of another context");
+    views[e] = edges[e]->view;
+    if (!views[e].frac_tgt.nrm) return fail(ctx, SHERD_E_INVALID, "edge target without normals");
+  }
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<PairView> dv;
+  DBuf<double> dp, di, dval, dgrad;
+  if ((rc = upload(ctx, dv, views.data(), views.size())) ||
+      (rc = upload(ctx, dp, poses, 16 * n_pe)) || (rc = upload(ctx, di, inverses, 16 * n_pe)))
+    return rc;
+  CK(dval.alloc(n_pe * ADJ_VALUES));
+  CK(dgrad.alloc(n_pe * ADJ_VALUES * 6));
+  AdjointConsts kc{opt->radius_k, opt->width_k, opt->window_k};
+  k_adjoint<<<unsigned(n_pe * 3), ADJ_BLOCK, 0, ctx->stream>>>(dv.p, n_edges, dp.p, di.p, kc, dval.p,
+                                                              dgrad.p, ctx->d_status);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(values, dval.p, sizeof(double) * n_pe * ADJ_VALUES, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaMemcpyAsync(grads, dgrad.p, sizeof(double) * n_pe * ADJ_VALUES * 6,
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, "adjoint", n_pe, true);
 }
 
 }  // extern "C"

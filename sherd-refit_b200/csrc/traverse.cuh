@@ -195,31 +195,22 @@ __device__ __forceinline__ float box_dist2(const float *lo, const float *hi, con
   return s;
 }
 
-// RayScene::bounded_distance (spatial/bvh.rs:123-131): the distance to the
-// nearest face when it is <= window (inclusive), else +inf. window = +inf is
-// RayScene::distance (bvh.rs:110-113).
-__device__ __noinline__ float mesh_distance(const MeshView &m, F3 p, float window, uint32_t &status) {
-  float best = f_inf();
-  if (m.nf == 0 || !(window > 0.0f)) return best;
-  float pc[3] = {p.x, p.y, p.z};
+// The closest-face walk shared by mesh_distance and mesh_nearest_face: nodes
+// nearer than the current bound (padded, so that a tie is still visited) are
+// opened nearest child first, and `leaf(first, count)` scores each leaf range.
+// `bound()` is the current search radius (+inf before anything is found).
+template <class Leaf, class Bound>
+__device__ __forceinline__ void mesh_walk(const MeshView &m, const float *pc, Leaf &&leaf,
+                                          Bound &&bound, uint32_t &status) {
   auto bound2 = [&]() {
-    float b = fminf(best, window);
+    float b = bound();
     if (b == f_inf()) return f_inf();
     float s = b + 4e-6f * b + m.pad;
     return s * s;
   };
-  auto leaf = [&](int first, int count) {
-    for (int s = first; s < first + count; ++s) {
-      F3 a, b, c;
-      uint32_t id;
-      tri_at(m, s, a, b, c, id);
-      float dd = tri_distance(p, a, b, c);
-      if (dd <= window && dd < best) best = dd;
-    }
-  };
   if (m.root_leaf) {
-    leaf(0, m.root_leaf);
-    return best;
+    leaf(0, int(m.root_leaf));
+    return;
   }
   int stack_n[STACK];
   float stack_k[STACK];
@@ -263,6 +254,56 @@ __device__ __noinline__ float mesh_distance(const MeshView &m, F3 p, float windo
     }
     if (!more) break;
   }
+}
+
+// RayScene::bounded_distance (spatial/bvh.rs:123-131): the distance to the
+// nearest face when it is <= window (inclusive), else +inf. window = +inf is
+// RayScene::distance (bvh.rs:110-113).
+__device__ __noinline__ float mesh_distance(const MeshView &m, F3 p, float window, uint32_t &status) {
+  float best = f_inf();
+  if (m.nf == 0 || !(window > 0.0f)) return best;
+  float pc[3] = {p.x, p.y, p.z};
+  mesh_walk(
+      m, pc,
+      [&](int first, int count) {
+        for (int s = first; s < first + count; ++s) {
+          F3 a, b, c;
+          uint32_t id;
+          tri_at(m, s, a, b, c, id);
+          float dd = tri_distance(p, a, b, c);
+          if (dd <= window && dd < best) best = dd;
+        }
+      },
+      [&]() { return fminf(best, window); }, status);
+  return best;
+}
+
+// mesh_distance that also names the face: the sorted slot of the nearest face
+// within the window, an exact f32 tie going to the lowest original face id
+// (the rule first_hit uses); slot = MISS when nothing is within the window.
+__device__ __noinline__ float mesh_nearest_face(const MeshView &m, F3 p, float window, uint32_t &slot,
+                                                uint32_t &status) {
+  float best = f_inf();
+  uint32_t best_id = MISS;
+  slot = MISS;
+  if (m.nf == 0 || !(window > 0.0f)) return best;
+  float pc[3] = {p.x, p.y, p.z};
+  mesh_walk(
+      m, pc,
+      [&](int first, int count) {
+        for (int s = first; s < first + count; ++s) {
+          F3 a, b, c;
+          uint32_t id;
+          tri_at(m, s, a, b, c, id);
+          float dd = tri_distance(p, a, b, c);
+          if (dd <= window && (dd < best || (dd == best && id < best_id))) {
+            best = dd;
+            best_id = id;
+            slot = uint32_t(s);
+          }
+        }
+      },
+      [&]() { return fminf(best, window); }, status);
   return best;
 }
 

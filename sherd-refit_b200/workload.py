@@ -110,3 +110,43 @@ def algorithmic_bytes(wl, cands, n_src):
         for p in wl.pairs], np.float64)
     ver = float(np.sum(per_pair[pair]) * 24)
     return icp, ver
+
+
+def perturbed_group_poses(wl, n_poses, seed=0, rot_deg=0.5, trans_t=0.2):
+    """The assembled world poses of a workload's fragments (fragment frame -> world, the
+    inverse of each Fragment.pose) and n_poses seeded perturbations of all of them: each
+    fragment turned by rot_deg about a uniform axis through its fracture centroid and moved by
+    trans_t * t in a uniform direction. Returns (truth (G, 4, 4), poses (P, G, 4, 4))."""
+    rng = np.random.default_rng(seed)
+    truth = np.stack([np.linalg.inv(fr.pose) for fr in wl.fragments])
+    g = len(truth)
+    out = np.empty((n_poses, g, 4, 4))
+    for k, fr in enumerate(wl.fragments):
+        c = truth[k, :3, :3] @ fr.pf.mean(0) + truth[k, :3, 3]
+        axis = rng.normal(size=(n_poses, 3))
+        axis /= np.linalg.norm(axis, axis=1, keepdims=True)
+        ang = np.radians(rot_deg)
+        kx = np.zeros((n_poses, 3, 3))
+        kx[:, 0, 1], kx[:, 0, 2], kx[:, 1, 2] = -axis[:, 2], axis[:, 1], -axis[:, 0]
+        kx -= kx.transpose(0, 2, 1)
+        r = np.eye(3) + np.sin(ang) * kx + (1.0 - np.cos(ang)) * (kx @ kx)
+        step = rng.normal(size=(n_poses, 3))
+        step *= trans_t * fr.t / np.linalg.norm(step, axis=1, keepdims=True)
+        d = np.tile(np.eye(4), (n_poses, 1, 1))
+        d[:, :3, :3] = r
+        d[:, :3, 3] = c - (r @ c) + step
+        out[:, k] = d @ truth[k]
+    return truth, out
+
+
+def assembled_group(dev: DeviceCollection, wl, opts=None):
+    """The adjacent pairs of a device collection as the edges of one assembled group."""
+    from .adjoint import Group
+    keep = [k for k, p in enumerate(wl.pairs) if p.adjacent]
+    opts = opts or A.AdjointOptions(0.2, 0.01, 30.0)
+    return Group(ctx=dev.ctx, edges=[dev.pairs[k] for k in keep],
+                 a=np.array([wl.pairs[k].a for k in keep], np.int64),
+                 b=np.array([wl.pairs[k].b for k in keep], np.int64),
+                 n_fragments=len(wl.fragments),
+                 n_source=np.array([len(wl.fragments[wl.pairs[k].b].pf) for k in keep], np.int64),
+                 t=np.array([dev.scales[k].t for k in keep]), opts=opts)

@@ -26,26 +26,6 @@ SCORE_KEYS = ("tight_a", "tight_b", "tight", "gap_a", "gap_b", "gap", "contact_a
 
 
 @pytest.fixture(scope="module")
-def gpu_slab(sherd, gpu_ctx, slab):
-    """Device meshes, surfaces, clouds and the pair of the slab, built once."""
-    out = {}
-    for name in ("pieceA", "pieceB"):
-        p = piece(slab, name)
-        mesh = gpu_ctx.mesh(p["V"], p["F"])
-        frac = mesh.subset(p["frac"])
-        surf = gpu_ctx.surfaces(frac, mesh, int(p["watertight"]), float(p["frac_area"]), p["Pf"],
-                                p["S"], p["brk_P"], p["brk_ns"], p["margin_p"], p["margin_n"])
-        out[name] = dict(mesh=mesh, frac=frac, surf=surf, arrays=p)
-    a, b = out["pieceA"], out["pieceB"]
-    reg_t = gpu_ctx.cloud(a["arrays"]["reg_p"], a["arrays"]["reg_n"])
-    frac_t = gpu_ctx.cloud(a["arrays"]["frac_p"], a["arrays"]["frac_n"])
-    scales = sherd.Scales(*[float(x) for x in slab["scales"]])
-    pair = gpu_ctx.pair(a["surf"], b["surf"], reg_t, frac_t, b["arrays"]["reg_p"],
-                        b["arrays"]["frac_p"], scales)
-    return dict(a=a, b=b, reg_t=reg_t, frac_t=frac_t, scales=scales, pair=pair)
-
-
-@pytest.fixture(scope="module")
 def cpu_slab(oracle, slab):
     return oracle_pair(oracle, slab)
 
