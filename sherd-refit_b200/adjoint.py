@@ -68,6 +68,8 @@ class Group:
     n_source: np.ndarray  # (E,) B's fracture sample count (the plane term's points)
     t: np.ndarray         # (E,) the pair's t
     opts: A.AdjointOptions
+    centroid: np.ndarray | None = None  # (G, 3) each fragment's fracture centroid, own frame
+    rho: np.ndarray | None = None       # (G,) RMS radius of its fracture samples about it
 
     def relative(self, w: np.ndarray):
         """(P, G, 4, 4) world poses -> T = W_a^-1 W_b and T^-1, each (P, E, 4, 4)."""
@@ -131,41 +133,109 @@ def alignment_loss(values: torch.Tensor, group: Group, plane_weight=1.0, tight_w
     return (plane_weight * plane - tight_weight * 0.5 * (tight_a + tight_b)).sum(-1)
 
 
-def refine(group: Group, w0: np.ndarray, steps=50, fixed=0, lr_rot=1e-3, lr_trans=0.02,
-           plane_weight=1.0, tight_weight=0.1):
-    """Joint refinement of every group pose in w0 (P, G, 4, 4): W = exp(xi^) W0 with one twist
-    per fragment, fragment `fixed` held (the objective is invariant to a common motion), Adam
-    steps of lr_rot radians and lr_trans * t with a cosine decay. Returns the refined poses
-    and the mean loss before each step."""
-    w0t = torch.from_numpy(np.ascontiguousarray(w0, np.float64))
-    p, g = w0t.shape[:2]
+class _BudgetSpent(Exception):
+    pass
+
+
+def refine(group: Group, w0: np.ndarray, steps=50, fixed=0, stages=((0.2, 0.0), (0.08, 1.0)),
+           plane_weight=1.0):
+    """Joint refinement of every group pose in w0 (P, G, 4, 4), one twist per fragment with
+    fragment `fixed` held (the objective is invariant to a common motion).
+
+    Each fragment turns about its own fracture centroid c (world frame, at w0), so that its
+    rotation and translation do not mix through the distance to the world origin:
+    W = C exp(xi^) C^-1 W0. The twist is scaled so that a unit step moves the fragment's
+    samples by about t: xi = (u_w t / rho, u_v t), with rho the RMS radius of its fracture
+    samples about c.
+
+    `stages` are (correspondence radius_k, tight_weight) pairs. Each gets an equal share of
+    the `steps` objective evaluations (one sherd_adjoint call each) under L-BFGS with a
+    strong-Wolfe line search, and ends at the best poses it evaluated. The default first
+    closes the gap with the point-to-plane term at the first rung's radius. It then
+    tightens with the smoothed tight fraction, whose distances are to the true faces and
+    not to sampled planes. Returns the refined poses and the mean loss at each evaluation
+    (at most `steps`)."""
+    w0 = np.ascontiguousarray(w0, np.float64)
+    p, g = w0.shape[:2]
     t_scale = float(np.min(group.t))
-    rot = torch.zeros(p, g, 3, dtype=torch.float64, requires_grad=True)
-    trans = torch.zeros(p, g, 3, dtype=torch.float64, requires_grad=True)
-    opt = torch.optim.Adam([{"params": [rot], "lr": lr_rot},
-                            {"params": [trans], "lr": lr_trans * t_scale}])
-    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, steps)
+    local = np.zeros((g, 3)) if group.centroid is None else np.asarray(group.centroid)
+    rho = np.full(g, t_scale) if group.rho is None else np.asarray(group.rho)
+    scale = torch.from_numpy(np.concatenate([np.repeat((t_scale / rho)[:, None], 3, 1),
+                                             np.full((g, 3), t_scale)], 1))[None]
     keep = torch.ones(1, g, 1, dtype=torch.float64)
     keep[0, fixed] = 0.0
     history = []
-    for _ in range(steps):
-        opt.zero_grad()
-        w = exp_se3(torch.cat([rot * keep, trans * keep], -1)) @ w0t
-        loss = alignment_loss(GroupObjectives.apply(w, group), group, plane_weight, tight_weight)
-        loss.sum().backward()
-        history.append(float(loss.mean()))
-        opt.step()
-        sched.step()
-    with torch.no_grad():
-        w = exp_se3(torch.cat([rot * keep, trans * keep], -1)) @ w0t
-    return w.numpy(), history
+    radius0 = group.opts.radius_k
+    per_stage = [steps // len(stages) + (1 if k < steps % len(stages) else 0)
+                 for k in range(len(stages))]
+    try:
+        w = w0
+        for (radius_k, tight_weight), n_eval in zip(stages, per_stage):
+            group.opts = A.AdjointOptions(radius_k, group.opts.width_k, group.opts.window_k)
+            c = np.einsum("pgij,gj->pgi", w[..., :3, :3], local) + w[..., :3, 3]
+            to_c = torch.from_numpy(np.tile(np.eye(4), (p, g, 1, 1)))
+            to_c[..., :3, 3] = torch.from_numpy(c)
+            from_c = torch.linalg.inv(to_c)
+            base = torch.from_numpy(w)
+            u = torch.zeros(p, g, 6, dtype=torch.float64, requires_grad=True)
+
+            def poses():
+                return to_c @ exp_se3(u * scale * keep) @ from_c @ base
+
+            opt = torch.optim.LBFGS([u], lr=1.0, max_iter=n_eval, max_eval=n_eval,
+                                    history_size=20, line_search_fn="strong_wolfe",
+                                    tolerance_grad=1e-12, tolerance_change=1e-15)
+            best = [float("inf"), None]
+            used = [0]
+
+            def closure():
+                if used[0] == n_eval:  # the line search may ask for more than the budget
+                    raise _BudgetSpent
+                used[0] += 1
+                opt.zero_grad()
+                loss = alignment_loss(GroupObjectives.apply(poses(), group), group,
+                                      plane_weight, tight_weight).sum()
+                loss.backward()
+                value = float(loss.detach())
+                history.append(value / p)
+                if value < best[0]:
+                    best[0], best[1] = value, u.detach().clone()
+                return loss
+
+            try:
+                opt.step(closure)
+            except _BudgetSpent:
+                pass
+            with torch.no_grad():
+                u.copy_(best[1])
+                w = poses().numpy()
+    finally:
+        group.opts = A.AdjointOptions(radius0, group.opts.width_k, group.opts.window_k)
+    return w, history
 
 
-def pose_errors(w: np.ndarray, truth: np.ndarray, fixed=0):
-    """Per group pose and fragment, the error of the pose relative to fragment `fixed` against
-    the truth: (rotation in degrees, translation) arrays of shape (P, G)."""
+def edge_errors(w: np.ndarray, group: Group, truth: np.ndarray):
+    """Per group pose and edge, the error of the relative pose T = W_a^-1 W_b against the
+    truth's: (rotation in degrees, displacement of B's fracture centroid), each (P, E)."""
+    te = np.linalg.inv(w[:, group.a]) @ w[:, group.b]
+    tt = np.linalg.inv(truth[group.a]) @ truth[group.b]
+    d = np.linalg.inv(tt)[None] @ te
+    cos = np.clip((np.trace(d[..., :3, :3], axis1=-2, axis2=-1) - 1.0) / 2.0, -1.0, 1.0)
+    cb = np.asarray(group.centroid)[group.b]
+    moved = np.einsum("peij,ej->pei", te[..., :3, :3], cb) + te[..., :3, 3]
+    true = np.einsum("eij,ej->ei", tt[..., :3, :3], cb) + tt[..., :3, 3]
+    return np.degrees(np.arccos(cos)), np.linalg.norm(moved - true[None], axis=-1)
+
+
+def pose_errors(w: np.ndarray, truth: np.ndarray, centroid: np.ndarray, fixed=0):
+    """Per group pose and fragment, the error of its pose relative to fragment `fixed` against
+    the truth: (rotation in degrees, displacement of its fracture centroid `centroid` (G, 3,
+    own frame) in length units), each of shape (P, G)."""
     rel = np.linalg.inv(w[:, fixed:fixed + 1]) @ w
     rel_true = np.linalg.inv(truth[fixed]) @ truth
     d = np.linalg.inv(rel_true)[None] @ rel
     cos = np.clip((np.trace(d[..., :3, :3], axis1=-2, axis2=-1) - 1.0) / 2.0, -1.0, 1.0)
-    return np.degrees(np.arccos(cos)), np.linalg.norm(d[..., :3, 3], axis=-1)
+    c = np.asarray(centroid)
+    moved = np.einsum("pgij,gj->pgi", rel[..., :3, :3], c) + rel[..., :3, 3]
+    true = np.einsum("gij,gj->gi", rel_true[..., :3, :3], c) + rel_true[..., :3, 3]
+    return np.degrees(np.arccos(cos)), np.linalg.norm(moved - true[None], axis=-1)

@@ -149,4 +149,7 @@ def assembled_group(dev: DeviceCollection, wl, opts=None):
                  b=np.array([wl.pairs[k].b for k in keep], np.int64),
                  n_fragments=len(wl.fragments),
                  n_source=np.array([len(wl.fragments[wl.pairs[k].b].pf) for k in keep], np.int64),
-                 t=np.array([dev.scales[k].t for k in keep]), opts=opts)
+                 t=np.array([dev.scales[k].t for k in keep]), opts=opts,
+                 centroid=np.stack([fr.pf.mean(0) for fr in wl.fragments]),
+                 rho=np.array([np.sqrt(((fr.pf - fr.pf.mean(0)) ** 2).sum(1).mean())
+                               for fr in wl.fragments]))
