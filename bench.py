@@ -12,7 +12,9 @@ HBM, CUDA events around the batch's graph on the library's stream, max over rank
 copied in and the candidates copied out every step), the roofline of the dominant kernel,
 the clocks seen during the timed region and the oracle's CPU baseline on a bounded sample.
 `--impl reference` times the reference algorithm's CPU restatement (the oracle; the Rust
-reference cannot be built here) on all host cores instead.
+reference cannot be built here) on all host cores instead. `--config group` measures the
+differentiation workload instead (sherd_adjoint over 4096 perturbed poses of an assembled
+8-fragment pot, and a 50-evaluation joint refinement).
 """
 
 from __future__ import annotations
@@ -189,6 +191,69 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_group(args):
+    """The differentiation workload: the 8-fragment pot assembled (its 18 adjacent pairs as
+    edges), every fragment pose perturbed by 0.5 deg and 0.2 t, 4096 group poses. One step is
+    one sherd_adjoint evaluation of all of them (values and twist gradients of every edge);
+    the line also reports a 50-evaluation joint refinement of the same 4096 poses."""
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    sherd = _pkg()
+    synth = _pkg("synth")
+    workload = _pkg("workload")
+    adj = _pkg("adjoint")
+    wl = synth.make("pot", args.seed)
+    ctx = sherd.Context(local)
+    dev = workload.to_device(ctx, wl)
+    group = workload.assembled_group(dev, wl)
+    truth, w0 = workload.perturbed_group_poses(wl, args.group_poses, seed=args.seed + 1)
+    for _ in range(args.warmup):
+        group.evaluate(w0)
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        values, _ = group.evaluate(w0)
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    step = float(np.mean(times))
+    queries = args.group_poses * int(sum(
+        len(wl.fragments[b].pf) * 2 + len(wl.fragments[a].pf) for a, b in zip(group.a, group.b)))
+    t0 = time.perf_counter()
+    w, history = adj.refine(group, w0, steps=50)
+    t_refine = time.perf_counter() - t0
+    rot0, disp0 = adj.edge_errors(w0, group, truth)
+    rot1, disp1 = adj.edge_errors(w, group, truth)
+    v1, _ = group.evaluate(w)
+    t = float(np.min(group.t))
+    line = {
+        "metric": "group-pose adjoint evaluations/s", "value": args.group_poses / step,
+        "unit": "group poses/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"pot group: {len(wl.fragments)} fragments, {len(group.a)} "
+                               f"edges, {args.group_poses} perturbed group poses "
+                               "(0.5 deg, 0.2 t per fragment)",
+                   "queries_per_step": queries,
+                   "timer": "host wall clock around the synchronous C-ABI call (poses in, "
+                            "values and gradients out)"},
+        "queries_per_s": queries / step,
+        "refinement": {"evaluations": len(history), "seconds": t_refine,
+                       "edge_rot_deg": [float(rot0.mean()), float(rot1.mean())],
+                       "edge_disp_t": [float(disp0.mean()) / t, float(disp1.mean()) / t],
+                       "tight": [float((values[..., 1] / values[..., 2]).mean()),
+                                 float((v1[..., 1] / v1[..., 2]).mean())]},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def _config_dict(wl, args, extra=None):
     d = wl.describe()
     cfg = {"workload": f"{args.config}: {d['fragments']} fragments, {d['pairs']} pairs x "
@@ -212,9 +277,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--reference-items", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--group-poses", type=int, default=4096)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.config == "group":
+        run_group(args)
         return
 
     import torch

@@ -360,6 +360,55 @@ int sherd_batch_run(sherd_batch *batch, float ms[SHERD_BATCH_TIMES]);
 int sherd_batch_results(sherd_batch *batch, sherd_candidate *out);
 int sherd_batch_free(sherd_batch *batch);
 
+/* ---- segmentation: R 3.4 end to end (fragment/segment.rs:511-631) ------- */
+
+/* SegParams (segment.rs:86-118); sherd_seg_params_default gives the shipped values. */
+typedef struct sherd_seg_params {
+    double smooth_res;             /* smoothing radius max(t/3, smooth_res * res)       */
+    double coarse_at;              /* coarse mesh: res > coarse_at * t                   */
+    double boundary_angle;         /* shell growth limit, degrees                        */
+    uint32_t votes;                /* cone rays of seven that must reach the far wall   */
+    uint32_t votes_coarse;         /* ... on a coarse mesh                               */
+    uint32_t smoothed_hit_normal;  /* judge the hit face by its smoothed normal          */
+    uint32_t boundary_angle_auto;  /* max(angle, median shell normal noise + 15 deg)     */
+} sherd_seg_params;
+
+/* What Segmentation reports besides the labels (segment.rs:121-141); the
+ * area fractions are the caller's, a pairwise sum of the areas under the
+ * labels (segment.rs:645-648). */
+typedef struct sherd_seg_info {
+    uint32_t votes;         /* the vote count this mesh's resolution asked for */
+    uint32_t n_rep;         /* voxel representatives                           */
+    double smooth_radius;   /* max(t/3, smooth_res * res)                      */
+    double boundary_angle;  /* the growth angle used, degrees                  */
+} sherd_seg_info;
+
+/* SegTrace (segment.rs:143-166): every intermediate array, each nullable.
+ * rep holds n_rep entries (at most nf), ns 3 doubles per face, the rest one
+ * entry per face. */
+typedef struct sherd_seg_trace {
+    uint32_t *rep, *near;
+    double *ns;
+    uint8_t *good, *frac_raw, *frac_majority, *frac_islands, *has_ref;
+} sherd_seg_trace;
+
+void sherd_seg_params_default(sherd_seg_params *out);
+
+/* segment::segment_faces (segment.rs:476-631): shell/fracture labels
+ * (1 = fracture) of the working mesh `v` (f64, nv) / `f` (nf), whose ray
+ * scene `mesh` was uploaded from the same faces; `thick` is R 3.2's wall and
+ * `res` the median edge. Every step runs on the device: voxel representatives
+ * (lowest face per t/8 voxel, ascending), each face's nearest representative,
+ * the smoothed normals, the seven-ray cone vote, the majority filter, the
+ * island removals over the face adjacency, the shell reference normals and the
+ * boundary growth. Radius balls are inclusive and summed in ascending face
+ * order, component areas in face order, as the reference does, so the labels
+ * are bit-exact to a sequential restatement. */
+int sherd_segment(sherd_ctx *ctx, const sherd_mesh *mesh, const double *v, uint32_t nv,
+                  const uint32_t *f, uint32_t nf, double thick, double res,
+                  const sherd_seg_params *sp, uint8_t *labels, sherd_seg_info *info,
+                  const sherd_seg_trace *trace);
+
 /* ---- differentiation: the adjoint of two group-alignment objectives ----- */
 
 /* Options of sherd_adjoint. No counterpart in the reference: the objectives

@@ -73,6 +73,24 @@ class AdjointOptions(C.Structure):
     _fields_ = [("radius_k", C.c_double), ("width_k", C.c_double), ("window_k", C.c_double)]
 
 
+class SegParams(C.Structure):
+    _fields_ = [("smooth_res", C.c_double), ("coarse_at", C.c_double),
+                ("boundary_angle", C.c_double), ("votes", C.c_uint32),
+                ("votes_coarse", C.c_uint32), ("smoothed_hit_normal", C.c_uint32),
+                ("boundary_angle_auto", C.c_uint32)]
+
+
+class SegInfo(C.Structure):
+    _fields_ = [("votes", C.c_uint32), ("n_rep", C.c_uint32), ("smooth_radius", C.c_double),
+                ("boundary_angle", C.c_double)]
+
+
+class SegTrace(C.Structure):
+    _fields_ = [("rep", C.c_void_p), ("near", C.c_void_p), ("ns", C.c_void_p),
+                ("good", C.c_void_p), ("frac_raw", C.c_void_p), ("frac_majority", C.c_void_p),
+                ("frac_islands", C.c_void_p), ("has_ref", C.c_void_p)]
+
+
 class InsideOutcome(C.Structure):
     _fields_ = [("depth", C.c_float), ("inside", C.c_uint32)]
 
@@ -130,6 +148,9 @@ def lib() -> C.CDLL:
         "or_adjoint": (None, [vp, F64P, F64P, C.POINTER(AdjointOptions), C.c_int, I32P, F64P,
                               F64P]),
         "or_normal_equations": (None, [F64P, C.c_uint32, vp, F64P, C.c_double, F64P, F64P]),
+        "or_segment": (None, [vp, F64P, U32P, C.c_uint32, C.c_double, C.c_double,
+                              C.POINTER(SegParams), vp, U8P, C.POINTER(SegInfo),
+                              C.POINTER(SegTrace)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -306,6 +327,38 @@ def adjoint(pair: Pair, t, t_inv, opts: AdjointOptions, assign=None):
     lib().or_adjoint(pair.h, f64(t).reshape(16), f64(t_inv).reshape(16), C.byref(opts),
                      int(frozen), assign, values, grads)
     return values, grads, assign
+
+
+def seg_params(**kw) -> SegParams:
+    """SegParams::default (segment.rs:107-118), with keyword overrides."""
+    p = SegParams(smooth_res=0.0, coarse_at=0.1, boundary_angle=25.0, votes=5, votes_coarse=4,
+                  smoothed_hit_normal=0, boundary_angle_auto=0)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def segment(mesh: Mesh, v, f, thick, res, params: SegParams | None = None, good=None):
+    """segment::segment_faces (segment.rs:476-631) on the working mesh (v f64, f) whose ray
+    scene is `mesh`. `good` (optional votes per face) replaces the cone vote. Returns
+    (labels (nf,) u8, SegInfo, trace dict of every intermediate array)."""
+    v = f64(v).reshape(-1, 3)
+    f = u32(f).reshape(-1, 3)
+    nf = len(f)
+    params = params or seg_params()
+    tr = {"rep": np.zeros(nf, np.uint32), "near": np.zeros(nf, np.uint32),
+          "ns": np.zeros((nf, 3)), "good": np.zeros(nf, np.uint8),
+          "frac_raw": np.zeros(nf, np.uint8), "frac_majority": np.zeros(nf, np.uint8),
+          "frac_islands": np.zeros(nf, np.uint8), "has_ref": np.zeros(nf, np.uint8)}
+    trace = SegTrace(*[a.ctypes.data for a in tr.values()])
+    labels = np.zeros(nf, np.uint8)
+    info = SegInfo()
+    g = None if good is None else np.ascontiguousarray(good, np.uint8)
+    lib().or_segment(mesh.h, v, f, nf, float(thick), float(res), C.byref(params),
+                     None if g is None else g.ctypes.data, labels, C.byref(info),
+                     C.byref(trace))
+    tr["rep"] = tr["rep"][:info.n_rep]
+    return labels, info, tr
 
 
 def normal_equations(source, target: Cloud, pose, distance):

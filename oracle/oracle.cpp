@@ -31,6 +31,7 @@
 #include <cstdint>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -1325,6 +1326,313 @@ int default_threads() {
 // ===========================================================================
 // C ABI (loaded by the tests through ctypes)
 // ===========================================================================
+// ---------------------------------------------------------------------------
+// Segmentation, R 3.4 (fragment/segment.rs:189-631, mesh/adjacency.rs:43-175,
+// mesh/components.rs:120-191)
+// ---------------------------------------------------------------------------
+
+// Points bucketed in cubes of side `cell`: every point within r <= cell of a
+// query lies in the 27 cubes around the query's own.
+struct BallGrid {
+  const double *p = nullptr;
+  size_t n = 0;
+  double cell = 1.0, lo[3] = {0, 0, 0};
+  std::map<std::array<int64_t, 3>, std::vector<uint32_t>> cells;
+
+  BallGrid(const double *pts, size_t count, double side) : p(pts), n(count), cell(side) {
+    for (int k = 0; k < 3; ++k) lo[k] = D_INF;
+    for (size_t i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], p[3 * i + k]);
+    for (size_t i = 0; i < n; ++i) cells[key(p + 3 * i)].push_back(uint32_t(i));
+  }
+  std::array<int64_t, 3> key(const double *q) const {
+    return {int64_t(std::floor((q[0] - lo[0]) / cell)), int64_t(std::floor((q[1] - lo[1]) / cell)),
+            int64_t(std::floor((q[2] - lo[2]) / cell))};
+  }
+  // PointTree::within (kdtree.rs:219-245): every point with d2 <= r2, d2 =
+  // ((dx dx + dy dy) + dz dz), ascending by index.
+  void within(const double *q, double r, std::vector<uint32_t> &out) const {
+    out.clear();
+    if (r < 0.0 || n == 0) return;
+    double r2 = r * r;
+    std::array<int64_t, 3> c = key(q);
+    for (int64_t dx = -1; dx <= 1; ++dx)
+      for (int64_t dy = -1; dy <= 1; ++dy)
+        for (int64_t dz = -1; dz <= 1; ++dz) {
+          auto it = cells.find({c[0] + dx, c[1] + dy, c[2] + dz});
+          if (it == cells.end()) continue;
+          for (uint32_t j : it->second) {
+            const double *x = p + 3 * size_t(j);
+            double ex = q[0] - x[0], ey = q[1] - x[1], ez = q[2] - x[2];
+            if ((ex * ex + ey * ey) + ez * ez <= r2) out.push_back(j);
+          }
+        }
+    std::sort(out.begin(), out.end());
+  }
+};
+
+// voxel_representatives (segment.rs:217-259): the lowest index of every
+// occupied voxel floor((c - (min - 1)) / spacing), ascending.
+std::vector<uint32_t> voxel_representatives(const double *c, size_t n, double spacing) {
+  std::vector<uint32_t> rep;
+  if (n == 0 || !std::isfinite(spacing) || spacing <= 0.0) return rep;
+  double mb[3] = {D_INF, D_INF, D_INF};
+  for (size_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) mb[k] = std::min(mb[k], c[3 * i + k]);
+  for (double &m : mb) m -= 1.0;
+  std::vector<std::pair<std::array<int64_t, 3>, uint32_t>> cells(n);
+  for (size_t i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k)
+      cells[i].first[k] = int64_t(std::floor((c[3 * i + k] - mb[k]) / spacing));
+    cells[i].second = uint32_t(i);
+  }
+  std::sort(cells.begin(), cells.end());
+  for (size_t i = 0; i < n; ++i)
+    if (i == 0 || cells[i - 1].first != cells[i].first) rep.push_back(cells[i].second);
+  std::sort(rep.begin(), rep.end());
+  return rep;
+}
+
+// ball_normals (segment.rs:267-296) over the points `idx` of a BallGrid:
+// m = sum A FN / max(sum A, 1e-12), then m / max(|m|, 1e-12), summed in
+// ascending index order; `has` is false for an empty ball.
+void ball_normals(const BallGrid &grid, const std::vector<std::array<double, 3>> &queries,
+                  const double *normals, const double *areas, double radius,
+                  std::vector<std::array<double, 3>> &out, std::vector<uint8_t> &has) {
+  out.assign(queries.size(), {0.0, 0.0, 0.0});
+  has.assign(queries.size(), 0);
+  parallel_for(uint32_t(queries.size()), default_threads(), [&](uint32_t r) {
+    std::vector<uint32_t> ball;
+    grid.within(queries[r].data(), radius, ball);
+    double m[3] = {0.0, 0.0, 0.0}, wsum = 0.0;
+    for (uint32_t j : ball) {
+      const double *n = normals + 3 * size_t(j);
+      double a = areas[j];
+      for (int k = 0; k < 3; ++k) m[k] += n[k] * a;
+      wsum += a;
+    }
+    double den = std::max(wsum, 1e-12);
+    for (double &x : m) x /= den;
+    double norm = std::max(std::sqrt((m[0] * m[0] + m[1] * m[1]) + m[2] * m[2]), 1e-12);
+    out[r] = {m[0] / norm, m[1] / norm, m[2] / norm};
+    has[r] = !ball.empty();
+  });
+}
+
+// face_adjacency (adjacency.rs:138-160): edge keys in slot-major order,
+// sorted stably, every two consecutive equal keys one face pair.
+void face_adjacency(const uint32_t *f, uint32_t nf, std::vector<uint32_t> &fa,
+                    std::vector<uint32_t> &fb) {
+  size_t m = size_t(3) * nf;
+  std::vector<uint64_t> keys(m);
+  const int slot[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+  for (int s = 0; s < 3; ++s)
+    for (uint32_t t = 0; t < nf; ++t) {
+      uint32_t a = f[3 * t + slot[s][0]], b = f[3 * t + slot[s][1]];
+      uint32_t lo = std::min(a, b), hi = std::max(a, b);
+      keys[size_t(s) * nf + t] = (uint64_t(lo) << 32) | hi;
+    }
+  std::vector<uint32_t> order(m);
+  for (size_t i = 0; i < m; ++i) order[i] = uint32_t(i);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t x, uint32_t y) { return keys[x] < keys[y]; });
+  fa.clear();
+  fb.clear();
+  for (size_t w = 0; w + 1 < m; ++w) {
+    uint32_t i = order[w], j = order[w + 1];
+    if (keys[i] == keys[j]) {
+      fa.push_back(i % nf);
+      fb.push_back(j % nf);
+    }
+  }
+}
+
+// drop_small_components (components.rs:170-191) over mask_components
+// (components.rs:120-159): components of mask == target over the pairs whose
+// both faces are in the set, areas summed in face order, those below
+// min_area flipped.
+void drop_small_components(std::vector<uint8_t> &mask, bool target, double min_area,
+                           const std::vector<uint32_t> &fa, const std::vector<uint32_t> &fb,
+                           const double *areas) {
+  size_t n = mask.size();
+  std::vector<uint32_t> parent(n);
+  for (size_t i = 0; i < n; ++i) parent[i] = uint32_t(i);
+  auto find = [&](uint32_t x) {
+    while (parent[x] != x) {
+      parent[x] = parent[parent[x]];
+      x = parent[x];
+    }
+    return x;
+  };
+  for (size_t i = 0; i < fa.size(); ++i) {
+    uint32_t a = fa[i], b = fb[i];
+    if (bool(mask[a]) == target && bool(mask[b]) == target) {
+      uint32_t ra = find(a), rb = find(b);
+      if (ra != rb) parent[std::max(ra, rb)] = std::min(ra, rb);
+    }
+  }
+  std::vector<double> size(n, 0.0);
+  for (size_t i = 0; i < n; ++i)
+    if (bool(mask[i]) == target) size[find(uint32_t(i))] += areas[i];
+  for (size_t i = 0; i < n; ++i)
+    if (bool(mask[i]) == target && size[find(uint32_t(i))] < min_area) mask[i] = !target;
+}
+
+// refine_boundary (segment.rs:438-474): at most 60 passes; each flips, all
+// at once, the fracture faces touching the shell whose normal is within the
+// angle of their fixed shell reference normal.
+void refine_boundary(std::vector<uint8_t> &frac, const std::vector<uint32_t> &fa,
+                     const std::vector<uint32_t> &fb, const double *normals,
+                     const std::vector<std::array<double, 3>> &ref,
+                     const std::vector<uint8_t> &has_ref, double angle_deg) {
+  double cos_grow = std::cos(angle_deg * (3.14159265358979323846 / 180.0));
+  std::vector<uint8_t> cand(frac.size(), 0);
+  for (int pass = 0; pass < 60; ++pass) {
+    std::vector<uint32_t> list;
+    for (size_t i = 0; i < fa.size(); ++i) {
+      uint32_t a = fa[i], b = fb[i];
+      if (frac[a] != frac[b]) {
+        uint32_t face = frac[a] ? a : b;
+        if (!cand[face]) {
+          cand[face] = 1;
+          list.push_back(face);
+        }
+      }
+    }
+    if (list.empty()) break;
+    bool flipped = false;
+    for (uint32_t face : list) {
+      cand[face] = 0;
+      const double *n = normals + 3 * size_t(face);
+      const double *r = ref[face].data();
+      if (has_ref[face] && (n[0] * r[0] + n[1] * r[1]) + n[2] * r[2] > cos_grow) {
+        frac[face] = 0;
+        flipped = true;
+      }
+    }
+    if (!flipped) break;
+  }
+}
+
+// segment::run (segment.rs:511-631).
+void segment(const Mesh &scene, const double *v, const uint32_t *f, uint32_t nf, double thick,
+             double res, const sherd_seg_params &sp, const uint8_t *good_in, uint8_t *labels,
+             sherd_seg_info *info, const sherd_seg_trace *trace) {
+  info->votes = res > sp.coarse_at * thick ? sp.votes_coarse : sp.votes;
+  info->smooth_radius = std::max(thick / 3.0, sp.smooth_res * res);
+  info->boundary_angle = sp.boundary_angle;
+  info->n_rep = 0;
+  if (nf == 0 || !std::isfinite(thick) || thick <= 0.0) {
+    std::fill(labels, labels + nf, 0);
+    return;
+  }
+  std::vector<double> normals(size_t(3) * nf), areas(nf), cent(size_t(3) * nf);
+  face_geometry(v, f, nf, normals.data(), areas.data(), cent.data());
+  // 3.4.1 the grid
+  std::vector<uint32_t> rep = voxel_representatives(cent.data(), nf, thick * (1.0 / 8.0));
+  info->n_rep = uint32_t(rep.size());
+  std::vector<double> rep_xyz(3 * rep.size());
+  std::vector<std::array<double, 3>> rep_pts(rep.size());
+  for (size_t r = 0; r < rep.size(); ++r)
+    for (int k = 0; k < 3; ++k) rep_pts[r][k] = rep_xyz[3 * r + k] = cent[3 * size_t(rep[r]) + k];
+  Cloud rep_cloud;
+  rep_cloud.p = rep_xyz;
+  rep_cloud.build();
+  std::vector<uint32_t> near(nf);
+  parallel_for(nf, default_threads(), [&](uint32_t i) {
+    uint32_t j;
+    double d2;
+    rep_cloud.nearest_within_sq(&cent[3 * size_t(i)], D_INF, &j, &d2);
+    near[i] = j;
+  });
+  BallGrid all(cent.data(), nf, std::max(info->smooth_radius, thick * 0.5));
+  // 3.4.2 the smoothed normals
+  std::vector<std::array<double, 3>> ns_g, ref_g;
+  std::vector<uint8_t> has_g;
+  ball_normals(all, rep_pts, normals.data(), areas.data(), info->smooth_radius, ns_g, has_g);
+  std::vector<double> ns(size_t(3) * nf);
+  for (uint32_t i = 0; i < nf; ++i)
+    for (int k = 0; k < 3; ++k) ns[3 * size_t(i) + k] = ns_g[near[i]][k];
+  // 3.4.3 the cone vote
+  std::vector<uint8_t> good(nf);
+  if (good_in) {
+    std::copy(good_in, good_in + nf, good.begin());
+  } else {
+    const double *hit = sp.smoothed_hit_normal ? ns.data() : normals.data();
+    parallel_for(nf, default_threads(), [&](uint32_t i) {
+      good[i] = cone_vote(scene, &cent[3 * size_t(i)], &normals[3 * size_t(i)], &ns[3 * size_t(i)],
+                          hit, nf, thick);
+    });
+  }
+  std::vector<uint8_t> frac(nf);
+  for (uint32_t i = 0; i < nf; ++i) frac[i] = uint32_t(good[i]) < info->votes;
+  if (trace) {
+    if (trace->rep) std::copy(rep.begin(), rep.end(), trace->rep);
+    if (trace->near) std::copy(near.begin(), near.end(), trace->near);
+    if (trace->ns) std::copy(ns.begin(), ns.end(), trace->ns);
+    if (trace->good) std::copy(good.begin(), good.end(), trace->good);
+    if (trace->frac_raw) std::copy(frac.begin(), frac.end(), trace->frac_raw);
+  }
+  // 3.4.4 the majority filter
+  std::vector<uint8_t> per_rep(rep.size());
+  parallel_for(uint32_t(rep.size()), default_threads(), [&](uint32_t r) {
+    std::vector<uint32_t> ball;
+    all.within(rep_pts[r].data(), thick * 0.25, ball);
+    double wet = 0.0, total = 0.0;
+    for (uint32_t j : ball) {
+      total += areas[j];
+      if (frac[j]) wet += areas[j];
+    }
+    per_rep[r] = wet > 0.5 * total;
+  });
+  for (uint32_t i = 0; i < nf; ++i) frac[i] = per_rep[near[i]];
+  if (trace && trace->frac_majority) std::copy(frac.begin(), frac.end(), trace->frac_majority);
+  // 3.4.5-3.4.6 islands
+  std::vector<uint32_t> fa, fb;
+  face_adjacency(f, nf, fa, fb);
+  drop_small_components(frac, true, 0.5 * thick * thick, fa, fb, areas.data());
+  drop_small_components(frac, false, 2.0 * thick * thick, fa, fb, areas.data());
+  if (trace && trace->frac_islands) std::copy(frac.begin(), frac.end(), trace->frac_islands);
+  // 3.4.7 the boundary growth
+  std::vector<uint32_t> shell;
+  for (uint32_t i = 0; i < nf; ++i)
+    if (!frac[i]) shell.push_back(i);
+  double angle = sp.boundary_angle;
+  if (sp.boundary_angle_auto && !shell.empty()) {
+    std::vector<double> noise;
+    for (uint32_t i : shell) {
+      const double *a = &normals[3 * size_t(i)], *b = &ns[3 * size_t(i)];
+      double c = std::min(1.0, std::max(-1.0, (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]));
+      noise.push_back(std::acos(c) * (180.0 / 3.14159265358979323846));
+    }
+    angle = std::max(angle, median(noise) + 15.0);
+  }
+  info->boundary_angle = angle;
+  std::vector<std::array<double, 3>> reference(nf, {0.0, 0.0, 0.0});
+  std::vector<uint8_t> has_ref(nf, 0);
+  if (!shell.empty()) {
+    std::vector<double> sp_xyz(3 * shell.size()), sn(3 * shell.size()), sa(shell.size());
+    for (size_t k = 0; k < shell.size(); ++k) {
+      for (int q = 0; q < 3; ++q) {
+        sp_xyz[3 * k + q] = cent[3 * size_t(shell[k]) + q];
+        sn[3 * k + q] = normals[3 * size_t(shell[k]) + q];
+      }
+      sa[k] = areas[shell[k]];
+    }
+    BallGrid shell_grid(sp_xyz.data(), shell.size(), thick * 0.5);
+    ball_normals(shell_grid, rep_pts, sn.data(), sa.data(), thick * 0.5, ref_g, has_g);
+    for (uint32_t i = 0; i < nf; ++i) {
+      reference[i] = ref_g[near[i]];
+      has_ref[i] = has_g[near[i]];
+    }
+  }
+  if (trace && trace->has_ref) std::copy(has_ref.begin(), has_ref.end(), trace->has_ref);
+  refine_boundary(frac, fa, fb, normals.data(), reference, has_ref, angle);
+  // 3.4.8 one more island pass
+  drop_small_components(frac, true, 0.5 * thick * thick, fa, fb, areas.data());
+  std::copy(frac.begin(), frac.end(), labels);
+}
+
 extern "C" {
 
 void *or_mesh_new(const float *v, uint32_t nv, const uint32_t *f, uint32_t nf) {
@@ -1640,6 +1948,15 @@ void or_normal_equations(const double *src, uint32_t ns, const void *target, con
     jtr6[k] = jtr[k];
     for (int l = 0; l <= k; ++l) jtj36[6 * k + l] = jtj36[6 * l + k] = jtj[k][l];
   }
+}
+
+// segment::segment_faces (segment.rs:476-631); `good_in` (nullable) replaces
+// the cone vote, to run the later steps on given votes.
+void or_segment(const void *mesh, const double *v, const uint32_t *f, uint32_t nf, double thick,
+                double res, const sherd_seg_params *sp, const uint8_t *good_in, uint8_t *labels,
+                sherd_seg_info *info, const sherd_seg_trace *trace) {
+  segment(*static_cast<const Mesh *>(mesh), v, f, nf, thick, res, *sp, good_in, labels, info,
+          trace);
 }
 
 }  // extern "C"

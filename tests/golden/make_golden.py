@@ -9,8 +9,11 @@ without the reference tree present:
 * thickness (`fragment/thickness.rs:139-162`): the original component `load.V0`/`F0`, the
   face ids of the rays `thick.idx`, the Embree hits `thick.t_hit`/`thick.prim`, and the two
   answers `thick.t` / `thick.thick_mode` (bit-exact targets);
-* segmentation (`fragment/segment.rs:318-376`): the working mesh `mesh.V`/`mesh.F`, the
-  smoothed normals `seg.NS`, the cone votes `seg.good` and the final mask `seg.frac_final`;
+* segmentation (`fragment/segment.rs:189-631`): the working mesh `mesh.V`/`mesh.F` and its
+  `mesh.res`, the voxel representatives `seg.rep` and each face's `seg.near`, the smoothed
+  normals `seg.NS`, the cone votes `seg.good`, every intermediate mask (`seg.frac_raw`,
+  `seg.frac_majority`, `seg.frac_islands`), `seg.has_ref`, the final mask `seg.frac_final` and
+  `seg.info` (votes, smoothing radius, growth angle, raw fraction);
 * stage 2 and verification (`sherd-parity/src/stages/{stage2,verify}.rs`): the sample arrays
   at the pair's own `t` (`md.Pf`, `md.fp`, `md.S`, `md.sp`, `md.margin_idx`, `md.brk_P`,
   `md.brk_ns`), the pair's `scales.json`, the starts `s1.T[nms2.kept]`, the four rung poses
@@ -109,6 +112,14 @@ def main(reference: Path) -> None:
         out[p + "seg_good"] = np.load(fd / "seg.good.npy").astype(np.uint8)
         frac = np.load(fd / "seg.frac_final.npy").astype(bool)
         out[p + "frac"] = frac.astype(np.uint8)
+        for k in ("frac_raw", "frac_majority", "frac_islands", "has_ref"):
+            out[p + "seg_" + k] = np.load(fd / f"seg.{k}.npy").astype(np.uint8)
+        out[p + "seg_rep"] = np.load(fd / "seg.rep.npy").astype(np.uint32)
+        out[p + "seg_near"] = np.load(fd / "seg.near.npy").astype(np.uint32)
+        info = json.loads((fd / "seg.info.json").read_text())
+        out[p + "seg_info"] = np.array([info["votes"], info["smooth_radius"],
+                                        info["boundary_angle"], info["raw_fraction"]])
+        out[p + "res"] = np.float64(json.loads((fd / "mesh.res.json").read_text()))
         wt = json.loads((fd / "mesh.watertight.json").read_text())
         out[p + "watertight"] = np.uint32(bool(wt["watertight"]))
         out[p + "n_boundary"] = np.uint32(wt["n_boundary"])

@@ -123,3 +123,24 @@ def test_the_batched_ladder_reproduces_the_reference_verdicts(slab, oracle):
         if slab["s2_accepted"][k]:
             assert trace_deg(mine, ref) <= ROT_DEG and origin_t(mine, ref, op["scales"].t) <= TRANS_T
             assert abs(c.scores.tight - reference_scores(slab, k)["tight"]) <= VERIFY_TOL["tight"]
+
+
+@pytest.mark.parametrize("name", ["pieceA", "pieceB"])
+def test_segmentation_reproduces_every_stage_of_the_fixture(slab, oracle, name):
+    """R 3.4 end to end (segment.rs:511-631) on the dump's working mesh, t and res, against
+    every intermediate the fixture records. The reference's own gate (sherd-parity
+    stages/segmentation.rs:48-63) is area agreement >= 0.995; the restatement, with its balls
+    summed in ascending face order as PointTree::within returns them, meets it exactly."""
+    p = piece(slab, name)
+    mesh = oracle.Mesh(p["V"], p["F"])
+    labels, info, tr = oracle.segment(mesh, p["V"], p["F"], float(p["thick_t"]), float(p["res"]))
+    votes, radius, angle, _ = p["seg_info"]
+    assert info.votes == votes and info.smooth_radius == radius and info.boundary_angle == angle
+    assert info.n_rep == len(p["seg_rep"])
+    assert np.array_equal(tr["rep"][tr["near"]], p["seg_rep"][p["seg_near"]])
+    cos = np.clip(np.sum(tr["ns"] * p["seg_NS"], axis=1), -1.0, 1.0)
+    assert np.degrees(np.arccos(cos)).max() < 1e-4
+    assert np.array_equal(tr["good"], p["seg_good"])
+    for k in ("frac_raw", "frac_majority", "frac_islands", "has_ref"):
+        assert np.array_equal(tr[k], p["seg_" + k]), k
+    assert np.array_equal(labels, p["frac"])
