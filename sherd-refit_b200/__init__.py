@@ -8,8 +8,8 @@ verification and the batched persistent stage-2 path, plus the differentiable po
 """
 
 from ._abi import (AdjointOptions, Candidate, IcpOptions, InsideOutcome, Params, Registration,
-                   Scales, Scores, SherdError, WorkItem, REDUCE_ALL, REDUCE_MIN, SCHED_BATCHED,
-                   SCHED_PLAIN, exported_symbols, lib)
+                   Scales, Scores, SegInfo, SegParams, SherdError, WorkItem, REDUCE_ALL,
+                   REDUCE_MIN, SCHED_BATCHED, SCHED_PLAIN, exported_symbols, lib)
 from .backend import (CANDIDATE, WORK_ITEM, Batch, Cloud, Context, CudaExecutor, DistBatch,
                       IcpBatch, InsideBatch, Mesh, Pair, Surfaces, accept, candidates,
                       default_params, scales_for_pair, work_item_array, work_items)
@@ -18,7 +18,14 @@ __all__ = [
     "AdjointOptions", "Batch", "CANDIDATE", "WORK_ITEM", "candidates", "work_item_array",
     "Candidate", "Cloud", "Context", "CudaExecutor", "DistBatch", "IcpBatch", "IcpOptions",
     "InsideBatch", "InsideOutcome", "Mesh", "Pair", "Params", "Registration", "Scales", "Scores",
-    "SherdError", "Surfaces", "WorkItem", "REDUCE_ALL", "REDUCE_MIN", "SCHED_BATCHED",
+    "SegInfo", "SegParams", "SherdError", "Surfaces", "WorkItem", "REDUCE_ALL", "REDUCE_MIN", "SCHED_BATCHED",
     "SCHED_PLAIN", "accept", "default_params", "exported_symbols", "lib", "scales_for_pair",
-    "work_items",
+    "seg_params_default", "work_items",
 ]
+
+
+def seg_params_default() -> SegParams:
+    """SegParams::default (fragment/segment.rs:107-118), from the library."""
+    p = SegParams()
+    lib().sherd_seg_params_default(p)
+    return p

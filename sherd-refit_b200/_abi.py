@@ -102,6 +102,24 @@ class AdjointOptions(C.Structure):
 
 ADJOINT_VALUES = 5
 
+
+class SegParams(C.Structure):
+    _fields_ = [("smooth_res", C.c_double), ("coarse_at", C.c_double),
+                ("boundary_angle", C.c_double), ("votes", C.c_uint32),
+                ("votes_coarse", C.c_uint32), ("smoothed_hit_normal", C.c_uint32),
+                ("boundary_angle_auto", C.c_uint32)]
+
+
+class SegInfo(C.Structure):
+    _fields_ = [("votes", C.c_uint32), ("n_rep", C.c_uint32), ("smooth_radius", C.c_double),
+                ("boundary_angle", C.c_double)]
+
+
+class SegTrace(C.Structure):
+    _fields_ = [("rep", C.c_void_p), ("near", C.c_void_p), ("ns", C.c_void_p),
+                ("good", C.c_void_p), ("frac_raw", C.c_void_p), ("frac_majority", C.c_void_p),
+                ("frac_islands", C.c_void_p), ("has_ref", C.c_void_p)]
+
 _lib = None
 
 _SIGNATURES = {
@@ -158,6 +176,10 @@ _SIGNATURES = {
     "sherd_batch_free": (C.c_int, [VP]),
     "sherd_adjoint": (C.c_int, [VP, VP, C.c_uint32, F64P, F64P, C.c_uint32,
                                 C.POINTER(AdjointOptions), F64P, F64P]),
+    "sherd_seg_params_default": (None, [C.POINTER(SegParams)]),
+    "sherd_segment": (C.c_int, [VP, VP, F64P, C.c_uint32, U32P, C.c_uint32, C.c_double,
+                                C.c_double, C.POINTER(SegParams), U8P, C.POINTER(SegInfo),
+                                C.POINTER(SegTrace)]),
 }
 
 

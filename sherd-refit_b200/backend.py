@@ -234,6 +234,34 @@ class Context:
                                                        C.cast(out, C.c_void_p)))
         return out
 
+    # -- segmentation ---------------------------------------------------------------------------
+    def segment(self, mesh: "Mesh", v, f, thick, res, params: A.SegParams | None = None,
+                trace=False):
+        """segment::segment_faces (fragment/segment.rs:476-631): shell (0) / fracture (1)
+        labels of the working mesh (v f64, f) whose ray scene is `mesh`, with R 3.2's wall
+        `thick` and the median edge `res`. Returns (labels, SegInfo) or, with trace=True,
+        (labels, SegInfo, dict of every intermediate array)."""
+        v = _f64(v)
+        f = _u32(f, (-1, 3))
+        nf = len(f)
+        labels = np.zeros(nf, np.uint8)
+        info = A.SegInfo()
+        tr = None
+        if trace:
+            tr = {"rep": np.zeros(nf, np.uint32), "near": np.zeros(nf, np.uint32),
+                  "ns": np.zeros((nf, 3)), "good": np.zeros(nf, np.uint8),
+                  "frac_raw": np.zeros(nf, np.uint8), "frac_majority": np.zeros(nf, np.uint8),
+                  "frac_islands": np.zeros(nf, np.uint8), "has_ref": np.zeros(nf, np.uint8)}
+            ct = A.SegTrace(*[a.ctypes.data for a in tr.values()])
+        check(self.h, A.lib().sherd_segment(self.h, mesh.h, v, len(v), f, nf, float(thick),
+                                            float(res), C.byref(params) if params else None,
+                                            labels, C.byref(info),
+                                            C.byref(ct) if trace else None))
+        if not trace:
+            return labels, info
+        tr["rep"] = tr["rep"][:info.n_rep]
+        return labels, info, tr
+
     # -- differentiation ------------------------------------------------------------------------
     def adjoint(self, edges, poses, inverses, opts: A.AdjointOptions):
         """The group-alignment objectives of every (pose, edge): `poses` and `inverses` are

@@ -35,6 +35,7 @@ enum : uint32_t {
   ST_TIMEOUT = 2u,  // the persistent kernel ran past its time budget
   ST_ABORTED = 4u,  // the host asked the persistent kernel to stop
   ST_SCRATCH = 8u,  // a per-item scratch buffer was too small
+  ST_RANGE = 16u,   // a value outside the range a kernel's encoding supports
 };
 
 struct F3 {

@@ -9,6 +9,7 @@
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
 
 #include <algorithm>
 #include <array>
@@ -24,6 +25,7 @@
 
 #include "kernels.cuh"
 #include "adjoint.cuh"
+#include "segment.cuh"
 
 using namespace sherd;
 
@@ -153,6 +155,8 @@ int finish(sherd_ctx *ctx, const char *method, size_t items, bool timed) {
   if (st & ST_TIMEOUT) return fail(ctx, SHERD_E_TIMEOUT, std::string(method) + ": time budget spent");
   if (st & ST_STACK) return fail(ctx, SHERD_E_DEVICE, std::string(method) + ": traversal stack overflow");
   if (st & ST_SCRATCH) return fail(ctx, SHERD_E_INVALID, std::string(method) + ": scratch too small");
+  if (st & ST_RANGE)
+    return fail(ctx, SHERD_E_INVALID, std::string(method) + ": input outside the supported range");
   return SHERD_OK;
 }
 
@@ -381,9 +385,34 @@ int mesh_build(sherd_ctx *ctx, sherd_mesh *m) {
   return SHERD_OK;
 }
 
+// Builds the point LBVH over np points already on the device (normals
+// optional); `pad` is the outward padding of its boxes.
+int cloud_build_dev(sherd_ctx *ctx, const double *dp, const double *dn, uint32_t np, float pad,
+                    sherd_cloud *c) {
+  DBuf<uint32_t> sorted;
+  float lo[3], hi[3];
+  int rc = build_lbvh<false>(ctx, nullptr, 0, nullptr, dp, np, pad, POINT_LEAF, c->nodes, sorted,
+                             lo, hi);
+  if (rc) return rc;
+  CK(c->pts.alloc(np));
+  if (dn) CK(c->nrm.alloc(np));
+  k_store_pts<<<blocks_for(np), 256, 0, ctx->stream>>>(dp, dn, sorted.p, np, c->pts.p,
+                                                       dn ? c->nrm.p : nullptr);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  c->ctx = ctx;
+  CloudView &v = c->view;
+  v.nodes = c->nodes.p;
+  v.pts = c->pts.p;
+  v.nrm = dn ? c->nrm.p : nullptr;
+  v.n = np;
+  v.root_leaf = np <= uint32_t(POINT_LEAF) ? np : 0;
+  v.pad = pad;
+  return SHERD_OK;
+}
+
 int cloud_build(sherd_ctx *ctx, const double *p, const double *nrm, uint32_t np, sherd_cloud *c) {
   DBuf<double> dp, dn;
-  DBuf<uint32_t> sorted;
   int rc = upload(ctx, dp, p, size_t(3) * np);
   if (rc) return rc;
   if (nrm) {
@@ -392,25 +421,36 @@ int cloud_build(sherd_ctx *ctx, const double *p, const double *nrm, uint32_t np,
   }
   double mag = 1.0;
   for (size_t i = 0; i < size_t(3) * np; ++i) mag = std::max(mag, std::fabs(p[i]));
-  float pad = float(1e-6 * mag);
-  float lo[3], hi[3];
-  rc = build_lbvh<false>(ctx, nullptr, 0, nullptr, dp.p, np, pad, POINT_LEAF, c->nodes, sorted, lo,
-                         hi);
-  if (rc) return rc;
-  CK(c->pts.alloc(np));
-  if (nrm) CK(c->nrm.alloc(np));
-  k_store_pts<<<blocks_for(np), 256, 0, ctx->stream>>>(dp.p, nrm ? dn.p : nullptr, sorted.p, np,
-                                                       c->pts.p, nrm ? c->nrm.p : nullptr);
-  CK(cudaGetLastError());
+  return cloud_build_dev(ctx, dp.p, nrm ? dn.p : nullptr, np, float(1e-6 * mag), c);
+}
+
+// The cone's constants in f64 on the host, as segment.rs:330-355 computes
+// them: 15 degrees through to_radians and the six azimuths 2 pi (k-1) / 6.
+ConeConsts cone_consts() {
+  const double PI = 3.14159265358979323846;
+  ConeConsts cc;
+  double angle = 15.0 * (PI / 180.0);
+  cc.cos_a = std::cos(angle);
+  cc.sin_a = std::sin(angle);
+  for (int k = 1; k < 7; ++k) {
+    double phi = 2.0 * PI * double(k - 1) / 6.0;
+    cc.cp[k - 1] = std::cos(phi);
+    cc.sp[k - 1] = std::sin(phi);
+  }
+  return cc;
+}
+
+template <typename K, typename V>
+int radix_sort_pairs(sherd_ctx *ctx, const K *kin, K *kout, const V *vin, V *vout, uint32_t n,
+                     int end_bit) {
+  size_t bytes = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, int(n), 0, end_bit,
+                                     ctx->stream));
+  DBuf<unsigned char> tmp;
+  CK(tmp.alloc(bytes));
+  CK(cub::DeviceRadixSort::SortPairs(tmp.p, bytes, kin, kout, vin, vout, int(n), 0, end_bit,
+                                     ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  c->ctx = ctx;
-  CloudView &v = c->view;
-  v.nodes = c->nodes.p;
-  v.pts = c->pts.p;
-  v.nrm = nrm ? c->nrm.p : nullptr;
-  v.n = np;
-  v.root_leaf = np <= uint32_t(POINT_LEAF) ? np : 0;
-  v.pad = pad;
   return SHERD_OK;
 }
 
@@ -844,18 +884,7 @@ int sherd_cone_votes(sherd_ctx *ctx, const sherd_mesh *mesh, const double *centr
     return fail(ctx, SHERD_E_INVALID, "null argument");
   if (nf != mesh->view.nf) return fail(ctx, SHERD_E_INVALID, "face count differs from the mesh");
   if (nf == 0) return SHERD_OK;
-  // The cone's constants in f64 on the host, as segment.rs:330-355 computes
-  // them: 15 degrees through to_radians and the six azimuths 2 pi (k-1) / 6.
-  const double PI = 3.14159265358979323846;
-  ConeConsts cc;
-  double angle = 15.0 * (PI / 180.0);
-  cc.cos_a = std::cos(angle);
-  cc.sin_a = std::sin(angle);
-  for (int k = 1; k < 7; ++k) {
-    double phi = 2.0 * PI * double(k - 1) / 6.0;
-    cc.cp[k - 1] = std::cos(phi);
-    cc.sp[k - 1] = std::sin(phi);
-  }
+  ConeConsts cc = cone_consts();
   std::lock_guard<std::mutex> lock(ctx->mu);
   int rc = begin(ctx);
   if (rc) return rc;
@@ -1629,6 +1658,293 @@ int sherd_adjoint(sherd_ctx *ctx, sherd_pair *const *edges, uint32_t n_edges, co
   CK(cudaMemcpyAsync(grads, dgrad.p, sizeof(double) * n_pe * ADJ_VALUES * 6,
                      cudaMemcpyDeviceToHost, ctx->stream));
   return finish(ctx, "adjoint", n_pe, true);
+}
+
+// ---- segmentation ---------------------------------------------------------------
+
+void sherd_seg_params_default(sherd_seg_params *out) {
+  if (!out) return;
+  *out = sherd_seg_params{};
+  out->smooth_res = 0.0;
+  out->coarse_at = 0.1;
+  out->boundary_angle = 25.0;
+  out->votes = 5;
+  out->votes_coarse = 4;
+  out->smoothed_hit_normal = 0;
+  out->boundary_angle_auto = 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// drop_small_components (components.rs:170-191) on the device mask.
+int drop_small(sherd_ctx *ctx, DBuf<uint8_t> &mask, uint8_t target, double min_area,
+               const DBuf<uint32_t> &fa, const DBuf<uint32_t> &fb, uint32_t n_pairs,
+               const DBuf<double> &areas, uint32_t nf) {
+  cudaStream_t s = ctx->stream;
+  DBuf<uint32_t> parent, root, face, root2, face2;
+  DBuf<double> size;
+  CK(parent.alloc(nf));
+  CK(root.alloc(nf));
+  CK(face.alloc(nf));
+  CK(root2.alloc(nf));
+  CK(face2.alloc(nf));
+  CK(size.alloc(nf));
+  k_uf_init<<<blocks_for(nf), 256, 0, s>>>(parent.p, nf);
+  k_uf_union<<<std::max(1u, std::min(blocks_for(n_pairs), unsigned(ctx->sm_count) * 16u)), 256, 0,
+               s>>>(fa.p, fb.p, n_pairs, mask.p, target, parent.p, ctx->d_status);
+  k_uf_roots<<<blocks_for(nf), 256, 0, s>>>(parent.p, mask.p, target, nf, root.p, face.p);
+  CK(cudaGetLastError());
+  int rc = radix_sort_pairs(ctx, root.p, root2.p, face.p, face2.p, nf, 32);
+  if (rc) return rc;
+  k_component_areas<<<blocks_for(nf), 256, 0, s>>>(root2.p, face2.p, nf, areas.p, size.p);
+  k_drop_small<<<blocks_for(nf), 256, 0, s>>>(mask.p, target, nf, parent.p, size.p, min_area);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  return SHERD_OK;
+}
+
+// One radius-ball pass over every representative (k_ball), its shared memory
+// sized to the largest ball by a counting pass (k_ball_size).
+int ball_pass(sherd_ctx *ctx, const CloudView &all, const double *cent, const uint32_t *rep,
+              uint32_t n_rep, double radius, int mode, const double *normals, const double *areas,
+              const uint8_t *frac, double *out3, uint8_t *flag) {
+  cudaStream_t s = ctx->stream;
+  const unsigned grid = std::max(1u, std::min(n_rep, unsigned(ctx->sm_count) * 16u));
+  DBuf<uint32_t> mx;
+  CK(mx.alloc(2));
+  CK(cudaMemsetAsync(mx.p, 0, 8, s));
+  k_ball_size<<<std::min(blocks_for(n_rep, 128), unsigned(ctx->sm_count) * 8u), 128, 0, s>>>(
+      all, cent, rep, n_rep, radius, mode, frac, mx.p, mx.p + 1, ctx->d_status);
+  CK(cudaGetLastError());
+  uint32_t h[2];
+  CK(cudaMemcpyAsync(h, mx.p, 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  uint32_t cap = 1;
+  while (cap < h[0]) cap <<= 1;
+  const uint32_t rcap = std::max(1u, h[1]);
+  const size_t bytes = size_t(cap) * 4 + size_t(rcap) * 8;
+  if (bytes > size_t(200) << 10)
+    return fail(ctx, SHERD_E_INVALID, "a radius ball holds more faces than shared memory does");
+  CK(cudaFuncSetAttribute(k_ball, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+  k_ball<<<grid, BALL_BLOCK, bytes, s>>>(all, cent, rep, n_rep, radius, mode, normals, areas, frac,
+                                         out3, flag, cap, rcap, ctx->d_status);
+  CK(cudaGetLastError());
+  return SHERD_OK;
+}
+
+template <typename T>
+int to_host(sherd_ctx *ctx, T *host, const T *dev, size_t n) {
+  if (host && n) CK(cudaMemcpyAsync(host, dev, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  return SHERD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sherd_segment(sherd_ctx *ctx, const sherd_mesh *mesh, const double *v, uint32_t nv,
+                  const uint32_t *f, uint32_t nf, double thick, double res,
+                  const sherd_seg_params *sp_in, uint8_t *labels, sherd_seg_info *info,
+                  const sherd_seg_trace *trace) {
+  if (!ctx || !mesh || ((!v || !f || !labels) && nf)) return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (nf != mesh->view.nf) return fail(ctx, SHERD_E_INVALID, "face count differs from the mesh");
+  for (size_t i = 0; i < size_t(3) * nf; ++i)
+    if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
+  sherd_seg_params sp;
+  if (sp_in) sp = *sp_in; else sherd_seg_params_default(&sp);
+  sherd_seg_info inf{};
+  inf.votes = res > sp.coarse_at * thick ? sp.votes_coarse : sp.votes;
+  inf.smooth_radius = std::max(thick / 3.0, sp.smooth_res * res);
+  inf.boundary_angle = sp.boundary_angle;
+  if (nf == 0 || !std::isfinite(thick) || thick <= 0.0) {
+    std::fill(labels, labels + nf, uint8_t(0));
+    if (info) *info = inf;
+    return SHERD_OK;
+  }
+  double mag = 1.0;
+  for (size_t i = 0; i < size_t(3) * nv; ++i) {
+    if (!std::isfinite(v[i])) return fail(ctx, SHERD_E_INVALID, "non-finite vertex");
+    mag = std::max(mag, std::fabs(v[i]));
+  }
+  const float pad = float(1e-6 * mag);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  const unsigned grid_sm = unsigned(ctx->sm_count) * 16u;
+  DBuf<double> dv, normals, areas, cent;
+  DBuf<uint32_t> df;
+  if ((rc = upload(ctx, dv, v, size_t(3) * nv)) || (rc = upload(ctx, df, f, size_t(3) * nf))) return rc;
+  CK(normals.alloc(size_t(3) * nf));
+  CK(areas.alloc(nf));
+  CK(cent.alloc(size_t(3) * nf));
+  k_face_geometry<<<blocks_for(nf), 256, 0, s>>>(dv.p, df.p, nf, normals.p, areas.p, cent.p);
+  CK(cudaGetLastError());
+
+  // 3.4.1 the grid: the lowest face of every t/8 voxel, ascending, and each
+  // face's nearest representative.
+  DBuf<unsigned long long> mb, keys, keys2;
+  DBuf<uint32_t> idx, idx2, rep_unsorted, rep, nrep_dev, near;
+  DBuf<uint8_t> heads;
+  CK(mb.alloc(3));
+  CK(cudaMemsetAsync(mb.p, 0xFF, 3 * sizeof(unsigned long long), s));
+  k_min_bound<<<std::min(blocks_for(nf), 1024u), 256, 0, s>>>(cent.p, nf, mb.p);
+  CK(keys.alloc(nf));
+  CK(keys2.alloc(nf));
+  CK(idx.alloc(nf));
+  CK(idx2.alloc(nf));
+  k_voxel_keys<<<blocks_for(nf), 256, 0, s>>>(cent.p, nf, mb.p, thick * (1.0 / 8.0), keys.p, idx.p,
+                                              ctx->d_status);
+  CK(cudaGetLastError());
+  if ((rc = radix_sort_pairs(ctx, keys.p, keys2.p, idx.p, idx2.p, nf, 63))) return rc;
+  CK(heads.alloc(nf));
+  k_run_heads<<<blocks_for(nf), 256, 0, s>>>(keys2.p, nf, heads.p);
+  CK(rep_unsorted.alloc(nf));
+  CK(nrep_dev.alloc(1));
+  {
+    size_t bytes = 0;
+    CK(cub::DeviceSelect::Flagged(nullptr, bytes, idx2.p, heads.p, rep_unsorted.p, nrep_dev.p,
+                                  int(nf), s));
+    DBuf<unsigned char> tmp;
+    CK(tmp.alloc(bytes));
+    CK(cub::DeviceSelect::Flagged(tmp.p, bytes, idx2.p, heads.p, rep_unsorted.p, nrep_dev.p,
+                                  int(nf), s));
+    CK(cudaStreamSynchronize(s));
+  }
+  uint32_t n_rep = 0;
+  CK(cudaMemcpy(&n_rep, nrep_dev.p, 4, cudaMemcpyDeviceToHost));
+  inf.n_rep = n_rep;
+  CK(rep.alloc(n_rep));
+  {
+    size_t bytes = 0;
+    CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, rep_unsorted.p, rep.p, int(n_rep), 0, 32, s));
+    DBuf<unsigned char> tmp;
+    CK(tmp.alloc(bytes));
+    CK(cub::DeviceRadixSort::SortKeys(tmp.p, bytes, rep_unsorted.p, rep.p, int(n_rep), 0, 32, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  DBuf<double> rep_pts;
+  CK(rep_pts.alloc(size_t(3) * n_rep));
+  k_gather_points<<<blocks_for(n_rep), 256, 0, s>>>(cent.p, rep.p, n_rep, rep_pts.p);
+  CK(cudaGetLastError());
+  sherd_cloud rep_cloud, all;
+  if ((rc = cloud_build_dev(ctx, rep_pts.p, nullptr, n_rep, pad, &rep_cloud))) return rc;
+  CK(near.alloc(nf));
+  k_nearest_rep<<<std::min(blocks_for(nf, 128), grid_sm), 128, 0, s>>>(rep_cloud.view, cent.p, nf,
+                                                                       near.p, ctx->d_status);
+  CK(cudaGetLastError());
+  if ((rc = cloud_build_dev(ctx, cent.p, nullptr, nf, pad, &all))) return rc;
+
+  // 3.4.2 the smoothed normals.
+  DBuf<double> g3, ns, ref;
+  DBuf<uint8_t> gflag, good, frac, has_ref, cand;
+  CK(g3.alloc(size_t(3) * n_rep));
+  CK(gflag.alloc(n_rep));
+  CK(ns.alloc(size_t(3) * nf));
+  if ((rc = ball_pass(ctx, all.view, cent.p, rep.p, n_rep, inf.smooth_radius, BALL_NORMALS,
+                      normals.p, areas.p, nullptr, g3.p, gflag.p)))
+    return rc;
+  k_spread<<<blocks_for(nf), 256, 0, s>>>(near.p, nf, g3.p, gflag.p, ns.p, nullptr);
+  CK(cudaGetLastError());
+
+  // 3.4.3 the cone vote.
+  CK(good.alloc(nf));
+  CK(frac.alloc(nf));
+  k_cone_votes<<<blocks_for(nf, 128), 128, 0, s>>>(mesh->view, cent.p, normals.p, ns.p,
+                                                  sp.smoothed_hit_normal ? ns.p : normals.p, nf,
+                                                  thick, cone_consts(), good.p, ctx->d_status);
+  k_votes_to_frac<<<blocks_for(nf), 256, 0, s>>>(good.p, nf, inf.votes, frac.p);
+  CK(cudaGetLastError());
+  if (trace) {
+    if ((rc = to_host(ctx, trace->rep, rep.p, n_rep)) || (rc = to_host(ctx, trace->near, near.p, nf)) ||
+        (rc = to_host(ctx, trace->ns, ns.p, size_t(3) * nf)) ||
+        (rc = to_host(ctx, trace->good, good.p, nf)) ||
+        (rc = to_host(ctx, trace->frac_raw, frac.p, nf)))
+      return rc;
+  }
+
+  // 3.4.4 the majority filter.
+  if ((rc = ball_pass(ctx, all.view, cent.p, rep.p, n_rep, thick * 0.25, BALL_MAJORITY,
+                      normals.p, areas.p, frac.p, nullptr, gflag.p)))
+    return rc;
+  k_spread<<<blocks_for(nf), 256, 0, s>>>(near.p, nf, nullptr, gflag.p, nullptr, frac.p);
+  CK(cudaGetLastError());
+  if (trace && (rc = to_host(ctx, trace->frac_majority, frac.p, nf))) return rc;
+
+  // 3.4.5-3.4.6 islands, over the face adjacency.
+  const uint32_t m = 3 * nf, n_pairs = m - 1;
+  DBuf<unsigned long long> ek, ek2;
+  DBuf<uint32_t> ep, ep2, fa, fb;
+  CK(ek.alloc(m));
+  CK(ek2.alloc(m));
+  CK(ep.alloc(m));
+  CK(ep2.alloc(m));
+  k_edge_keys<<<blocks_for(nf), 256, 0, s>>>(df.p, nf, ek.p, ep.p);
+  CK(cudaGetLastError());
+  if ((rc = radix_sort_pairs(ctx, ek.p, ek2.p, ep.p, ep2.p, m, 64))) return rc;
+  CK(fa.alloc(n_pairs));
+  CK(fb.alloc(n_pairs));
+  k_face_pairs<<<blocks_for(m), 256, 0, s>>>(ek2.p, ep2.p, m, nf, fa.p, fb.p);
+  CK(cudaGetLastError());
+  const double min_frac = 0.5 * thick * thick, min_shell = 2.0 * thick * thick;
+  if ((rc = drop_small(ctx, frac, 1, min_frac, fa, fb, n_pairs, areas, nf)) ||
+      (rc = drop_small(ctx, frac, 0, min_shell, fa, fb, n_pairs, areas, nf)))
+    return rc;
+  if (trace && (rc = to_host(ctx, trace->frac_islands, frac.p, nf))) return rc;
+
+  // 3.4.7 the boundary growth against the fixed shell reference normals.
+  if (sp.boundary_angle_auto) {
+    DBuf<double> dots;
+    CK(dots.alloc(nf));
+    k_shell_dots<<<blocks_for(nf), 256, 0, s>>>(frac.p, nf, normals.p, ns.p, dots.p);
+    CK(cudaGetLastError());
+    std::vector<double> h(nf);
+    CK(cudaMemcpyAsync(h.data(), dots.p, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::vector<double> noise;
+    for (double c : h)
+      if (c <= 1.0) noise.push_back(std::acos(c) * (180.0 / 3.14159265358979323846));
+    if (!noise.empty()) {
+      std::sort(noise.begin(), noise.end());
+      size_t k = noise.size();
+      double med = k % 2 ? noise[k / 2] : (noise[k / 2 - 1] + noise[k / 2]) / 2.0;
+      inf.boundary_angle = std::max(inf.boundary_angle, med + 15.0);
+    }
+  }
+  CK(ref.alloc(size_t(3) * nf));
+  CK(has_ref.alloc(nf));
+  if ((rc = ball_pass(ctx, all.view, cent.p, rep.p, n_rep, thick * 0.5, BALL_SHELL_NORMALS,
+                      normals.p, areas.p, frac.p, g3.p, gflag.p)))
+    return rc;
+  k_spread<<<blocks_for(nf), 256, 0, s>>>(near.p, nf, g3.p, gflag.p, ref.p, has_ref.p);
+  CK(cudaGetLastError());
+  if (trace && (rc = to_host(ctx, trace->has_ref, has_ref.p, nf))) return rc;
+  const double cos_grow = std::cos(inf.boundary_angle * (3.14159265358979323846 / 180.0));
+  CK(cand.alloc(nf));
+  CK(cudaMemsetAsync(cand.p, 0, nf, s));
+  DBuf<uint32_t> flipped;
+  CK(flipped.alloc(1));
+  for (int pass = 0; pass < 60; ++pass) {
+    CK(cudaMemsetAsync(flipped.p, 0, 4, s));
+    k_grow_candidates<<<blocks_for(n_pairs), 256, 0, s>>>(fa.p, fb.p, n_pairs, frac.p, cand.p);
+    k_grow_flip<<<blocks_for(nf), 256, 0, s>>>(cand.p, frac.p, nf, normals.p, ref.p, has_ref.p,
+                                               cos_grow, flipped.p);
+    CK(cudaGetLastError());
+    uint32_t any = 0;
+    CK(cudaMemcpyAsync(&any, flipped.p, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (!any) break;
+  }
+
+  // 3.4.8 one more island pass.
+  if ((rc = drop_small(ctx, frac, 1, min_frac, fa, fb, n_pairs, areas, nf))) return rc;
+  CK(cudaMemcpyAsync(labels, frac.p, nf, cudaMemcpyDeviceToHost, s));
+  rc = finish(ctx, "segment", nf, true);
+  if (rc) return rc;
+  if (info) *info = inf;
+  return SHERD_OK;
 }
 
 }  // extern "C"
