@@ -112,13 +112,7 @@ def _barrier(world):
 
 
 def _max_over_ranks(world, x):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return x if world == 1 else _pkg("shard").max_over_ranks(x, device="cuda")
 
 
 def cpu_baseline(wl, seconds, params_fn):
@@ -258,7 +252,9 @@ def _config_dict(wl, args, extra=None):
     d = wl.describe()
     cfg = {"workload": f"{args.config}: {d['fragments']} fragments, {d['pairs']} pairs x "
                        f"{d['starts_per_pair']} starts = {d['items']} (pair, start) items",
-           **d, "sched": args.sched}
+           **d, "sched": args.sched,
+           "parallelism": (f"{int(os.environ.get('WORLD_SIZE', '1'))} ranks, one GPU each; every "
+                           "rank verifies its own starts for every pair (weak scaling)")}
     if extra:
         cfg.update(extra)
     return cfg
@@ -300,8 +296,9 @@ def main():
     sherd = _pkg()
     synth = _pkg("synth")
     workload = _pkg("workload")
+    shard = _pkg("shard")
     t_gen = time.perf_counter()
-    wl = synth.make(args.config, args.seed)
+    wl = shard.rank_workload(synth.make(args.config, args.seed), rank, args.seed)
     t_gen = time.perf_counter() - t_gen
     ctx = sherd.Context(local)
     params = sherd.default_params()
