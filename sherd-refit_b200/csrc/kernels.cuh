@@ -283,6 +283,12 @@ __global__ void __launch_bounds__(ICP_BLOCK, 4) k_icp_rung(const double4 *src, u
 
 // ---- the batched stage-2 path ----------------------------------------------------
 
+// Resident ladder CTAs per SM the register budget is cut for (65536 / (ICP_BLOCK * this)
+// registers a thread at most).
+#ifndef LADDER_BLOCKS_PER_SM
+#define LADDER_BLOCKS_PER_SM 10
+#endif
+
 struct QueueCtl {
   unsigned *head;             // next queue position to take
   const uint32_t *order;      // item indices, most expensive first
@@ -315,7 +321,7 @@ __device__ __forceinline__ bool take(const QueueCtl &q, unsigned long long start
 }
 
 // R 5.6's four point-to-plane rungs per (pair, start) (ladder.rs:142-161).
-__global__ void __launch_bounds__(ICP_BLOCK, 6) k_ladder(const PairView *pairs,
+__global__ void __launch_bounds__(ICP_BLOCK, LADDER_BLOCKS_PER_SM) k_ladder(const PairView *pairs,
                                                       const sherd_work_item *items, QueueCtl q,
                                                       int *hints, size_t hint_stride,
                                                       sherd_candidate *out, uint32_t *status) {
