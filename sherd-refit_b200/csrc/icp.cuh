@@ -155,20 +155,33 @@ __device__ __noinline__ void plane_step(IcpShared &sh, bool has_normals) {
   matmul4(u, sh.t, sh.t);
 }
 
+// A source point's match (a target slot, or -1) as the pass keeps it: an int,
+// or 16 bits (0xFFFF for none) when every target of the batch has fewer than
+// 65535 points, which halves the bytes the ladder writes and re-reads.
+__device__ __forceinline__ int hint_get(const int *h, uint32_t i) { return h[i]; }
+__device__ __forceinline__ int hint_get(const uint16_t *h, uint32_t i) {
+  uint16_t v = h[i];
+  return v == 0xFFFFu ? -1 : int(v);
+}
+__device__ __forceinline__ void hint_set(int *h, uint32_t i, int s) { h[i] = s; }
+__device__ __forceinline__ void hint_set(uint16_t *h, uint32_t i, int s) {
+  h[i] = s < 0 ? uint16_t(0xFFFFu) : uint16_t(s);
+}
+
 // Sums B..E-1 of one pass (count, err2, the 21 lower-triangle terms of J^T J
 // and the 6 of J^T r, in that order) over the correspondences found in hint[],
 // reduced over the warp into sh.red[warp][B..E). The squared distance is
 // re-formed exactly as the search formed it.
-template <int B, int E>
+template <int B, int E, class H>
 __device__ __forceinline__ void icp_accumulate(const double4 *src, uint32_t ns, const CloudView &tgt,
                                                const double *t, double r2, bool valid,
-                                               const int *hint, IcpShared &sh) {
+                                               const H *hint, IcpShared &sh) {
   double acc[E - B];
 #pragma unroll
   for (int k = 0; k < E - B; ++k) acc[k] = 0.0;
   if (valid) {
     for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) {
-      int s = hint[i];
+      int s = hint_get(hint, i);
       if (s < 0) continue;
       double4 p = src[i];
       double x, y, z;
@@ -212,8 +225,9 @@ __device__ __forceinline__ void icp_accumulate(const double4 *src, uint32_t ns, 
 // `src` under the pose sh.t; leaves the block totals in sh.sums. `hint[i]`
 // carries each source point's last match (a target slot, or -1) from pass to
 // pass as the warm start of its search.
+template <class H>
 __device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, double r2,
-                         bool valid, IcpShared &sh, int *hint, uint32_t &status) {
+                         bool valid, IcpShared &sh, H *hint, uint32_t &status) {
   double t[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) t[k] = sh.t[k];
@@ -228,7 +242,7 @@ __device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, 
       double x, y, z;
       apply_pose(t, p.x, p.y, p.z, x, y, z);
       double d2;
-      hint[i] = nearest_within_sq(tgt, x, y, z, r2, d2, status, hint[i]);
+      hint_set(hint, i, nearest_within_sq(tgt, x, y, z, r2, d2, status, hint_get(hint, i)));
     }
   }
   icp_accumulate<0, 15>(src, ns, tgt, t, r2, valid, hint, sh);
@@ -256,8 +270,9 @@ __device__ __forceinline__ void fit_rmse(const double *s, uint32_t ns, double &f
 // icp::register (icp.rs:308-356) for the pose in sh.t; every thread of the
 // block calls it. On return sh.t holds the refined pose and thread 0 has
 // written *out.
+template <class H>
 __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView &tgt,
-                               double distance, int max_iter, IcpShared &sh, int *hint,
+                               double distance, int max_iter, IcpShared &sh, H *hint,
                                sherd_registration *out, uint32_t &status) {
   if (ns == 0 || tgt.n == 0) {
     if (threadIdx.x == 0) {
@@ -273,7 +288,7 @@ __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView 
   }
   bool valid = distance > 0.0;  // a NaN radius is not valid either
   double r2 = distance * distance;
-  for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) hint[i] = -1;
+  for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) hint_set(hint, i, -1);
   icp_pass(src, ns, tgt, r2, valid, sh, hint, status);
   double fit, rmse;
   fit_rmse(sh.sums, ns, fit, rmse);

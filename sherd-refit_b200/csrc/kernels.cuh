@@ -321,13 +321,14 @@ __device__ __forceinline__ bool take(const QueueCtl &q, unsigned long long start
 }
 
 // R 5.6's four point-to-plane rungs per (pair, start) (ladder.rs:142-161).
+template <class H>
 __global__ void __launch_bounds__(ICP_BLOCK, LADDER_BLOCKS_PER_SM) k_ladder(const PairView *pairs,
                                                       const sherd_work_item *items, QueueCtl q,
-                                                      int *hints, size_t hint_stride,
+                                                      H *hints, size_t hint_stride,
                                                       sherd_candidate *out, uint32_t *status) {
   __shared__ IcpShared sh;
   uint32_t st = 0;
-  int *hint = hints + hint_stride * blockIdx.x;
+  H *hint = hints + hint_stride * blockIdx.x;
   unsigned long long start = global_ns();
   unsigned it;
   while (take(q, start, it, st)) {

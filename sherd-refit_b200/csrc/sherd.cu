@@ -1267,8 +1267,21 @@ struct sherd_batch {
   DBuf<sherd_candidate> dc;
   DBuf<uint32_t> dorder;
   DBuf<unsigned> heads, scratch;
-  DBuf<int> hints;  // per ladder CTA: each source point's last match
+  // Per ladder CTA, each source point's last match: 16 bits when every target
+  // of the batch has fewer than 65535 points, else an int.
+  DBuf<unsigned char> hints;
+  bool hint16 = true;
   size_t hint_stride = 1;
+  // Launches the ladder kernel with the batch's hint width.
+  void ladder(unsigned grid, QueueCtl q, cudaStream_t s) {
+    if (hint16)
+      k_ladder<uint16_t><<<grid, ICP_BLOCK, 0, s>>>(dv.p, di.p, q,
+                                                    reinterpret_cast<uint16_t *>(hints.p),
+                                                    hint_stride, dc.p, ctx->d_status);
+    else
+      k_ladder<int><<<grid, ICP_BLOCK, 0, s>>>(dv.p, di.p, q, reinterpret_cast<int *>(hints.p),
+                                               hint_stride, dc.p, ctx->d_status);
+  }
   // The penetration wavefront: per item the inverse pose, per (item, side)
   // unit its counters and its first chunk.
   DBuf<double> inv;
@@ -1305,8 +1318,7 @@ int launch_ladder(sherd_batch *b, cudaStream_t s) {
   unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
   CK(cudaMemsetAsync(b->heads.p, 0, 2 * sizeof(unsigned), s));
   QueueCtl ql{b->heads.p, b->dorder.p, b->n_items, ctx->abort_dev, budget};
-  k_ladder<<<std::min<unsigned>(b->grid_l, b->n_items), ICP_BLOCK, 0, s>>>(
-      b->dv.p, b->di.p, ql, b->hints.p, b->hint_stride, b->dc.p, ctx->d_status);
+  b->ladder(std::min<unsigned>(b->grid_l, b->n_items), ql, s);
   CK(cudaGetLastError());
   return SHERD_OK;
 }
@@ -1415,6 +1427,7 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
                    double(v.a.n_pf + v.b.n_pf);
     b->max_scratch = std::max(b->max_scratch, v.scratch_floats);
     b->hint_stride = std::max<size_t>(b->hint_stride, std::max(v.n_reg, v.n_frac));
+    if (v.reg_tgt.n >= 0xFFFFu || v.frac_tgt.n >= 0xFFFFu) b->hint16 = false;
   }
   std::vector<PairView> views(n_pairs);
   for (uint32_t i = 0; i < n_pairs; ++i) views[i] = pairs[i]->view;
@@ -1444,7 +1457,7 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
   CK(cudaMemsetAsync(b->dc.p, 0, sizeof(sherd_candidate) * n_items, ctx->stream));
   CK(b->heads.alloc(2 * size_t(std::max<uint32_t>(n_pairs, 1))));
   int occ_l = 0, occ_v = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, k_ladder, ICP_BLOCK, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, k_ladder<uint16_t>, ICP_BLOCK, 0));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_v, k_verify_items, VER_BLOCK, 0));
   b->grid_l = unsigned(std::max(1, occ_l) * ctx->sm_count);
   b->grid_v = unsigned(std::max(1, occ_v) * ctx->sm_count);
@@ -1482,7 +1495,7 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
   // hint slots as the largest pair has items.
   size_t slots = b->grid_l;
   for (uint32_t c : b->pair_count) slots = std::max<size_t>(slots, c);
-  CK(b->hints.alloc(slots * b->hint_stride));
+  CK(b->hints.alloc(slots * b->hint_stride * (b->hint16 ? sizeof(uint16_t) : sizeof(int))));
   for (cudaEvent_t &e : b->ev) CK(cudaEventCreate(&e));
   CK(cudaStreamSynchronize(ctx->stream));
   if (sched == SHERD_SCHED_BATCHED) return capture(b);
@@ -1511,8 +1524,7 @@ int batch_run(sherd_batch *b, float *ms) {
       if (!cnt) continue;
       QueueCtl ql{b->heads.p + 2 * i, b->dorder.p + b->pair_first[i], cnt, ctx->abort_dev, budget};
       QueueCtl qv{b->heads.p + 2 * i + 1, b->dorder.p + b->pair_first[i], cnt, ctx->abort_dev, budget};
-      k_ladder<<<cnt, ICP_BLOCK, 0, s>>>(b->dv.p, b->di.p, ql, b->hints.p, b->hint_stride, b->dc.p,
-                                         ctx->d_status);
+      b->ladder(cnt, ql, s);
       CK(cudaGetLastError());
       k_verify_items<<<std::min<unsigned>(cnt, b->grid_v), VER_BLOCK, 0, s>>>(
           b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, nullptr,
