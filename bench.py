@@ -37,6 +37,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "pair-pose verifications/s"
 UNIT = "verifications/s"
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) of one k_ladder launch on the default collection workload (seed 0),
+# from one ncu capture of `python bench.py --steps 1 --warmup 3 --no-cpu`
+# (profiles/k_ladder_collection_dram.md).
+LADDER_TRAFFIC = {("collection", 0): (539.88 + 270.85) * 1e9}
 
 
 def _pkg(name=""):
@@ -359,8 +363,13 @@ def main():
                      "gbs": sbytes[k] / (ms / 1000.0) / 1e9 if ms > 0 else None}
     dom = max(("ladder", "verify", "pen_inside", "pen_min"), key=lambda k: stage_ms[k])
     achieved = stages[dom]["gbs"]
+    traffic = LADDER_TRAFFIC.get((args.config, args.seed)) if dom == "ladder" else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "kernel": stages[dom]["kernel"],
+                "frac": achieved / peak, "traffic": traffic,
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                   "full-size launch (profiles/k_ladder_collection_dram.md)"
+                                   if traffic else None),
+                "kernel": stages[dom]["kernel"],
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "per_unit": ("48 B per ICP point-iteration (16 B source point + 32 B matched "
                              "target point and normal) over the passes each rung ran"
