@@ -86,6 +86,12 @@ typedef struct sherd_params {
         near_delta, pen_delta, nms_delta, icp_delta;
     double coarse_res, stage1_res, tight_res, facing_res, gap_res, seam_res,
         near_res, pen_res, icp_res;
+    /* R 5.6's early rejection (params.rs:78-80, pair.rs:315-340), 0 = off:
+     * after the two pc_reg rungs an item whose fracture tight fraction is
+     * below this keeps those scores (partial), skips the pc_frac rungs and
+     * the rest of R 6, and is rejected. Its rungs[2] and rungs[3] are not
+     * run: they hold the pose after rungs[1] with zero counts. */
+    double early_reject_tight;
 } sherd_params;
 
 /* Scores (matching/verify.rs:72-135): the twenty numbers of R 6. */

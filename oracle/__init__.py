@@ -46,7 +46,7 @@ class Params(C.Structure):
         "coarse_delta", "stage1_delta", "tight_delta", "facing_delta", "seam_delta",
         "near_delta", "pen_delta", "nms_delta", "icp_delta",
         "coarse_res", "stage1_res", "tight_res", "facing_res", "gap_res", "seam_res",
-        "near_res", "pen_res", "icp_res")]
+        "near_res", "pen_res", "icp_res", "early_reject_tight")]
 
 
 SCORE_FIELDS = ("tight_a", "tight_b", "tight", "gap_a", "gap_b", "gap", "contact_a",
@@ -440,7 +440,7 @@ def default_params() -> Params:
                   seam_delta=0.12, near_delta=0.5, pen_delta=0.06, nms_delta=0.5,
                   icp_delta=0.04, coarse_res=2.3, stage1_res=0.9, tight_res=0.15,
                   facing_res=1.0, gap_res=0.45, seam_res=1.8, near_res=4.0, pen_res=0.9,
-                  icp_res=0.6)
+                  icp_res=0.6, early_reject_tight=0.0)
 
 
 def collection(wl, params=None):

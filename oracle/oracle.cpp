@@ -1138,6 +1138,21 @@ sherd_candidate ladder_verify(const Pair &pr, const sherd_work_item &item,
   double pose[16];
   std::memcpy(pose, item.init, sizeof pose);
   for (int r = 0; r < 4; ++r) {
+    if (r == 2 && p.early_reject_tight > 0.0) {
+      // R 5.6's early rejection (pair.rs:315-340): the fracture scores at the
+      // pc_reg pose, and below the limit the partial scores of verify.rs:584-
+      // 617 with the pc_frac rungs not run.
+      sherd_scores s = verify(*pr.a, *pr.b, pose, pr.sc, false);
+      if (s.tight < p.early_reject_tight) {
+        for (int q = 2; q < 4; ++q) {
+          c.rungs[q] = sherd_registration{};
+          std::memcpy(c.rungs[q].transform, pose, sizeof pose);
+        }
+        c.scores = s;
+        c.accepted = 0;
+        return c;
+      }
+    }
     sherd_icp_options o{SHERD_POINT_TO_PLANE, 30, K[r] * pr.sc.t * pr.sc.icp};
     const std::vector<double> &src = r < 2 ? pr.reg_source : pr.frac_source;
     const Cloud &tgt = r < 2 ? *pr.reg_target : *pr.frac_target;

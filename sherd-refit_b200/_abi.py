@@ -61,7 +61,7 @@ PARAM_FIELDS = ("min_tight", "max_gap", "max_pen", "min_seam", "min_cont_n",
                 "coarse_delta", "stage1_delta", "tight_delta", "facing_delta", "seam_delta",
                 "near_delta", "pen_delta", "nms_delta", "icp_delta",
                 "coarse_res", "stage1_res", "tight_res", "facing_res", "gap_res", "seam_res",
-                "near_res", "pen_res", "icp_res")
+                "near_res", "pen_res", "icp_res", "early_reject_tight")
 
 
 class Params(C.Structure):

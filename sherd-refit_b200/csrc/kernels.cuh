@@ -320,12 +320,16 @@ __device__ __forceinline__ bool take(const QueueCtl &q, unsigned long long start
   return slot != 0xFFFFFFFFu;
 }
 
-// R 5.6's four point-to-plane rungs per (pair, start) (ladder.rs:142-161).
+// R 5.6's point-to-plane rungs r_lo..r_hi-1 of the four per (pair, start)
+// (ladder.rs:142-161): from the item's start pose when r_lo is 0, else from
+// its rung r_lo - 1. With skip_partial, items an early rejection left partial
+// are passed over.
 template <class H>
 __global__ void __launch_bounds__(ICP_BLOCK, LADDER_BLOCKS_PER_SM) k_ladder(const PairView *pairs,
                                                       const sherd_work_item *items, QueueCtl q,
                                                       H *hints, size_t hint_stride,
-                                                      sherd_candidate *out, uint32_t *status) {
+                                                      sherd_candidate *out, int r_lo, int r_hi,
+                                                      int skip_partial, uint32_t *status) {
   __shared__ IcpShared sh;
   uint32_t st = 0;
   H *hint = hints + hint_stride * blockIdx.x;
@@ -335,14 +339,16 @@ __global__ void __launch_bounds__(ICP_BLOCK, LADDER_BLOCKS_PER_SM) k_ladder(cons
     const sherd_work_item &w = items[it];
     const PairView &pr = pairs[w.pair];
     sherd_candidate *c = out + it;
-    if (threadIdx.x < 16) sh.t[threadIdx.x] = w.init[threadIdx.x];
-    if (threadIdx.x == 0) {
+    if (skip_partial && c->scores.partial) continue;  // the same for the whole block
+    if (threadIdx.x < 16)
+      sh.t[threadIdx.x] = r_lo == 0 ? w.init[threadIdx.x] : c->rungs[r_lo - 1].transform[threadIdx.x];
+    if (threadIdx.x == 0 && r_lo == 0) {
       c->pair = w.pair;
       c->start = w.start;
     }
     __syncthreads();
     const double k[4] = {0.2, 0.08, 0.08, 0.04};
-    for (int r = 0; r < 4; ++r) {
+    for (int r = r_lo; r < r_hi; ++r) {
       double distance = k[r] * pr.sc.t * pr.sc.icp;
       if (r < 2)
         icp_rung_block(pr.reg_src, pr.n_reg, pr.reg_tgt, distance, 30, sh, hint, &c->rungs[r], st);
@@ -354,15 +360,18 @@ __global__ void __launch_bounds__(ICP_BLOCK, LADDER_BLOCKS_PER_SM) k_ladder(cons
   if (st) atomicOr(status, st);
 }
 
-// R 6 + R 6.5 at each item's last rung pose (verify.rs:590-638). With `inv`
-// set, the penetration half is left to the wavefront kernels below and the
-// inverse pose of every item is written for them.
+// R 6 + R 6.5 at each item's rung `pose_rung` pose (verify.rs:590-638): the
+// last rung, or rung 1 for R 5.6's early-rejection check (full = 0). With
+// `inv` set, the penetration half is left to the wavefront kernels below and
+// the inverse pose of every item is written for them. With skip_partial,
+// items an early rejection left partial are passed over.
 __global__ void __launch_bounds__(VER_BLOCK, 3) k_verify_items(const PairView *pairs,
                                                             const sherd_work_item *items,
                                                             QueueCtl q, sherd_params p,
                                                             unsigned *scratch, size_t stride,
                                                             sherd_candidate *out, int full,
-                                                            double *inv, uint32_t *status) {
+                                                            double *inv, int pose_rung,
+                                                            int skip_partial, uint32_t *status) {
   __shared__ VerShared sh;
   uint32_t st = 0;
   unsigned long long start = global_ns();
@@ -371,7 +380,8 @@ __global__ void __launch_bounds__(VER_BLOCK, 3) k_verify_items(const PairView *p
   while (take(q, start, it, st)) {
     const PairView &pr = pairs[items[it].pair];
     sherd_candidate *c = out + it;
-    if (threadIdx.x < 16) sh.t[threadIdx.x] = c->rungs[3].transform[threadIdx.x];
+    if (skip_partial && c->scores.partial) continue;  // the same for the whole block
+    if (threadIdx.x < 16) sh.t[threadIdx.x] = c->rungs[pose_rung].transform[threadIdx.x];
     __syncthreads();
     if (pr.scratch_floats > stride) {
       if (threadIdx.x == 0) {
@@ -385,6 +395,32 @@ __global__ void __launch_bounds__(VER_BLOCK, 3) k_verify_items(const PairView *p
                  inv ? inv + 16 * size_t(it) : nullptr);
   }
   if (st) atomicOr(status, st);
+}
+
+// R 5.6's early rejection (pair.rs:315-340) after the fracture and seam
+// scores at rung 1: an item below the tight limit keeps those partial scores,
+// is rejected, and its pc_frac rungs stay unrun (the rung-1 pose, zero
+// counts); the others are cleared to go on.
+__global__ void k_early_mark(sherd_candidate *cands, const uint32_t *order, uint32_t n,
+                             double limit) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  sherd_candidate &c = cands[order[k]];
+  if (c.status) return;
+  if (c.scores.tight < limit) {
+    for (int r = 2; r < 4; ++r) {
+      sherd_registration &g = c.rungs[r];
+      for (int k = 0; k < 16; ++k) g.transform[k] = c.rungs[1].transform[k];
+      g.fitness = 0.0;
+      g.inlier_rmse = 0.0;
+      g.correspondences = 0;
+      g.iterations = 0;
+      g.converged = 0;
+    }
+    c.accepted = 0;
+  } else {
+    c.scores.partial = 0;
+  }
 }
 
 // ---- the penetration wavefront of the batched path ------------------------------
@@ -423,7 +459,8 @@ __device__ __forceinline__ PenUnit pen_unit(const PairView *pairs, const sherd_w
   uint32_t item = u >> 1, side = u & 1u;
   const PairView &pr = pairs[items[item].pair];
   PenUnit x;
-  x.avail = pr.a.has_mesh && pr.b.has_mesh && pr.a.watertight && pr.b.watertight;
+  x.avail = pr.a.has_mesh && pr.b.has_mesh && pr.a.watertight && pr.b.watertight &&
+            !cands[item].scores.partial;
   x.pts = side ? pr.a.s : pr.b.s;
   x.n = side ? pr.a.n_s : pr.b.n_s;
   x.mesh = side ? &pr.b.mesh : &pr.a.mesh;
@@ -645,7 +682,7 @@ __global__ void k_pen_finalize(const PairView *pairs, const sherd_work_item *ite
   if (it >= n_items) return;
   const PairView &pr = pairs[items[it].pair];
   sherd_candidate &c = cands[it];
-  if (c.status) return;
+  if (c.status || c.scores.partial) return;  // an early rejection's scores are final
   sherd_scores &s = c.scores;
   bool avail = pr.a.has_mesh && pr.b.has_mesh && pr.a.watertight && pr.b.watertight;
   if (avail) {

@@ -1116,7 +1116,7 @@ void sherd_params_default(sherd_params *p) {
   if (!p) return;
   *p = sherd_params{0.25, 0.03, 0.005, 3.0, 0.8,
                     0.15, 0.06, 0.01, 0.3, 0.12, 0.5, 0.06, 0.5, 0.04,
-                    2.3, 0.9, 0.15, 1.0, 0.45, 1.8, 4.0, 0.9, 0.6};
+                    2.3, 0.9, 0.15, 1.0, 0.45, 1.8, 4.0, 0.9, 0.6, 0.0};
 }
 
 int sherd_scales_for_pair(const sherd_params *p, double t, double res, sherd_scales *out) {
@@ -1191,7 +1191,7 @@ int sherd_verify(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfaces *
   sherd_params p;
   sherd_params_default(&p);
   k_verify_items<<<1, VER_BLOCK, 0, ctx->stream>>>(dv.p, di.p, q, p, scratch.p, v.scratch_floats, dc.p,
-                                                  full, nullptr, ctx->d_status);
+                                                  full, nullptr, 3, 0, ctx->d_status);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(&cand, dc.p, sizeof cand, cudaMemcpyDeviceToHost, ctx->stream));
   rc = finish(ctx, "verify", 1, true);
@@ -1272,16 +1272,22 @@ struct sherd_batch {
   DBuf<unsigned char> hints;
   bool hint16 = true;
   size_t hint_stride = 1;
-  // Launches the ladder kernel with the batch's hint width.
-  void ladder(unsigned grid, QueueCtl q, cudaStream_t s) {
+  // Launches the ladder kernel (rungs r_lo..r_hi-1) with the batch's hint width.
+  void ladder(unsigned grid, QueueCtl q, cudaStream_t s, int r_lo, int r_hi, int skip_partial) {
     if (hint16)
       k_ladder<uint16_t><<<grid, ICP_BLOCK, 0, s>>>(dv.p, di.p, q,
                                                     reinterpret_cast<uint16_t *>(hints.p),
-                                                    hint_stride, dc.p, ctx->d_status);
+                                                    hint_stride, dc.p, r_lo, r_hi, skip_partial,
+                                                    ctx->d_status);
     else
       k_ladder<int><<<grid, ICP_BLOCK, 0, s>>>(dv.p, di.p, q, reinterpret_cast<int *>(hints.p),
-                                               hint_stride, dc.p, ctx->d_status);
+                                               hint_stride, dc.p, r_lo, r_hi, skip_partial,
+                                               ctx->d_status);
   }
+  bool early() const { return params.early_reject_tight > 0.0; }
+  // Queue heads per group of items (the whole batch, or one pair of the plain
+  // schedule): ladder, verification, early-rejection check, fine ladder.
+  static constexpr int HEADS = 4;
   // The penetration wavefront: per item the inverse pose, per (item, side)
   // unit its counters and its first chunk.
   DBuf<double> inv;
@@ -1313,14 +1319,37 @@ namespace {
 // reset and the persistent ladder kernel; the persistent fracture, seam and
 // continuity kernel; the penetration box/parity/depth wavefront; its minimum
 // pass; the finalising pass.
-int launch_ladder(sherd_batch *b, cudaStream_t s) {
+// The ladder stage of one group of items (`order[0..n)`, queues at `heads`):
+// the four rungs, or, with R 5.6's early rejection, the two pc_reg rungs, the
+// fracture and seam scores at rung 1, the marking, and the two pc_frac rungs
+// of the items that go on (pair.rs:309-346).
+int ladder_stage(sherd_batch *b, cudaStream_t s, unsigned *heads, const uint32_t *order,
+                 uint32_t n, unsigned grid) {
   sherd_ctx *ctx = b->ctx;
   unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
-  CK(cudaMemsetAsync(b->heads.p, 0, 2 * sizeof(unsigned), s));
-  QueueCtl ql{b->heads.p, b->dorder.p, b->n_items, ctx->abort_dev, budget};
-  b->ladder(std::min<unsigned>(b->grid_l, b->n_items), ql, s);
+  const bool early = b->early();
+  QueueCtl q0{heads, order, n, ctx->abort_dev, budget};
+  b->ladder(grid, q0, s, 0, early ? 2 : 4, 0);
   CK(cudaGetLastError());
+  if (early) {
+    QueueCtl q1{heads + 2, order, n, ctx->abort_dev, budget};
+    k_verify_items<<<std::min<unsigned>(b->grid_v, n), VER_BLOCK, 0, s>>>(
+        b->dv.p, b->di.p, q1, b->params, b->scratch.p, b->max_scratch, b->dc.p, 0, nullptr, 1, 0,
+        ctx->d_status);
+    k_early_mark<<<blocks_for(n), 256, 0, s>>>(b->dc.p, order, n, b->params.early_reject_tight);
+    CK(cudaGetLastError());
+    QueueCtl q2{heads + 3, order, n, ctx->abort_dev, budget};
+    b->ladder(grid, q2, s, 2, 4, 1);
+    CK(cudaGetLastError());
+  }
   return SHERD_OK;
+}
+
+int launch_ladder(sherd_batch *b, cudaStream_t s) {
+  sherd_ctx *ctx = b->ctx;
+  CK(cudaMemsetAsync(b->heads.p, 0, sherd_batch::HEADS * sizeof(unsigned), s));
+  return ladder_stage(b, s, b->heads.p, b->dorder.p, b->n_items,
+                      std::min<unsigned>(b->grid_l, b->n_items));
 }
 
 int launch_verify_items(sherd_batch *b, cudaStream_t s) {
@@ -1328,8 +1357,8 @@ int launch_verify_items(sherd_batch *b, cudaStream_t s) {
   unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
   QueueCtl qv{b->heads.p + 1, b->dorder.p, b->n_items, ctx->abort_dev, budget};
   k_verify_items<<<std::min<unsigned>(b->grid_v, b->n_items), VER_BLOCK, 0, s>>>(
-      b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, b->inv.p,
-      ctx->d_status);
+      b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, b->inv.p, 3,
+      b->early() ? 1 : 0, ctx->d_status);
   CK(cudaGetLastError());
   return SHERD_OK;
 }
@@ -1455,7 +1484,7 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
     return rc;
   CK(b->dc.alloc(n_items));
   CK(cudaMemsetAsync(b->dc.p, 0, sizeof(sherd_candidate) * n_items, ctx->stream));
-  CK(b->heads.alloc(2 * size_t(std::max<uint32_t>(n_pairs, 1))));
+  CK(b->heads.alloc(sherd_batch::HEADS * size_t(std::max<uint32_t>(n_pairs, 1))));
   int occ_l = 0, occ_v = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, k_ladder<uint16_t>, ICP_BLOCK, 0));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_v, k_verify_items, VER_BLOCK, 0));
@@ -1517,18 +1546,18 @@ int batch_run(sherd_batch *b, float *ms) {
     }
   } else {
     unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
-    CK(cudaMemsetAsync(b->heads.p, 0, sizeof(unsigned) * 2 * b->n_pairs, s));
+    CK(cudaMemsetAsync(b->heads.p, 0, sizeof(unsigned) * sherd_batch::HEADS * b->n_pairs, s));
     CK(cudaEventRecord(b->ev[0], s));
     for (uint32_t i = 0; i < b->n_pairs; ++i) {
       uint32_t cnt = b->pair_count[i];
       if (!cnt) continue;
-      QueueCtl ql{b->heads.p + 2 * i, b->dorder.p + b->pair_first[i], cnt, ctx->abort_dev, budget};
-      QueueCtl qv{b->heads.p + 2 * i + 1, b->dorder.p + b->pair_first[i], cnt, ctx->abort_dev, budget};
-      b->ladder(cnt, ql, s);
-      CK(cudaGetLastError());
+      unsigned *heads = b->heads.p + sherd_batch::HEADS * size_t(i);
+      const uint32_t *order = b->dorder.p + b->pair_first[i];
+      if ((rc = ladder_stage(b, s, heads, order, cnt, cnt))) return rc;
+      QueueCtl qv{heads + 1, order, cnt, ctx->abort_dev, budget};
       k_verify_items<<<std::min<unsigned>(cnt, b->grid_v), VER_BLOCK, 0, s>>>(
-          b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, nullptr,
-          ctx->d_status);
+          b->dv.p, b->di.p, qv, b->params, b->scratch.p, b->max_scratch, b->dc.p, 1, nullptr, 3,
+          b->early() ? 1 : 0, ctx->d_status);
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(s));
     }

@@ -287,3 +287,37 @@ def test_abort_reaches_a_running_batch(sherd, gpu_ctx, gpu_slab, slab):
         th.join()
     out = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items[:10], sherd.default_params())
     assert out[4].accepted == 1
+
+
+@pytest.mark.parametrize("sched", [0, 1])
+@pytest.mark.parametrize("limit", [0.1, 0.3])
+def test_early_rejection_matches_the_oracle(sherd, gpu_ctx, gpu_slab, cpu_slab, oracle, slab,
+                                            sched, limit):
+    """R 5.6's early rejection under both schedules: the same items rejected early as the
+    oracle, their pc_frac rungs unrun, partial scores within D 10.2 of the oracle's, and the
+    same verdicts for every item."""
+    params = slab_params(oracle, slab)
+    params.early_reject_tight = limit
+    sparams = sherd.default_params()
+    for f in ("min_tight", "max_gap", "max_pen", "min_seam", "min_cont_n", "early_reject_tight"):
+        setattr(sparams, f, getattr(params, f))
+    items = [(0, k, slab["starts"][k]) for k in range(len(slab["starts"]))]
+    cand_g = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items, sparams, sched)
+    witems = [oracle.WorkItem(0, k, (C.c_double * 16)(*slab["starts"][k].reshape(16)))
+              for k in range(len(items))]
+    cand_c, _ = oracle.ladder_verify_batch([cpu_slab["pair"]], witems, params)
+    n_partial = 0
+    for g, c in zip(cand_g, cand_c):
+        assert g.status == 0
+        assert g.scores.partial == c.scores.partial
+        assert g.accepted == c.accepted
+        if g.scores.partial:
+            n_partial += 1
+            assert g.accepted == 0
+            for q in (2, 3):
+                assert g.rungs[q].transform[:] == g.rungs[1].transform[:]
+                assert g.rungs[q].iterations == 0
+            for key, tol in VERIFY_TOL.items():
+                if key in ("tight", "gap", "seam"):
+                    assert abs(getattr(g.scores, key) - getattr(c.scores, key)) <= tol, key
+    assert n_partial > 0

@@ -144,3 +144,28 @@ def test_segmentation_reproduces_every_stage_of_the_fixture(slab, oracle, name):
     for k in ("frac_raw", "frac_majority", "frac_islands", "has_ref"):
         assert np.array_equal(tr[k], p["seg_" + k]), k
     assert np.array_equal(labels, p["frac"])
+
+
+def test_early_rejection_keeps_the_partial_scores_and_skips_the_fine_rungs(slab, oracle):
+    """R 5.6 (pair.rs:315-340): below early_reject_tight at the pc_reg pose an item keeps the
+    fracture and seam scores there, is rejected and runs no pc_frac rung; the others are the
+    same as without the rule."""
+    op = oracle_pair(oracle, slab)
+    params = slab_params(oracle, slab)
+    items = [oracle.WorkItem(0, k, (C.c_double * 16)(*slab["starts"][k].reshape(16)))
+             for k in range(len(slab["starts"]))]
+    base, _ = oracle.ladder_verify_batch([op["pair"]], items, params)
+    params.early_reject_tight = 0.3
+    early, _ = oracle.ladder_verify_batch([op["pair"]], items, params)
+    rejected = [c.scores.partial == 1 for c in early]
+    assert 0 < sum(rejected) < len(items)
+    for b, e, r in zip(base, early, rejected):
+        assert bytes(e.rungs[0]) == bytes(b.rungs[0]) and bytes(e.rungs[1]) == bytes(b.rungs[1])
+        if r:
+            assert e.accepted == 0 and e.scores.tight < 0.3
+            assert e.scores.cont == 1.0 and e.scores.cont_n == -1.0 and e.scores.pen == 0.0
+            for q in (2, 3):
+                assert e.rungs[q].transform[:] == b.rungs[1].transform[:]
+                assert e.rungs[q].iterations == 0 and e.rungs[q].correspondences == 0
+        else:
+            assert bytes(e) == bytes(b)
