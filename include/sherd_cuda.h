@@ -256,6 +256,19 @@ int sherd_nearest_below(sherd_ctx *ctx, const sherd_cloud *cloud,
                         const double *queries, uint32_t n, double bound,
                         uint32_t *idx, double *dist);
 
+/* Executor::coarse_scores (executor/mod.rs:110, cpu.rs:46-68,136-169): for
+ * each of the k row-major 4x4 `poses` (Poses::Homogeneous; a Split batch
+ * passes its rotations and translations as 4x4), the fraction of the n
+ * `points` whose moved position has its nearest `target` point strictly
+ * within `radius` (PointTree::nearest_below, ties to the lowest index) and
+ * whose turned normal agrees with that point's normal (dot > normal_agree):
+ * count / n, a division. `target` is A's breakline with its shell normals;
+ * the reference's NearMask is a prefilter that moves no score and has no
+ * counterpart here. n == 0 gives zeros. */
+int sherd_coarse_scores(sherd_ctx *ctx, const sherd_cloud *target, const double *points,
+                        const double *normals, uint32_t n, const double *poses, uint32_t k,
+                        double radius, double normal_agree, double *out);
+
 /* ---- ICP (matching/icp.rs:308-440) ------------------------------------- */
 
 /* Executor::icp_rung (executor/mod.rs:114, cpu.rs:70-82): one

@@ -148,6 +148,8 @@ def lib() -> C.CDLL:
         "or_adjoint": (None, [vp, F64P, F64P, C.POINTER(AdjointOptions), C.c_int, I32P, F64P,
                               F64P]),
         "or_normal_equations": (None, [F64P, C.c_uint32, vp, F64P, C.c_double, F64P, F64P]),
+        "or_coarse_scores": (None, [vp, F64P, F64P, C.c_uint32, F64P, C.c_uint32, C.c_double,
+                                    C.c_double, F64P]),
         "or_segment": (None, [vp, F64P, U32P, C.c_uint32, C.c_double, C.c_double,
                               C.POINTER(SegParams), vp, U8P, C.POINTER(SegInfo),
                               C.POINTER(SegTrace)]),
@@ -327,6 +329,16 @@ def adjoint(pair: Pair, t, t_inv, opts: AdjointOptions, assign=None):
     lib().or_adjoint(pair.h, f64(t).reshape(16), f64(t_inv).reshape(16), C.byref(opts),
                      int(frozen), assign, values, grads)
     return values, grads, assign
+
+
+def coarse_scores(target: Cloud, points, normals, poses, radius, normal_agree=0.7):
+    """CpuExecutor::coarse_scores (executor/cpu.rs:46-68,136-169) for 4x4 poses."""
+    p, n = f64(points).reshape(-1, 3), f64(normals).reshape(-1, 3)
+    t = f64(poses).reshape(-1, 16)
+    out = np.empty(len(t))
+    lib().or_coarse_scores(target.h, p, n, len(p), t, len(t), float(radius), float(normal_agree),
+                           out)
+    return out
 
 
 def seg_params(**kw) -> SegParams:

@@ -1974,4 +1974,31 @@ void or_segment(const void *mesh, const double *v, const uint32_t *f, uint32_t n
           trace);
 }
 
+// CpuExecutor::coarse_scores (executor/cpu.rs:46-68) with agreeing
+// (cpu.rs:136-169), for k row-major 4x4 poses.
+void or_coarse_scores(const void *target, const double *points, const double *normals, uint32_t n,
+                      const double *poses, uint32_t k, double radius, double normal_agree,
+                      double *out) {
+  const Cloud &tgt = *static_cast<const Cloud *>(target);
+  for (uint32_t h = 0; h < k; ++h) {
+    const double *t = poses + 16 * size_t(h);
+    if (n == 0) {
+      out[h] = 0.0;
+      continue;
+    }
+    uint32_t agree = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      double moved[3], turned[3];
+      apply(t, points + 3 * size_t(i), moved);
+      uint32_t j;
+      double d;
+      if (!tgt.nearest_below(moved, radius, &j, &d)) continue;
+      rotate(t, normals + 3 * size_t(i), turned);
+      const double *m = &tgt.n[3 * size_t(j)];
+      if ((m[0] * turned[0] + m[1] * turned[1]) + m[2] * turned[2] > normal_agree) ++agree;
+    }
+    out[h] = double(agree) / double(n);
+  }
+}
+
 }  // extern "C"

@@ -10,13 +10,14 @@ verification and the batched persistent stage-2 path, plus the differentiable po
 from ._abi import (AdjointOptions, Candidate, IcpOptions, InsideOutcome, Params, Registration,
                    Scales, Scores, SegInfo, SegParams, SherdError, WorkItem, REDUCE_ALL,
                    REDUCE_MIN, SCHED_BATCHED, SCHED_PLAIN, exported_symbols, lib)
-from .backend import (CANDIDATE, WORK_ITEM, Batch, Cloud, Context, CudaExecutor, DistBatch,
-                      IcpBatch, InsideBatch, Mesh, Pair, Surfaces, accept, candidates,
+from .backend import (CANDIDATE, WORK_ITEM, Batch, Cloud, CoarseBatch, Context, CudaExecutor,
+                      DistBatch, IcpBatch, InsideBatch, Mesh, Pair, Surfaces, accept, candidates,
                       default_params, scales_for_pair, work_item_array, work_items)
 
 __all__ = [
     "AdjointOptions", "Batch", "CANDIDATE", "WORK_ITEM", "candidates", "work_item_array",
-    "Candidate", "Cloud", "Context", "CudaExecutor", "DistBatch", "IcpBatch", "IcpOptions",
+    "Candidate", "Cloud", "CoarseBatch", "Context", "CudaExecutor", "DistBatch", "IcpBatch",
+    "IcpOptions",
     "InsideBatch", "InsideOutcome", "Mesh", "Pair", "Params", "Registration", "Scales", "Scores",
     "SegInfo", "SegParams", "SherdError", "Surfaces", "WorkItem", "REDUCE_ALL", "REDUCE_MIN", "SCHED_BATCHED",
     "SCHED_PLAIN", "accept", "default_params", "exported_symbols", "lib", "scales_for_pair",

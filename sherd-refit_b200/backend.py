@@ -234,6 +234,18 @@ class Context:
                                                        C.cast(out, C.c_void_p)))
         return out
 
+    # -- the coarse breakline score -----------------------------------------------------------
+    def coarse_scores(self, target: "Cloud", points, normals, poses, radius, normal_agree=0.7):
+        """Executor::coarse_scores (executor/cpu.rs:46-68, 136-169): per 4x4 pose the fraction
+        of `points` whose nearest `target` point (A's breakline, with normals) is strictly
+        within `radius` and whose turned normal agrees with it (dot > normal_agree)."""
+        p, n = _f64(points), _f64(normals)
+        t = _f64(poses, (-1, 16))
+        out = np.empty(len(t))
+        check(self.h, A.lib().sherd_coarse_scores(self.h, target.h, p, n, len(p), t, len(t),
+                                                  float(radius), float(normal_agree), out))
+        return out
+
     # -- segmentation ---------------------------------------------------------------------------
     def segment(self, mesh: "Mesh", v, f, thick, res, params: A.SegParams | None = None,
                 trace=False):
@@ -455,6 +467,19 @@ class IcpBatch:
 
 
 @dataclass
+class CoarseBatch:
+    """CoarseBatch (executor/batch.rs:152-177), with Poses::Homogeneous 4x4 poses (a Split batch
+    stacks its rotations and translations into 4x4s). `target` is a Cloud over A's breakline
+    with its shell normals; the reference's NearMask moves no score and is not carried."""
+    target: Cloud
+    points: np.ndarray
+    normals: np.ndarray
+    poses: np.ndarray
+    radius: float
+    normal_agree: float = 0.7
+
+
+@dataclass
 class DistBatch:
     """DistBatch (executor/batch.rs:283-296)."""
     points: np.ndarray
@@ -473,10 +498,8 @@ class InsideBatch:
 
 
 class CudaExecutor:
-    """`impl Executor for CudaExecutor`: the trait's methods, answered on the device only.
-
-    `coarse_scores` (R 5.2) is not part of this backend; it raises rather than answering on
-    the host. Errors raise `SherdError`: there is no silent CPU fallback.
+    """`impl Executor for CudaExecutor`: every method of the trait, answered on the device
+    only. Errors raise `SherdError`: there is no silent CPU fallback.
     """
 
     def __init__(self, ctx: Context):
@@ -485,8 +508,9 @@ class CudaExecutor:
     def name(self) -> str:
         return self.ctx.name
 
-    def coarse_scores(self, batch):
-        raise NotImplementedError("the coarse breakline score is not on this backend")
+    def coarse_scores(self, batch: CoarseBatch) -> np.ndarray:
+        return self.ctx.coarse_scores(batch.target, batch.points, batch.normals, batch.poses,
+                                      batch.radius, batch.normal_agree)
 
     def icp_rung(self, batch: IcpBatch):
         if batch.estimation != A.POINT_TO_PLANE:

@@ -281,6 +281,39 @@ __global__ void __launch_bounds__(ICP_BLOCK, 4) k_icp_rung(const double4 *src, u
   if (st) atomicOr(status, st);
 }
 
+// Executor::coarse_scores (cpu.rs:46-68, 136-169): one warp per pose, its
+// lanes over the points, the agreeing points counted by ballot.
+__global__ void k_coarse_scores(CloudView tgt, const double *pts, const double *nrm, uint32_t n,
+                                const double *poses, uint32_t k, double radius,
+                                double normal_agree, double *out, uint32_t *status) {
+  uint32_t st = 0;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < k; h += warps) {
+    const double *t = poses + 16 * size_t(h);
+    uint32_t agree = 0;
+    for (uint32_t base = 0; base < n; base += 32) {
+      uint32_t i = base + lane;
+      bool ok = false;
+      if (i < n) {
+        double x, y, z;
+        apply_pose(t, pts[3 * size_t(i)], pts[3 * size_t(i) + 1], pts[3 * size_t(i) + 2], x, y, z);
+        double d;
+        int s = nearest_below(tgt, x, y, z, radius, d, st);
+        if (s >= 0) {
+          double u, v, w;
+          rotate_pose(t, nrm[3 * size_t(i)], nrm[3 * size_t(i) + 1], nrm[3 * size_t(i) + 2], u, v, w);
+          double4 m = ldg4(tgt.nrm + s);
+          ok = (m.x * u + m.y * v) + m.z * w > normal_agree;
+        }
+      }
+      agree += __popc(__ballot_sync(0xFFFFFFFFu, ok));
+    }
+    if (lane == 0) out[h] = n ? double(agree) / double(n) : 0.0;
+  }
+  if (st) atomicOr(status, st);
+}
+
 // ---- the batched stage-2 path ----------------------------------------------------
 
 // Resident ladder CTAs per SM the register budget is cut for (65536 / (ICP_BLOCK * this)

@@ -971,6 +971,35 @@ int sherd_nearest_below(sherd_ctx *ctx, const sherd_cloud *cloud, const double *
   return finish(ctx, "nearest_below", n, true);
 }
 
+int sherd_coarse_scores(sherd_ctx *ctx, const sherd_cloud *target, const double *points,
+                        const double *normals, uint32_t n, const double *poses, uint32_t k,
+                        double radius, double normal_agree, double *out) {
+  if (!ctx || !target || ((!points || !normals) && n) || ((!poses || !out) && k))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (!target->view.nrm) return fail(ctx, SHERD_E_INVALID, "the target carries no normals");
+  if (k == 0) return SHERD_OK;
+  for (uint32_t h = 0; h < k; ++h)
+    if (!finite_pose(poses + 16 * size_t(h))) return fail(ctx, SHERD_E_INVALID, "pose is not finite");
+  if (n == 0) {
+    std::fill(out, out + k, 0.0);
+    return SHERD_OK;
+  }
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> dp, dn, dt, dout;
+  if ((rc = upload(ctx, dp, points, size_t(3) * n)) || (rc = upload(ctx, dn, normals, size_t(3) * n)) ||
+      (rc = upload(ctx, dt, poses, size_t(16) * k)))
+    return rc;
+  CK(dout.alloc(k));
+  unsigned grid = std::min(blocks_for(size_t(k) * 32, 128), unsigned(ctx->sm_count) * 16u);
+  k_coarse_scores<<<grid, 128, 0, ctx->stream>>>(target->view, dp.p, dn.p, n, dt.p, k, radius,
+                                                 normal_agree, dout.p, ctx->d_status);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, dout.p, sizeof(double) * k, cudaMemcpyDeviceToHost, ctx->stream));
+  return finish(ctx, "coarse_scores", size_t(n) * k, true);
+}
+
 // ---- ICP -----------------------------------------------------------------------
 
 int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source, const sherd_cloud *target,

@@ -17,7 +17,10 @@ without the reference tree present:
 * stage 2 and verification (`sherd-parity/src/stages/{stage2,verify}.rs`): the sample arrays
   at the pair's own `t` (`md.Pf`, `md.fp`, `md.S`, `md.sp`, `md.margin_idx`, `md.brk_P`,
   `md.brk_ns`), the pair's `scales.json`, the starts `s1.T[nms2.kept]`, the four rung poses
-  `s2.T_reg1..s2.T_frac2`, the scores `s2.scores.json` and the verdicts `s2.accepted`.
+  `s2.T_reg1..s2.T_frac2`, the scores `s2.scores.json` and the verdicts `s2.accepted`;
+* the coarse breakline score (`executor/cpu.rs:46-68,136-169`) through R 5.4's re-score:
+  B's breakline subset `md.brk_sub`, the refined stage-1 poses `s1.T` and their scores
+  `s1.score` against A's whole breakline at `scales.stage1`.
 
 Derived arrays are computed here with numpy exactly as the reference's harness computes them:
 the f64 face normals and areas of `mesh::geometry::face_geometry` (`mesh/geometry.rs:70-96`,
@@ -135,6 +138,7 @@ def main(reference: Path) -> None:
         out[p + "S"] = s
         out[p + "brk_P"] = np.load(md / "md.brk_P.npy")
         out[p + "brk_ns"] = np.load(md / "md.brk_ns.npy")
+        out[p + "brk_sub"] = np.load(md / "md.brk_sub.npy").astype(np.uint32)
         nf_ = fn[fp]
         pm = s[margin_idx]
         nm = fn[sp[margin_idx]]
@@ -149,6 +153,8 @@ def main(reference: Path) -> None:
     out["scales"] = np.array([scales[k] for k in (
         "t", "res", "coarse", "stage1", "tight", "facing", "gap", "seam", "near", "pen", "nms",
         "icp")], dtype=np.float64)
+    out["s1_T"] = np.load(pair_dir / "s1.T.npy")
+    out["s1_score"] = np.load(pair_dir / "s1.score.npy")
     kept = np.load(pair_dir / "nms2.kept.npy").astype(np.int64)
     s1 = np.load(pair_dir / "s1.T.npy")
     out["starts"] = s1[kept]

@@ -321,3 +321,27 @@ def test_early_rejection_matches_the_oracle(sherd, gpu_ctx, gpu_slab, cpu_slab, 
                 if key in ("tight", "gap", "seam"):
                     assert abs(getattr(g.scores, key) - getattr(c.scores, key)) <= tol, key
     assert n_partial > 0
+
+
+def test_coarse_scores_are_bit_exact(sherd, gpu_ctx, oracle, slab):
+    """Executor::coarse_scores on the device: the fixture's s1.score at s1.T exactly, and the
+    oracle's scores for a 60-point probe over perturbed poses, through the Executor trait."""
+    a, b = piece(slab, "pieceA"), piece(slab, "pieceB")
+    target = gpu_ctx.cloud(a["brk_P"], a["brk_ns"])
+    sub = b["brk_sub"].astype(np.int64)
+    stage1, coarse = float(slab["scales"][3]), float(slab["scales"][2])
+    got = gpu_ctx.coarse_scores(target, b["brk_P"][sub], b["brk_ns"][sub], slab["s1_T"], stage1)
+    assert np.array_equal(got, slab["s1_score"])
+    rng = np.random.default_rng(7)
+    probe = rng.choice(len(b["brk_P"]), 60, replace=False)
+    poses = np.repeat(slab["s1_T"][:40], 8, axis=0)
+    poses[:, :3, 3] += rng.normal(size=(len(poses), 3)) * 0.3 * coarse
+    poses[::10, :3, 3] += 1000.0  # far from A: nothing within the radius
+    batch = sherd.CoarseBatch(target, b["brk_P"][probe], b["brk_ns"][probe], poses, coarse)
+    mine = sherd.CudaExecutor(gpu_ctx).coarse_scores(batch)
+    ref = oracle.coarse_scores(oracle.Cloud(a["brk_P"], a["brk_ns"]), b["brk_P"][probe],
+                               b["brk_ns"][probe], poses, coarse)
+    assert np.array_equal(mine, ref)
+    assert 0 < np.count_nonzero(mine) < len(mine)
+    empty = gpu_ctx.coarse_scores(target, np.zeros((0, 3)), np.zeros((0, 3)), poses[:3], coarse)
+    assert np.array_equal(empty, np.zeros(3))

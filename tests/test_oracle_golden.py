@@ -169,3 +169,14 @@ def test_early_rejection_keeps_the_partial_scores_and_skips_the_fine_rungs(slab,
                 assert e.rungs[q].iterations == 0 and e.rungs[q].correspondences == 0
         else:
             assert bytes(e) == bytes(b)
+
+
+def test_coarse_scores_reproduce_the_stage1_rescore(slab, oracle):
+    """R 5.4's re-score (executor/cpu.rs:46-68,136-169): B's breakline subset against A's whole
+    breakline at scales.stage1, at the fixture's refined poses s1.T, gives s1.score exactly."""
+    a, b = piece(slab, "pieceA"), piece(slab, "pieceB")
+    target = oracle.Cloud(a["brk_P"], a["brk_ns"])
+    sub = b["brk_sub"].astype(np.int64)
+    got = oracle.coarse_scores(target, b["brk_P"][sub], b["brk_ns"][sub], slab["s1_T"],
+                               float(slab["scales"][3]))
+    assert np.array_equal(got, slab["s1_score"])
