@@ -272,9 +272,11 @@ int sherd_coarse_scores(sherd_ctx *ctx, const sherd_cloud *target, const double 
 /* ---- ICP (matching/icp.rs:308-440) ------------------------------------- */
 
 /* Executor::icp_rung (executor/mod.rs:114, cpu.rs:70-82): one
- * registration_icp per init, every candidate an independent rung. Only
- * point-to-plane is implemented on the device (the stage-1 point-to-point
- * rung returns SHERD_E_INVALID). The target cloud must carry normals. */
+ * registration_icp per init, every candidate an independent rung, for both
+ * estimations: point-to-plane (the target must carry normals; a target
+ * without them leaves the pose unchanged, as icp.rs:414-416 does) and the
+ * stage-1 point-to-point rung (Eigen's umeyama without scaling, icp.rs:
+ * 527-592). */
 int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source,
                    const sherd_cloud *target, const double *inits, uint32_t k,
                    sherd_icp_options options, sherd_registration *out);

@@ -150,6 +150,7 @@ def lib() -> C.CDLL:
         "or_normal_equations": (None, [F64P, C.c_uint32, vp, F64P, C.c_double, F64P, F64P]),
         "or_coarse_scores": (None, [vp, F64P, F64P, C.c_uint32, F64P, C.c_uint32, C.c_double,
                                     C.c_double, F64P]),
+        "or_svd_rotation": (None, [F64P, F64P]),
         "or_segment": (None, [vp, F64P, U32P, C.c_uint32, C.c_double, C.c_double,
                               C.POINTER(SegParams), vp, U8P, C.POINTER(SegInfo),
                               C.POINTER(SegTrace)]),
@@ -260,11 +261,14 @@ class Cloud:
         return idx, d
 
 
-def icp_rung(source, target: Cloud, inits, distance, max_iteration=30, threads=0):
+def icp_rung(source, target: Cloud, inits, distance, max_iteration=30, threads=0,
+             point_to_point=False):
+    """icp::register for every init (icp.rs:308-356): point-to-plane, or the stage-1
+    point-to-point rung (umeyama, icp.rs:527-592) with point_to_point."""
     source = f64(source).reshape(-1, 3)
     inits = f64(inits).reshape(-1, 16)
     out = (Registration * len(inits))()
-    opt = IcpOptions(1, max_iteration, distance)
+    opt = IcpOptions(0 if point_to_point else 1, max_iteration, distance)
     lib().or_icp_rung(source, len(source), target.h, inits, len(inits), opt,
                       C.cast(out, C.c_void_p), threads or lib().or_default_threads())
     return list(out)
@@ -339,6 +343,13 @@ def coarse_scores(target: Cloud, points, normals, poses, radius, normal_agree=0.
     lib().or_coarse_scores(target.h, p, n, len(p), t, len(t), float(radius), float(normal_agree),
                            out)
     return out
+
+
+def svd_rotation(m):
+    """The rotation U diag(1, 1, det U det V) V^T of a 3x3's SVD (umeyama's, icp.rs:585-590)."""
+    r = np.empty(9)
+    lib().or_svd_rotation(f64(m).reshape(9), r)
+    return r.reshape(3, 3)
 
 
 def seg_params(**kw) -> SegParams:

@@ -751,6 +751,147 @@ void point_to_plane(const std::vector<double> &moved, const Cloud &tgt,
   }
 }
 
+// The rotation of a 3x3 SVD with the reflection on the smallest singular
+// value undone, R = U diag(1, 1, det(U) det(V)) V^T, as Eigen's umeyama takes
+// it from nalgebra 0.34.2's SVD (icp.rs:585-590; the SVD itself is
+// third-party and not in the reference tree). Restated with the eigen-
+// decomposition of m^T m by cyclic Jacobi: V its eigenvectors, singular values
+// the roots of its eigenvalues (descending), u0 and u1 from m V / sigma and
+// u2 = u0 x u1. R is unique whenever the second singular value is not zero,
+// so any exact SVD gives it up to rounding.
+void svd_rotation(const double m[3][3], double r[3][3]) {
+  double s[3][3], v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k) acc += m[k][i] * m[k][j];
+      s[i][j] = acc;
+    }
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    double off = std::fabs(s[0][1]) + std::fabs(s[0][2]) + std::fabs(s[1][2]);
+    double scale = std::fabs(s[0][0]) + std::fabs(s[1][1]) + std::fabs(s[2][2]);
+    if (!(off > 1e-30 * scale)) break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        if (s[p][q] == 0.0) continue;
+        double theta = (s[q][q] - s[p][p]) / (2.0 * s[p][q]);
+        double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < 3; ++k) {  // s <- J^T s J, v <- v J
+          double x = s[k][p], y = s[k][q];
+          s[k][p] = c * x - sn * y;
+          s[k][q] = sn * x + c * y;
+        }
+        for (int k = 0; k < 3; ++k) {
+          double x = s[p][k], y = s[q][k];
+          s[p][k] = c * x - sn * y;
+          s[q][k] = sn * x + c * y;
+        }
+        for (int k = 0; k < 3; ++k) {
+          double x = v[k][p], y = v[k][q];
+          v[k][p] = c * x - sn * y;
+          v[k][q] = sn * x + c * y;
+        }
+      }
+  }
+  int ord[3] = {0, 1, 2};
+  std::sort(ord, ord + 3, [&](int a, int b) { return s[a][a] > s[b][b]; });
+  double sv[3], u[3][3], w[3][3];
+  bool have[3];
+  double smax = std::sqrt(std::max(s[ord[0]][ord[0]], 0.0));
+  for (int k = 0; k < 3; ++k) {
+    int j = ord[k];
+    sv[k] = std::sqrt(std::max(s[j][j], 0.0));
+    for (int i = 0; i < 3; ++i) w[i][k] = v[i][j];
+    have[k] = smax > 0.0 && sv[k] > 1e-12 * smax;
+    for (int i = 0; i < 3; ++i) {
+      double mv = m[i][0] * w[0][k] + m[i][1] * w[1][k] + m[i][2] * w[2][k];
+      u[i][k] = have[k] ? mv / sv[k] : 0.0;
+    }
+  }
+  if (!have[0]) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) r[i][j] = i == j ? 1.0 : 0.0;
+    return;
+  }
+  auto cross = [](const double *a, const double *b, double *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  double c0[3] = {u[0][0], u[1][0], u[2][0]}, c1[3], c2[3];
+  if (have[1]) {  // m w1 / sigma1, made orthogonal to u0 again
+    double dp = c0[0] * u[0][1] + c0[1] * u[1][1] + c0[2] * u[2][1];
+    for (int i = 0; i < 3; ++i) c1[i] = u[i][1] - dp * c0[i];
+    double n1 = std::sqrt(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+    for (double &x : c1) x /= n1;
+  } else {
+    int e = 0;
+    for (int i = 1; i < 3; ++i)
+      if (std::fabs(c0[i]) < std::fabs(c0[e])) e = i;
+    double ev[3] = {0, 0, 0};
+    ev[e] = 1.0;
+    cross(c0, ev, c1);
+    double n1 = std::sqrt(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+    for (double &x : c1) x /= n1;
+  }
+  // u2 = u0 x u1 always: for rank 3 the SVD's own u2 is +-(u0 x u1) and the
+  // det(U) det(V) factor below absorbs the sign; for rank 2 it is the only
+  // stable choice (m w2 / sigma2 is round-off there).
+  cross(c0, c1, c2);
+  for (int i = 0; i < 3; ++i) {
+    u[i][0] = c0[i];
+    u[i][1] = c1[i];
+    u[i][2] = c2[i];
+  }
+  auto det3 = [](const double x[3][3]) {
+    return x[0][0] * (x[1][1] * x[2][2] - x[1][2] * x[2][1]) -
+           x[0][1] * (x[1][0] * x[2][2] - x[1][2] * x[2][0]) +
+           x[0][2] * (x[1][0] * x[2][1] - x[1][1] * x[2][0]);
+  };
+  double d = det3(u) * det3(w) < 0.0 ? -1.0 : 1.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      r[i][j] = u[i][0] * w[j][0] + u[i][1] * w[j][1] + d * u[i][2] * w[j][2];
+}
+
+// icp::umeyama without scaling (icp.rs:527-592) over the correspondences in
+// their order: means as sum * (1/n), the covariance with 1/n folded into each
+// term, R from the SVD, tau = mean_q - R mean_p.
+void point_to_point(const std::vector<double> &moved, const Cloud &tgt,
+                    const std::vector<Corr> &corr, double u[16]) {
+  for (int i = 0; i < 16; ++i) u[i] = (i % 5 == 0) ? 1.0 : 0.0;
+  if (corr.empty()) return;
+  double one_over_n = 1.0 / double(corr.size());
+  double sp[3] = {0, 0, 0}, sq[3] = {0, 0, 0};
+  for (const Corr &c : corr)
+    for (int k = 0; k < 3; ++k) {
+      sp[k] = sp[k] + moved[3 * c.i + k];
+      sq[k] = sq[k] + tgt.p[3 * c.j + k];
+    }
+  double mp[3], mq[3];
+  for (int k = 0; k < 3; ++k) {
+    mp[k] = sp[k] * one_over_n;
+    mq[k] = sq[k] * one_over_n;
+  }
+  double sigma[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (const Corr &c : corr) {
+    double a[3], b[3];
+    for (int k = 0; k < 3; ++k) {
+      a[k] = moved[3 * c.i + k] - mp[k];
+      b[k] = (tgt.p[3 * c.j + k] - mq[k]) * one_over_n;
+    }
+    for (int r = 0; r < 3; ++r)
+      for (int cc = 0; cc < 3; ++cc) sigma[r][cc] = sigma[r][cc] + b[r] * a[cc];
+  }
+  double rot[3][3];
+  svd_rotation(sigma, rot);
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) u[4 * i + j] = rot[i][j];
+    u[4 * i + 3] = mq[i] - (rot[i][0] * mp[0] + rot[i][1] * mp[1] + rot[i][2] * mp[2]);
+  }
+}
+
 void transform_points(std::vector<double> &pts, const double *m) {
   size_t n = pts.size() / 3;
   for (size_t i = 0; i < n; ++i) {
@@ -779,7 +920,10 @@ sherd_registration icp_register(const double *src, uint32_t ns, const Cloud &tgt
   bool converged = false;
   for (int it = 0; it < opt.max_iteration; ++it) {
     double u[16];
-    point_to_plane(moved, tgt, corr, u);
+    if (opt.estimation == SHERD_POINT_TO_POINT)
+      point_to_point(moved, tgt, corr, u);
+    else
+      point_to_plane(moved, tgt, corr, u);
     matmul4(u, t, t);
     transform_points(moved, u);
     ++iterations;
@@ -1999,6 +2143,14 @@ void or_coarse_scores(const void *target, const double *points, const double *no
     }
     out[h] = double(agree) / double(n);
   }
+}
+
+// The rotation svd_rotation takes from a row-major 3x3 (for its own test).
+void or_svd_rotation(const double *m9, double *r9) {
+  double m[3][3], r[3][3];
+  for (int i = 0; i < 9; ++i) m[i / 3][i % 3] = m9[i];
+  svd_rotation(m, r);
+  for (int i = 0; i < 9; ++i) r9[i] = r[i / 3][i % 3];
 }
 
 }  // extern "C"

@@ -147,12 +147,14 @@ class Context:
                             count=len(p))
         return arr["depth"].copy(), arr["inside"].copy()
 
-    def icp_rung(self, source, target: "Cloud", inits, distance, max_iteration=30):
-        """Executor::icp_rung (executor/cpu.rs:70-82), point-to-plane."""
+    def icp_rung(self, source, target: "Cloud", inits, distance, max_iteration=30,
+                 estimation=A.POINT_TO_PLANE):
+        """Executor::icp_rung (executor/cpu.rs:70-82): point-to-plane, or the stage-1
+        point-to-point rung (estimation=POINT_TO_POINT)."""
         s = _f64(source)
         inits = _f64(inits, (-1, 16))
         out = (A.Registration * max(len(inits), 1))()
-        opt = A.IcpOptions(A.POINT_TO_PLANE, int(max_iteration), float(distance))
+        opt = A.IcpOptions(int(estimation), int(max_iteration), float(distance))
         check(self.h, A.lib().sherd_icp_rung(self.h, ptr(s), len(s), target.h, inits, len(inits),
                                             opt, C.cast(out, C.c_void_p)))
         return list(out)[:len(inits)]
@@ -513,10 +515,9 @@ class CudaExecutor:
                                       batch.radius, batch.normal_agree)
 
     def icp_rung(self, batch: IcpBatch):
-        if batch.estimation != A.POINT_TO_PLANE:
-            raise A.SherdError(A.E_INVALID, "only the point-to-plane rung runs on the device")
         return self.ctx.icp_rung(batch.source, batch.target, batch.inits,
-                                 batch.max_correspondence_distance, batch.max_iteration)
+                                 batch.max_correspondence_distance, batch.max_iteration,
+                                 batch.estimation)
 
     def bounded_distance(self, batch: DistBatch) -> np.ndarray:
         return self.ctx.bounded_distance(batch.scene, batch.points, batch.transform,

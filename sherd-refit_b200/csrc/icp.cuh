@@ -155,6 +155,117 @@ __device__ __noinline__ void plane_step(IcpShared &sh, bool has_normals) {
   matmul4(u, sh.t, sh.t);
 }
 
+// The rotation of the SVD of m with a reflection on the smallest singular
+// value undone, R = U diag(1, 1, det(U) det(V)) V^T: the rotation part of
+// Eigen's umeyama (icp.rs:585-590). One-sided Jacobi (Hestenes): plane
+// rotations of the columns of a = m V until every two are orthogonal; then
+// a_j = sigma_j u_j, with u2 taken as u0 x u1. R is unique whenever the
+// second singular value is not zero.
+__device__ __noinline__ void svd_rotation(const double m[3][3], double r[3][3]) {
+  double a[3][3], v[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) a[i][j] = m[i][j];
+  for (int sweep = 0; sweep < 30; ++sweep) {
+    bool turned = false;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        double al = (a[0][p] * a[0][p] + a[1][p] * a[1][p]) + a[2][p] * a[2][p];
+        double be = (a[0][q] * a[0][q] + a[1][q] * a[1][q]) + a[2][q] * a[2][q];
+        double ga = (a[0][p] * a[0][q] + a[1][p] * a[1][q]) + a[2][p] * a[2][q];
+        if (!(fabs(ga) > 1e-15 * sqrt(al * be))) continue;
+        turned = true;
+        double ze = (be - al) / (2.0 * ga);
+        double tt = (ze >= 0.0 ? 1.0 : -1.0) / (fabs(ze) + sqrt(1.0 + ze * ze));
+        double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
+        for (int i = 0; i < 3; ++i) {
+          double x = a[i][p], y = a[i][q];
+          a[i][p] = c * x - sn * y;
+          a[i][q] = sn * x + c * y;
+          x = v[i][p];
+          y = v[i][q];
+          v[i][p] = c * x - sn * y;
+          v[i][q] = sn * x + c * y;
+        }
+      }
+    if (!turned) break;
+  }
+  double sv[3];
+  int ord[3] = {0, 1, 2};
+  for (int j = 0; j < 3; ++j) sv[j] = sqrt((a[0][j] * a[0][j] + a[1][j] * a[1][j]) + a[2][j] * a[2][j]);
+  for (int x = 0; x < 2; ++x)
+    for (int y = 0; y < 2 - x; ++y)
+      if (sv[ord[y]] < sv[ord[y + 1]]) {
+        int t = ord[y];
+        ord[y] = ord[y + 1];
+        ord[y + 1] = t;
+      }
+  const double smax = sv[ord[0]];
+  double u[3][3], w[3][3];
+  bool have[3];
+  for (int k = 0; k < 3; ++k) {
+    int j = ord[k];
+    for (int i = 0; i < 3; ++i) w[i][k] = v[i][j];
+    have[k] = smax > 0.0 && sv[j] > 1e-12 * smax;
+    for (int i = 0; i < 3; ++i) u[i][k] = have[k] ? a[i][j] / sv[j] : 0.0;
+  }
+  if (!have[0]) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) r[i][j] = i == j ? 1.0 : 0.0;
+    return;
+  }
+  if (!have[1]) {  // any unit vector orthogonal to u0
+    int e = fabs(u[0][0]) <= fabs(u[1][0]) ? (fabs(u[0][0]) <= fabs(u[2][0]) ? 0 : 2)
+                                          : (fabs(u[1][0]) <= fabs(u[2][0]) ? 1 : 2);
+    double ev[3] = {0.0, 0.0, 0.0};
+    ev[e] = 1.0;
+    double c[3] = {u[1][0] * ev[2] - u[2][0] * ev[1], u[2][0] * ev[0] - u[0][0] * ev[2],
+                   u[0][0] * ev[1] - u[1][0] * ev[0]};
+    double nc = sqrt((c[0] * c[0] + c[1] * c[1]) + c[2] * c[2]);
+    for (int i = 0; i < 3; ++i) u[i][1] = c[i] / nc;
+  }
+  // u2 = u0 x u1 always: for rank 3 the SVD's own u2 is +-(u0 x u1) and the
+  // det(U) det(V) factor below absorbs the sign; for rank 2, a2 / sigma2 is
+  // round-off.
+  u[0][2] = u[1][0] * u[2][1] - u[2][0] * u[1][1];
+  u[1][2] = u[2][0] * u[0][1] - u[0][0] * u[2][1];
+  u[2][2] = u[0][0] * u[1][1] - u[1][0] * u[0][1];
+  auto det3 = [](const double x[3][3]) {
+    return x[0][0] * (x[1][1] * x[2][2] - x[1][2] * x[2][1]) -
+           x[0][1] * (x[1][0] * x[2][2] - x[1][2] * x[2][0]) +
+           x[0][2] * (x[1][0] * x[2][1] - x[1][1] * x[2][0]);
+  };
+  const double d = det3(u) * det3(w) < 0.0 ? -1.0 : 1.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      r[i][j] = (u[i][0] * w[j][0] + u[i][1] * w[j][1]) + d * u[i][2] * w[j][2];
+}
+
+// icp::umeyama without scaling (icp.rs:527-592) from a point-to-point pass's
+// sums: s[0] count, s[2..5) and s[5..8) the sums of the moved source and of
+// the target points, s[8..17) the covariance already scaled by 1/n. T <- U T
+// (thread 0 only); identity when there is no correspondence.
+__device__ __noinline__ void point_step(IcpShared &sh) {
+  const double *s = sh.sums;
+  double u[16];
+  for (int i = 0; i < 16; ++i) u[i] = (i % 5 == 0) ? 1.0 : 0.0;
+  if (s[0] != 0.0) {
+    const double one_over_n = 1.0 / s[0];
+    double mp[3], mq[3], sigma[3][3], r[3][3];
+    for (int k = 0; k < 3; ++k) {
+      mp[k] = s[2 + k] * one_over_n;
+      mq[k] = s[5 + k] * one_over_n;
+    }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) sigma[i][j] = s[8 + 3 * i + j];
+    svd_rotation(sigma, r);
+    for (int i = 0; i < 3; ++i) {
+      for (int j = 0; j < 3; ++j) u[4 * i + j] = r[i][j];
+      u[4 * i + 3] = mq[i] - ((r[i][0] * mp[0] + r[i][1] * mp[1]) + r[i][2] * mp[2]);
+    }
+  }
+  matmul4(u, sh.t, sh.t);
+}
+
 // A source point's match (a target slot, or -1) as the pass keeps it: an int,
 // or 16 bits (0xFFFF for none) when every target of the batch has fewer than
 // 65535 points, which halves the bytes the ladder writes and re-reads.
@@ -221,13 +332,78 @@ __device__ __forceinline__ void icp_accumulate(const double4 *src, uint32_t ns, 
   }
 }
 
+// The sums of a point-to-point pass over the correspondences in hint[]:
+// MOMENTS gives count, err2 and the sums of the moved source and matched target
+// points (s[0..8)); otherwise the 9 covariance terms ((q - mean_q) / n)(p -
+// mean_p)^T (s[8..17)), centred as umeyama centres them (icp.rs:548-570).
+template <bool MOMENTS, class H>
+__device__ __forceinline__ void p2p_accumulate(const double4 *src, uint32_t ns,
+                                               const CloudView &tgt, const double *t, double r2,
+                                               bool valid, const H *hint, const double *mean,
+                                               double one_over_n, IcpShared &sh) {
+  constexpr int N = MOMENTS ? 8 : 9, B = MOMENTS ? 0 : 8;
+  double acc[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) acc[k] = 0.0;
+  if (valid) {
+    for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) {
+      int s = hint_get(hint, i);
+      if (s < 0) continue;
+      double4 p = src[i];
+      double x, y, z;
+      apply_pose(t, p.x, p.y, p.z, x, y, z);
+      double4 q = tgt.pts[s];
+      double dx = x - q.x, dy = y - q.y, dz = z - q.z;
+      double d2 = (dx * dx + dy * dy) + dz * dz;
+      if (!(d2 < r2)) continue;
+      if (MOMENTS) {
+        acc[0] += 1.0;
+        acc[1] += d2;
+        acc[2] += x;
+        acc[3] += y;
+        acc[4] += z;
+        acc[5] += q.x;
+        acc[6] += q.y;
+        acc[7] += q.z;
+      } else {
+        double a[3] = {x - mean[0], y - mean[1], z - mean[2]};
+        double b[3] = {(q.x - mean[3]) * one_over_n, (q.y - mean[4]) * one_over_n,
+                       (q.z - mean[5]) * one_over_n};
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[3 * r + c] += b[r] * a[c];
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double x = acc[k];
+    for (int o = 16; o; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh.red[warp][B + k] = x;
+  }
+}
+
+// sh.sums[lo..hi) from the warps' partial sums, in warp order.
+__device__ __forceinline__ void reduce_sums(IcpShared &sh, int lo, int hi) {
+  __syncthreads();
+  if (int(threadIdx.x) >= lo && int(threadIdx.x) < hi) {
+    double v = sh.red[0][threadIdx.x];
+    for (int w = 1; w < ICP_BLOCK / 32; ++w) v += sh.red[w][threadIdx.x];
+    sh.sums[threadIdx.x] = v;
+  }
+  __syncthreads();
+}
+
 // One correspondence pass (icp::correspondences + icp::normal_equations) over
 // `src` under the pose sh.t; leaves the block totals in sh.sums. `hint[i]`
 // carries each source point's last match (a target slot, or -1) from pass to
 // pass as the warm start of its search.
 template <class H>
 __device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, double r2,
-                         bool valid, IcpShared &sh, H *hint, uint32_t &status) {
+                         bool valid, IcpShared &sh, H *hint, uint32_t &status,
+                         bool point_to_point = false) {
   double t[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) t[k] = sh.t[k];
@@ -245,15 +421,19 @@ __device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, 
       hint_set(hint, i, nearest_within_sq(tgt, x, y, z, r2, d2, status, hint_get(hint, i)));
     }
   }
+  if (point_to_point) {
+    p2p_accumulate<true>(src, ns, tgt, t, r2, valid, hint, nullptr, 0.0, sh);
+    reduce_sums(sh, 0, 8);
+    double one_over_n = sh.sums[0] != 0.0 ? 1.0 / sh.sums[0] : 0.0;
+    double mean[6];
+    for (int k = 0; k < 6; ++k) mean[k] = sh.sums[2 + k] * one_over_n;
+    p2p_accumulate<false>(src, ns, tgt, t, r2, valid, hint, mean, one_over_n, sh);
+    reduce_sums(sh, 8, 17);
+    return;
+  }
   icp_accumulate<0, 15>(src, ns, tgt, t, r2, valid, hint, sh);
   icp_accumulate<15, ICP_SUMS>(src, ns, tgt, t, r2, valid, hint, sh);
-  __syncthreads();
-  if (threadIdx.x < ICP_SUMS) {
-    double v = sh.red[0][threadIdx.x];
-    for (int w = 1; w < ICP_BLOCK / 32; ++w) v += sh.red[w][threadIdx.x];
-    sh.sums[threadIdx.x] = v;
-  }
-  __syncthreads();
+  reduce_sums(sh, 0, ICP_SUMS);
 }
 
 // Open3D's (fitness, inlier_rmse) from the pass sums (icp.rs:385-391).
@@ -273,7 +453,8 @@ __device__ __forceinline__ void fit_rmse(const double *s, uint32_t ns, double &f
 template <class H>
 __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView &tgt,
                                double distance, int max_iter, IcpShared &sh, H *hint,
-                               sherd_registration *out, uint32_t &status) {
+                               sherd_registration *out, uint32_t &status,
+                               bool point_to_point = false) {
   if (ns == 0 || tgt.n == 0) {
     if (threadIdx.x == 0) {
       for (int k = 0; k < 16; ++k) out->transform[k] = sh.t[k];
@@ -289,15 +470,20 @@ __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView 
   bool valid = distance > 0.0;  // a NaN radius is not valid either
   double r2 = distance * distance;
   for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) hint_set(hint, i, -1);
-  icp_pass(src, ns, tgt, r2, valid, sh, hint, status);
+  icp_pass(src, ns, tgt, r2, valid, sh, hint, status, point_to_point);
   double fit, rmse;
   fit_rmse(sh.sums, ns, fit, rmse);
   uint32_t iterations = 0;
   bool converged = false;
   for (int it = 0; it < max_iter; ++it) {
-    if (threadIdx.x == 0) plane_step(sh, tgt.nrm != nullptr);
+    if (threadIdx.x == 0) {
+      if (point_to_point)
+        point_step(sh);
+      else
+        plane_step(sh, tgt.nrm != nullptr);
+    }
     __syncthreads();
-    icp_pass(src, ns, tgt, r2, valid, sh, hint, status);
+    icp_pass(src, ns, tgt, r2, valid, sh, hint, status, point_to_point);
     ++iterations;
     double nfit, nrmse;
     fit_rmse(sh.sums, ns, nfit, nrmse);

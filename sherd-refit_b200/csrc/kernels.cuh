@@ -277,7 +277,8 @@ __global__ void __launch_bounds__(ICP_BLOCK, 4) k_icp_rung(const double4 *src, u
   if (threadIdx.x < 16) sh.t[threadIdx.x] = inits[16 * blockIdx.x + threadIdx.x];
   __syncthreads();
   icp_rung_block(src, ns, tgt, opt.max_correspondence_distance, opt.max_iteration, sh,
-                 hints + size_t(ns) * blockIdx.x, out + blockIdx.x, st);
+                 hints + size_t(ns) * blockIdx.x, out + blockIdx.x, st,
+                 opt.estimation == SHERD_POINT_TO_POINT);
   if (st) atomicOr(status, st);
 }
 

@@ -1007,8 +1007,8 @@ int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source, cons
                    sherd_registration *out) {
   if (!ctx || !target || ((!inits || !out) && k) || (!source && n_source))
     return fail(ctx, SHERD_E_INVALID, "null argument");
-  if (options.estimation != SHERD_POINT_TO_PLANE)
-    return fail(ctx, SHERD_E_INVALID, "only the point-to-plane rung runs on the device");
+  if (options.estimation != SHERD_POINT_TO_PLANE && options.estimation != SHERD_POINT_TO_POINT)
+    return fail(ctx, SHERD_E_INVALID, "unknown estimation");
   if (options.max_iteration < 0) return fail(ctx, SHERD_E_INVALID, "negative iteration cap");
   for (uint32_t c = 0; c < k; ++c)
     if (!finite_pose(inits + 16 * size_t(c))) return fail(ctx, SHERD_E_INVALID, "init pose is not finite");
@@ -1042,8 +1042,8 @@ int sherd_icp_rung_noalloc(sherd_ctx *ctx, const double *source, uint32_t n_sour
                            sherd_icp_options options, sherd_registration *out) {
   if (!ctx || !target || ((!inits || !out) && k) || (!source && n_source))
     return fail(ctx, SHERD_E_INVALID, "null argument");
-  if (options.estimation != SHERD_POINT_TO_PLANE)
-    return fail(ctx, SHERD_E_INVALID, "only the point-to-plane rung runs on the device");
+  if (options.estimation != SHERD_POINT_TO_PLANE && options.estimation != SHERD_POINT_TO_POINT)
+    return fail(ctx, SHERD_E_INVALID, "unknown estimation");
   if (options.max_iteration < 0) return fail(ctx, SHERD_E_INVALID, "negative iteration cap");
   if (uint64_t(k) * n_source > SHERD_NOALLOC_CAPACITY)
     return fail(ctx, SHERD_E_INVALID,

@@ -345,3 +345,36 @@ def test_coarse_scores_are_bit_exact(sherd, gpu_ctx, oracle, slab):
     assert 0 < np.count_nonzero(mine) < len(mine)
     empty = gpu_ctx.coarse_scores(target, np.zeros((0, 3)), np.zeros((0, 3)), poses[:3], coarse)
     assert np.array_equal(empty, np.zeros(3))
+
+
+def test_point_to_point_rungs_match_the_oracle(sherd, gpu_ctx, oracle, slab):
+    """The stage-1 rung (point-to-point, umeyama) through Executor::icp_rung: B's breakline
+    subset against A's breakline from perturbed stage-1 poses, both R 5.4 rungs, against the
+    oracle; and the fixture's s1.T held in place by the last rung."""
+    a, b = piece(slab, "pieceA"), piece(slab, "pieceB")
+    t, icp = float(slab["scales"][0]), float(slab["scales"][11])
+    sub = b["brk_sub"].astype(np.int64)
+    src = b["brk_P"][sub]
+    rng = np.random.default_rng(11)
+    starts = slab["s1_T"][:40].copy()
+    starts[:, :3, 3] += rng.normal(size=(40, 3)) * 0.05 * t
+    target_g, target_c = gpu_ctx.cloud(a["brk_P"]), oracle.Cloud(a["brk_P"])
+    ex = sherd.CudaExecutor(gpu_ctx)
+    poses_g, poses_c = starts.reshape(-1, 16), starts.reshape(-1, 16)
+    for k in (0.2, 0.08):
+        batch = sherd.IcpBatch(src, target_g, poses_g, k * t * icp, 20, sherd._abi.POINT_TO_POINT)
+        regs_g = ex.icp_rung(batch)
+        regs_c = oracle.icp_rung(src, target_c, poses_c, k * t * icp, 20, point_to_point=True)
+        close = 0
+        for g, c in zip(regs_g, regs_c):
+            pg, pc = g.pose(), np.array(c.transform[:]).reshape(4, 4)
+            if origin_t(pg, pc, t) < 1e-6 and trace_deg(pg, pc) < 1e-4:
+                close += 1
+                assert g.correspondences == c.correspondences
+        assert close >= 0.9 * len(regs_g), close
+        poses_g = np.array([g.transform[:] for g in regs_g])
+        poses_c = np.array([c.transform[:] for c in regs_c])
+    held = gpu_ctx.icp_rung(src, target_g, slab["s1_T"], 0.08 * t * icp, 20,
+                            sherd._abi.POINT_TO_POINT)
+    for r, pose in zip(held, slab["s1_T"]):
+        assert trace_deg(r.pose(), pose) < 1e-3 and origin_t(r.pose(), pose, t) < 1e-6

@@ -180,3 +180,31 @@ def test_coarse_scores_reproduce_the_stage1_rescore(slab, oracle):
     got = oracle.coarse_scores(target, b["brk_P"][sub], b["brk_ns"][sub], slab["s1_T"],
                                float(slab["scales"][3]))
     assert np.array_equal(got, slab["s1_score"])
+
+
+def test_svd_rotation_matches_lapack(oracle):
+    """umeyama's rotation U diag(1, 1, det U det V) V^T (icp.rs:585-590) against numpy's SVD,
+    on full-rank, rank-2 and ill-conditioned matrices over twelve decades of scale."""
+    rng = np.random.default_rng(0)
+    for k in range(600):
+        m = rng.normal(size=(3, 3)) * 10 ** rng.uniform(-6, 6)
+        if k % 3 == 1:
+            m[:, 2] = m[:, 0] * 0.5 + m[:, 1]
+        elif k % 3 == 2:
+            m = m @ np.diag([1.0, 1e-9, 1.0])
+        u, _, vt = np.linalg.svd(m)
+        ref = u @ np.diag([1.0, 1.0, np.sign(np.linalg.det(u) * np.linalg.det(vt))]) @ vt
+        assert np.abs(oracle.svd_rotation(m) - ref).max() < 1e-11, k
+
+
+def test_the_stage1_rung_holds_the_fixture_poses(slab, oracle):
+    """R 5.4's last point-to-point rung (ladder.rs:131-141: 0.08 t icp, 20 iterations) started at
+    the reference's refined stage-1 poses s1.T leaves every one of them where it is."""
+    a, b = piece(slab, "pieceA"), piece(slab, "pieceB")
+    t, icp = float(slab["scales"][0]), float(slab["scales"][11])
+    sub = b["brk_sub"].astype(np.int64)
+    regs = oracle.icp_rung(b["brk_P"][sub], oracle.Cloud(a["brk_P"]), slab["s1_T"],
+                           0.08 * t * icp, 20, point_to_point=True)
+    for r, pose in zip(regs, slab["s1_T"]):
+        mine = np.array(r.transform[:]).reshape(4, 4)
+        assert trace_deg(mine, pose) < 1e-3 and origin_t(mine, pose, t) < 1e-6
