@@ -201,6 +201,12 @@ int sherd_bounded_distance(sherd_ctx *ctx, const sherd_mesh *mesh,
 int sherd_inside(sherd_ctx *ctx, const sherd_mesh *mesh, const double *points,
                  uint32_t n, const double pose[16], sherd_inside_outcome *out);
 
+/* verify::penetration_share (verify.rs:509-527), R 8's assembly question:
+ * the share of the n points, moved by `pose`, that the parity test calls
+ * inside `mesh` with a depth above `pen` (0 for n == 0). */
+int sherd_penetration_share(sherd_ctx *ctx, const sherd_mesh *mesh, const double *points,
+                            uint32_t n, const double pose[16], double pen, double *share);
+
 /* ---- preprocessing rays: the cone_cast extension ----------------------- */
 
 /* mesh::geometry::face_geometry (mesh/geometry.rs:70-96) in f64 on the

@@ -151,6 +151,7 @@ def lib() -> C.CDLL:
         "or_coarse_scores": (None, [vp, F64P, F64P, C.c_uint32, F64P, C.c_uint32, C.c_double,
                                     C.c_double, F64P]),
         "or_svd_rotation": (None, [F64P, F64P]),
+        "or_penetration_share": (C.c_double, [vp, F64P, C.c_uint32, F64P, C.c_double]),
         "or_segment": (None, [vp, F64P, U32P, C.c_uint32, C.c_double, C.c_double,
                               C.POINTER(SegParams), vp, U8P, C.POINTER(SegInfo),
                               C.POINTER(SegTrace)]),
@@ -343,6 +344,12 @@ def coarse_scores(target: Cloud, points, normals, poses, radius, normal_agree=0.
     lib().or_coarse_scores(target.h, p, n, len(p), t, len(t), float(radius), float(normal_agree),
                            out)
     return out
+
+
+def penetration_share(mesh: Mesh, points, pose, pen):
+    """verify::penetration_share (verify.rs:509-527)."""
+    p = f64(points).reshape(-1, 3)
+    return lib().or_penetration_share(mesh.h, p, len(p), f64(pose).reshape(16), float(pen))
 
 
 def svd_rotation(m):

@@ -2153,4 +2153,16 @@ void or_svd_rotation(const double *m9, double *r9) {
   for (int i = 0; i < 9; ++i) r9[i] = r[i / 3][i % 3];
 }
 
+// verify::penetration_share (verify.rs:509-527).
+double or_penetration_share(const void *mesh, const double *points, uint32_t n, const double *pose,
+                            double pen) {
+  if (n == 0) return 0.0;
+  std::vector<sherd_inside_outcome> out(n);
+  inside_batch(*static_cast<const Mesh *>(mesh), points, n, pose, out.data());
+  size_t deeper = 0;
+  for (const auto &o : out)
+    if (o.inside && double(o.depth) > pen) ++deeper;
+  return double(deeper) / double(n);
+}
+
 }  // extern "C"

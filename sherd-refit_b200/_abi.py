@@ -176,6 +176,8 @@ _SIGNATURES = {
     "sherd_batch_free": (C.c_int, [VP]),
     "sherd_adjoint": (C.c_int, [VP, VP, C.c_uint32, F64P, F64P, C.c_uint32,
                                 C.POINTER(AdjointOptions), F64P, F64P]),
+    "sherd_penetration_share": (C.c_int, [VP, VP, F64P, C.c_uint32, F64P, C.c_double,
+                                          C.POINTER(C.c_double)]),
     "sherd_coarse_scores": (C.c_int, [VP, VP, F64P, F64P, C.c_uint32, F64P, C.c_uint32,
                                       C.c_double, C.c_double, F64P]),
     "sherd_seg_params_default": (None, [C.POINTER(SegParams)]),

@@ -236,6 +236,15 @@ class Context:
                                                        C.cast(out, C.c_void_p)))
         return out
 
+    def penetration_share(self, mesh: "Mesh", points, pose, pen) -> float:
+        """verify::penetration_share (verify.rs:509-527), R 8's assembly question: the share
+        of `points` moved by `pose` inside `mesh` deeper than `pen`."""
+        p = _f64(points)
+        out = C.c_double(0.0)
+        check(self.h, A.lib().sherd_penetration_share(self.h, mesh.h, p, len(p), _pose(pose),
+                                                      float(pen), C.byref(out)))
+        return out.value
+
     # -- the coarse breakline score -----------------------------------------------------------
     def coarse_scores(self, target: "Cloud", points, normals, poses, radius, normal_agree=0.7):
         """Executor::coarse_scores (executor/cpu.rs:46-68, 136-169): per 4x4 pose the fraction

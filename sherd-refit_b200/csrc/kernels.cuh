@@ -315,6 +315,31 @@ __global__ void k_coarse_scores(CloudView tgt, const double *pts, const double *
   if (st) atomicOr(status, st);
 }
 
+// verify::penetration_share (verify.rs:509-527): points inside the mesh and
+// deeper than `pen`, counted per warp by ballot.
+__global__ void k_penetration_share(MeshView m, const double *pts, uint32_t n, Pose16 pose,
+                                    double pen, unsigned long long *count, uint32_t *status) {
+  uint32_t st = 0;
+  unsigned long long mine = 0;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    bool deeper = false;
+    if (i < n) {
+      double x, y, z;
+      apply_pose(pose.m, pts[3 * size_t(i)], pts[3 * size_t(i) + 1], pts[3 * size_t(i) + 2], x, y, z);
+      F3 p = {float(x), float(y), float(z)};
+      bool in_box = !(p.x < m.lo[0] || p.x > m.hi[0] || p.y < m.lo[1] || p.y > m.hi[1] ||
+                      p.z < m.lo[2] || p.z > m.hi[2]);
+      if (in_box && inside_mesh(m, p, st))
+        deeper = double(mesh_distance(m, p, f_inf(), st)) > pen;
+    }
+    unsigned ballot = __ballot_sync(0xFFFFFFFFu, deeper);
+    if ((threadIdx.x & 31) == 0) mine += __popc(ballot);
+  }
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(count, mine);
+  if (st) atomicOr(status, st);
+}
+
 // ---- the batched stage-2 path ----------------------------------------------------
 
 // Resident ladder CTAs per SM the register budget is cut for (65536 / (ICP_BLOCK * this)

@@ -741,6 +741,33 @@ int sherd_inside(sherd_ctx *ctx, const sherd_mesh *mesh, const double *points, u
   return finish(ctx, "inside", n, true);
 }
 
+int sherd_penetration_share(sherd_ctx *ctx, const sherd_mesh *mesh, const double *points,
+                            uint32_t n, const double pose[16], double pen, double *share) {
+  if (!ctx || !mesh || !share || (!points && n)) return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (!finite_pose(pose)) return fail(ctx, SHERD_E_INVALID, "pose is not finite");
+  *share = 0.0;
+  if (n == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  DBuf<double> p;
+  DBuf<unsigned long long> cnt;
+  if ((rc = upload(ctx, p, points, size_t(3) * n))) return rc;
+  CK(cnt.alloc(1));
+  CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), ctx->stream));
+  unsigned grid = std::min(blocks_for(n, 128), unsigned(ctx->sm_count) * 16u);
+  // Whole warps: the kernel's ballot needs every lane of a warp in the loop.
+  k_penetration_share<<<grid, 128, 0, ctx->stream>>>(mesh->view, p.p, n, pose_of(pose), pen, cnt.p,
+                                                     ctx->d_status);
+  CK(cudaGetLastError());
+  unsigned long long deeper = 0;
+  CK(cudaMemcpyAsync(&deeper, cnt.p, sizeof deeper, cudaMemcpyDeviceToHost, ctx->stream));
+  rc = finish(ctx, "penetration_share", n, true);
+  if (rc) return rc;
+  *share = double(deeper) / double(n);
+  return SHERD_OK;
+}
+
 // ---- preprocessing rays ------------------------------------------------------
 
 int sherd_face_geometry(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f, uint32_t nf,

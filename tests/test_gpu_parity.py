@@ -378,3 +378,22 @@ def test_point_to_point_rungs_match_the_oracle(sherd, gpu_ctx, oracle, slab):
                             sherd._abi.POINT_TO_POINT)
     for r, pose in zip(held, slab["s1_T"]):
         assert trace_deg(r.pose(), pose) < 1e-3 and origin_t(r.pose(), pose, t) < 1e-6
+
+
+def test_penetration_share_matches_verify_and_the_oracle(sherd, gpu_ctx, gpu_slab, cpu_slab,
+                                                         oracle, slab):
+    """verify::penetration_share (verify.rs:509-527) in each direction: equal to the oracle's,
+    and the larger of the two is R 6's pen for the same pose."""
+    sc = gpu_slab["scales"]
+    a, b = gpu_slab["a"], gpu_slab["b"]
+    for k in range(len(slab["s2_T_frac2"])):
+        t = slab["s2_T_frac2"][k]
+        ti = np.linalg.inv(t)
+        share_b = gpu_ctx.penetration_share(a["mesh"], b["arrays"]["S"], t, sc.pen)
+        share_a = gpu_ctx.penetration_share(b["mesh"], a["arrays"]["S"], ti, sc.pen)
+        cb = oracle.penetration_share(cpu_slab["a"]["mesh"], b["arrays"]["S"], t, sc.pen)
+        ca = oracle.penetration_share(cpu_slab["b"]["mesh"], a["arrays"]["S"], ti, sc.pen)
+        assert (share_a, share_b) == (ca, cb)
+        s = gpu_ctx.verify(a["surf"], b["surf"], t, sc)
+        assert max(share_a, share_b) == s.pen
+    assert gpu_ctx.penetration_share(a["mesh"], np.zeros((0, 3)), np.eye(4), sc.pen) == 0.0
