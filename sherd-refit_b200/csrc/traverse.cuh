@@ -113,7 +113,9 @@ __device__ __noinline__ void first_hit(const MeshView &m, F3 o, F3 d, float &bes
     int next = -1;
     for (int q = 0; q < 2; ++q) {
       int c = q == 0 ? near_c : 1 - near_c;
-      if (!(te[c] <= bound())) continue;
+      // A box the ray misses enters at +inf, which the bound (+inf until the
+      // first hit) would otherwise let through.
+      if (te[c] == f_inf() || !(te[c] <= bound())) continue;
       if (n.cnt[c]) {
         leaf(n.ref[c], n.cnt[c]);
       } else if (next < 0) {

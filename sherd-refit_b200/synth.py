@@ -611,7 +611,8 @@ def slab_collection(seed=0, t=10.0, edges_per_t=7.0, n_starts=16, noise_amp=0.3)
 CONFIGS = {
     # 1 slab, 2 pot (8 fragments, 28 pairs x 64 starts), 3 collection
     # (40 fragments of 3 pots, t = 5, 8, 12; 780 pairs x 128 starts; 1k-60k fracture points),
-    # 5 thin pot (t = 2 at 4-6 edges per t, 6 fragments of about 1M faces).
+    # 5 thin pot (t = 2 at 4-6 edges per t, 6 fragments of about 1M faces, 500k surface
+    # samples per fragment: 1M penetration samples per pair).
     # The ring meshing spends about twice the faces of an isotropic mesh at the same edge
     # length, so the edge lengths are set to land on each config's stated face counts.
     "slab": lambda seed=0: slab_collection(seed, edges_per_t=7.0),
@@ -621,7 +622,8 @@ CONFIGS = {
         seed, walls=(5.0, 8.0, 12.0), cells_per_wall=(14, 13, 13), edges_per_t=(6.5, 9.5),
         n_starts=128, frac_per_t2=(900.0, 300.0, 60.0), frac_range=(1000, 60000), name="coll"),
     "thin": lambda seed=0: pot_collection(seed, walls=(2.0,), cells_per_wall=(6,),
-                                          edges_per_t=(4.0, 5.0), n_starts=128, name="thin"),
+                                          edges_per_t=(4.0, 5.0), n_starts=128,
+                                          surface_points=500_000, name="thin"),
 }
 
 
