@@ -14,7 +14,9 @@ the clocks seen during the timed region and the oracle's CPU baseline on a bound
 `--impl reference` times the reference algorithm's CPU restatement (the oracle; the Rust
 reference cannot be built here) on all host cores instead. `--config group` measures the
 differentiation workload instead (sherd_adjoint over 4096 perturbed poses of an assembled
-8-fragment pot, and a 50-evaluation joint refinement).
+8-fragment pot, and a 50-evaluation joint refinement). `--config refine` measures R 9, the
+full-resolution join refinement of one assembled pot (fracture clouds and the spanning walk of
+two-rung ICP joins).
 """
 
 from __future__ import annotations
@@ -252,6 +254,148 @@ def run_group(args):
     ctx.close()
 
 
+def _edge_errors(poses, truth, edges, t):
+    """Mean rotation (deg) and translation (in t) of the relative poses over the joins."""
+    rot, disp = [], []
+    for a, b in edges:
+        mine = np.linalg.inv(poses[a]) @ poses[b]
+        want = np.linalg.inv(truth[a]) @ truth[b]
+        r = mine[:3, :3].T @ want[:3, :3]
+        rot.append(np.degrees(np.arccos(np.clip((np.trace(r) - 1.0) / 2.0, -1.0, 1.0))))
+        disp.append(np.linalg.norm(mine[:3, 3] - want[:3, 3]) / t[b])
+    return float(np.mean(rot)), float(np.mean(disp))
+
+
+def run_refine(args):
+    """R 9 on one assembled pot: every adjacent pair a join (in pair order), every fragment pose
+    perturbed by 0.1 deg about its fracture centroid and 0.02 t (the assembly's poses are right
+    to a fraction of the first rung's 0.05 t radius; larger errors are outside what R 9 can
+    capture). One step is the whole stage: each fragment's fracture cloud (vertex normals and
+    the vertex selection on the device, from the original mesh) and the spanning walk of
+    sherd_refine_join calls (two 40-iteration rungs per join)."""
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    sherd = _pkg()
+    synth = _pkg("synth")
+    workload = _pkg("workload")
+    refine = _pkg("refine")
+    t_gen = time.perf_counter()
+    wl = synth.make(args.refine_workload, args.seed)
+    t_gen = time.perf_counter() - t_gen
+    ctx = sherd.Context(local)
+    frags = wl.fragments
+    meshes = [(fr.v.astype(np.float64), fr.f) for fr in frags]
+    cents = [ctx.face_geometry(v, f)[2] for v, f in meshes]
+    used = [(p.a, p.b) for p in wl.pairs if p.adjacent]
+    groups = [list(range(len(frags)))]
+    truth, w0 = workload.perturbed_group_poses(wl, 1, seed=args.seed + 1, rot_deg=0.1,
+                                               trans_t=0.02)
+    poses = list(w0[0])
+    thick = np.array([fr.t for fr in frags])
+
+    def step():
+        t0 = time.perf_counter()
+        pieces = [refine.RefinePiece(fr.t, fr.res, refine.fracture_cloud(
+            ctx, v, f, c, fr.frac, fr.t, fr.res)) for fr, (v, f), c in zip(frags, meshes, cents)]
+        t1 = time.perf_counter()
+        out = refine.refine_joins(ctx, pieces, poses, groups, used)
+        t2 = time.perf_counter()
+        return pieces, out, t1 - t0, t2 - t1
+
+    for _ in range(args.warmup):
+        step()
+    stats0 = ctx.stats()["methods"]
+    sampler = ClockSampler(local)
+    sampler.start()
+    runs = [step() for _ in range(args.steps)]
+    clocks = sampler.stop()
+    stats1 = ctx.stats()["methods"]
+    device_ms = {k: {"ms_per_step": (v["ms"] - stats0.get(k, {}).get("ms", 0.0)) / args.steps,
+                     "calls_per_step": (v["calls"] - stats0.get(k, {}).get("calls", 0)) / args.steps,
+                     "items_per_step": (v["items"] - stats0.get(k, {}).get("items", 0)) / args.steps}
+                 for k, v in stats1.items()
+                 if v["calls"] > stats0.get(k, {}).get("calls", 0)}
+    pieces, out, _, _ = runs[-1]
+    t_clouds = float(np.mean([r[2] for r in runs]))
+    t_walk = float(np.mean([r[3] for r in runs]))
+    n_joins = len(out.joins)
+    point_passes = sum(len(pieces[j.moving].cloud) * (r.iterations + 1)
+                       for j in out.joins for r in j.registrations)
+    walked = [(j.fixed, j.moving) for j in out.joins]
+    before = _edge_errors(poses, truth, walked, thick)
+    after = _edge_errors(out.poses, truth, walked, thick)
+    cpu = None
+    if not args.no_cpu:
+        oracle = importlib.import_module("oracle")
+        first = out.joins[0]
+        o_pieces = []
+        t0 = time.perf_counter()
+        for k in (first.fixed, first.moving):
+            v, f = meshes[k]
+            nrm = oracle.vertex_normals(v, f)
+            o_pieces.append(oracle.cloud_from_indices(v, nrm, oracle.cap_selection(
+                oracle.select_candidates(v, cents[k], frags[k].frac, frags[k].t, frags[k].res))))
+        t_cloud_cpu = (time.perf_counter() - t0) / 2
+        op = [None] * len(frags)
+        op[first.fixed] = oracle.RefinePiece(frags[first.fixed].t, frags[first.fixed].res,
+                                             o_pieces[0])
+        op[first.moving] = oracle.RefinePiece(frags[first.moving].t, frags[first.moving].res,
+                                              o_pieces[1])
+        t0 = time.perf_counter()
+        oj = oracle.refine_one(op, poses, first.fixed, first.moving, oracle.default_params())
+        t_join_cpu = time.perf_counter() - t0
+        assert oj.dist == first.dist
+        vs = []
+        for mine, theirs in zip(first.rungs, oj.rungs):
+            r = mine[:3, :3].T @ theirs[:3, :3]
+            vs.append([float(np.degrees(np.arccos(np.clip((np.trace(r) - 1) / 2, -1, 1)))),
+                       float(np.linalg.norm(mine[:3, 3] - theirs[:3, 3]) / frags[first.moving].t)])
+        cpu_stage = len(frags) * t_cloud_cpu + n_joins * t_join_cpu
+        cpu = {"value": n_joins / cpu_stage, "unit": "joins/s",
+               "cores": oracle.lib().or_default_threads(), "kind": "port",
+               "sample": (f"the oracle on the walk's first join ({len(o_pieces[1].points)} source, "
+                          f"{len(o_pieces[0].points)} target points; {t_join_cpu:.2f} s, one "
+                          f"thread: one pose) and its two fragments' clouds ({t_cloud_cpu:.2f} s "
+                          f"each, all threads), scaled to {len(frags)} clouds and {n_joins} joins"),
+               "join_s": t_join_cpu, "cloud_s": t_cloud_cpu,
+               "first_join_device_vs_oracle": {"rung_rot_deg_trans_t": vs,
+                                               "fitness": [first.fitness, oj.fitness]}}
+    line = {
+        "metric": "refined joins/s (R 9 stage)", "value": n_joins / (t_clouds + t_walk),
+        "unit": "joins/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * (t_clouds + t_walk), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": (f"{args.refine_workload}: {len(frags)} fragments "
+                                f"({sum(len(f) for _, f in meshes)} faces), one group, "
+                                f"{len(used)} joins in used order, poses perturbed 0.1 deg / 0.02 t"),
+                   "cloud_points": [len(p.cloud) for p in pieces],
+                   "timer": "host wall clock around the synchronous C-ABI calls (meshes and "
+                            "clouds in from host memory, normals, indices and poses out)",
+                   "generate_s": round(t_gen, 1)},
+        "clouds_ms": 1000 * t_clouds, "walk_ms": 1000 * t_walk,
+        "walk_joins_per_s": n_joins / t_walk,
+        "point_passes_per_s": point_passes / t_walk,
+        "iterations": [[r.iterations for r in j.registrations] for j in out.joins],
+        "device_ms": device_ms,
+        "perturbation": "0.1 deg about the fracture centroid and 0.02 t per fragment",
+        "edge_error_before": {"rot_deg": before[0], "disp_t": before[1]},
+        "edge_error_after": {"rot_deg": after[0], "disp_t": after[1]},
+        "gpu_launches": int(args.steps * (device_ms.get("refine_join_rungs", {}).get(
+            "items_per_step", 0) + 5 * n_joins + 3 * len(frags))),
+        "gpu_launches_counts": ("k_wide_pass (one per pass), k_wide_reset and k_place_fused "
+                                "(5 per join), k_incidence, k_vertex_normals and k_nn_below (3 per "
+                                "fragment); the LBVH builds' and the radix sorts' own launches "
+                                "are not counted"),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def _config_dict(wl, args, extra=None):
     d = wl.describe()
     cfg = {"workload": f"{args.config}: {d['fragments']} fragments, {d['pairs']} pairs x "
@@ -278,12 +422,16 @@ def main():
     ap.add_argument("--reference-items", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--group-poses", type=int, default=4096)
+    ap.add_argument("--refine-workload", default="scan")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
         return
     if args.config == "group":
         run_group(args)
+        return
+    if args.config == "refine":
+        run_refine(args)
         return
 
     import torch

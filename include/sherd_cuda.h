@@ -469,6 +469,34 @@ int sherd_adjoint(sherd_ctx *ctx, sherd_pair *const *edges, uint32_t n_edges,
                   const double *poses, const double *inverses, uint32_t n_poses,
                   const sherd_adjoint_options *opt, double *values, double *grads);
 
+/* ---- R 9: full-resolution join refinement (refine.rs) ------------------- */
+
+/* refine::vertex_normals (refine.rs:121-151), Open3D's ComputeVertexNormals:
+ * every face's unnormalised normal (v1 - v0) x (v2 - v0) added to its three
+ * vertices, each vertex's sum taken in ascending face order, then one
+ * normalisation; a vertex whose sum is zero (or not a number) gets (0, 0, 1).
+ * Bit-identical to the reference's sequential loop. `normals` receives nv
+ * f64 triples. 3 * nf must stay below 2^31. */
+int sherd_vertex_normals(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f,
+                         uint32_t nf, double *normals);
+
+/* refine::refine_one (refine.rs:334-386) for one join: the moving fragment's
+ * cloud `source` (n_source points) placed by pose_moving, the fixed one's
+ * `target` and `target_normals` (n_target) placed by pose_fixed, both as
+ * types::apply_transform_fused / rotate_fused place them (types.rs:202-214,
+ * bit-identical); then two point-to-plane registration_icp rungs from the
+ * identity, at distances dist[0] and dist[1], max_iteration each, the second
+ * starting from the first's pose. out[0], out[1] receive the two rungs
+ * (transform = the correction in the fixed fragment's world frame; the caller
+ * applies out[1].transform to pose_moving). Each pass is spread over the
+ * whole device, a slice of the source per block, its sums added in block
+ * order (reproducible run to run). An empty cloud on either side leaves both
+ * rungs at the identity with no correspondence. */
+int sherd_refine_join(sherd_ctx *ctx, const double *source, uint32_t n_source,
+                      const double *target, const double *target_normals, uint32_t n_target,
+                      const double pose_fixed[16], const double pose_moving[16],
+                      const double dist[2], int32_t max_iteration, sherd_registration out[2]);
+
 #ifdef __cplusplus
 }
 #endif

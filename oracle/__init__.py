@@ -155,6 +155,8 @@ def lib() -> C.CDLL:
         "or_segment": (None, [vp, F64P, U32P, C.c_uint32, C.c_double, C.c_double,
                               C.POINTER(SegParams), vp, U8P, C.POINTER(SegInfo),
                               C.POINTER(SegTrace)]),
+        "or_vertex_normals": (None, [F64P, C.c_uint32, U32P, C.c_uint32, F64P]),
+        "or_place_fused": (None, [F64P, C.c_uint32, F64P, C.c_int, F64P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -528,3 +530,155 @@ def ladder_verify_items(pairs, items, params: Params, threads=0):
     used = lib().or_ladder_verify_batch(arr, len(pairs), C.cast(items, C.c_void_p), len(items),
                                         C.byref(params), threads, C.cast(out, C.c_void_p))
     return out, used
+
+
+# ---- R 9: full-resolution join refinement (refine.rs) ------------------------------------------
+
+REFINE_MAX_POINTS = 150_000   # refine.rs:56
+REFINE_CAP_SEED = 0           # refine.rs:64
+REFINE_SELECT_T = 0.15        # refine.rs:66
+REFINE_SELECT_RES = 1.5       # refine.rs:68
+REFINE_RUNGS = (0.05, 0.02)   # refine.rs:70
+REFINE_ITERATIONS = 40        # refine.rs:72
+MISS = 0xFFFFFFFF
+
+
+def vertex_normals(v, f):
+    """refine::vertex_normals (refine.rs:121-151): face-order sums of the unnormalised face
+    normals, normalised once, (0, 0, 1) where the sum is zero."""
+    v = f64(v).reshape(-1, 3)
+    f = u32(f).reshape(-1, 3)
+    out = np.empty_like(v)
+    lib().or_vertex_normals(v, len(v), f, len(f), out)
+    return out
+
+
+def place_fused(points, pose, rotate_only=False):
+    """types::apply_transform_fused / rotate_fused (types.rs:202-214), row-major pose."""
+    p = f64(points).reshape(-1, 3)
+    out = np.empty_like(p)
+    lib().or_place_fused(p, len(p), f64(pose).reshape(16), int(bool(rotate_only)), out)
+    return out
+
+
+def refine_radius(thick, res):
+    """The acceptance radius of select_candidates (refine.rs:168)."""
+    return max(REFINE_SELECT_T * float(thick), REFINE_SELECT_RES * float(res))
+
+
+def select_candidates(v, centroids, fracture, thick, res):
+    """refine::select_candidates (refine.rs:161-178): every vertex whose nearest working-mesh
+    centroid is a fracture face at a distance below max(0.15 t, 1.5 res), ascending. The bounded
+    search (kdtree.rs:182-190) finds the unbounded nearest whenever it passes that test."""
+    v = f64(v).reshape(-1, 3)
+    centroids = f64(centroids).reshape(-1, 3)
+    if len(centroids) == 0 or len(v) == 0:
+        return np.zeros(0, np.uint32)
+    j, _ = Cloud(centroids).nearest_below(v, refine_radius(thick, res))
+    frac = np.asarray(fracture).astype(bool)
+    keep = j != MISS
+    keep[keep] = frac[j[keep]]
+    return np.nonzero(keep)[0].astype(np.uint32)
+
+
+def cap_selection(idx, max_points=REFINE_MAX_POINTS, seed=REFINE_CAP_SEED):
+    """refine::cap_selection (refine.rs:186-193). Above the cap this draws numpy's
+    default_rng(seed).choice(idx, max_points, replace=False), the draw refine.rs:30-37 names;
+    under it the selection comes back untouched."""
+    idx = np.asarray(idx, np.uint32)
+    if len(idx) > max_points:
+        idx = np.random.default_rng(seed).choice(idx, max_points, replace=False).astype(np.uint32)
+    return idx
+
+
+class FractureCloud:
+    """refine::FractureCloud (refine.rs:78-113): indices, points and normals in ICP order."""
+
+    def __init__(self, idx, points, normals):
+        self.idx = np.asarray(idx, np.uint32)
+        self.points = f64(points).reshape(-1, 3)
+        self.normals = f64(normals).reshape(-1, 3)
+
+
+def cloud_from_indices(v, normals, idx):
+    """refine::cloud_from_indices (refine.rs:208-214)."""
+    idx = np.asarray(idx, np.int64)
+    return FractureCloud(idx, f64(v).reshape(-1, 3)[idx], f64(normals).reshape(-1, 3)[idx])
+
+
+class RefinePiece:
+    """refine::RefinePiece (refine.rs:236-244): the fragment's thickness and res, and its cloud
+    (None when it has none)."""
+
+    def __init__(self, thick, res, cloud):
+        self.thick, self.res, self.cloud = float(thick), float(res), cloud
+
+
+class RefinedJoin:
+    """refine::RefinedJoin (refine.rs:247-262)."""
+
+    def __init__(self, fixed, moving, dist, rungs, fitness, rmse_t):
+        self.fixed, self.moving = int(fixed), int(moving)
+        self.dist, self.rungs = list(dist), [np.asarray(r, np.float64) for r in rungs]
+        self.fitness, self.rmse_t = float(fitness), float(rmse_t)
+
+
+def matmul4(a, b):
+    """A 4x4 product summed k = 0..3 left to right, without fused multiply-adds."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return ((a[:, 0:1] * b[0] + a[:, 1:2] * b[1]) + a[:, 2:3] * b[2]) + a[:, 3:4] * b[3]
+
+
+def refine_one(pieces, poses, fixed, moving, params: Params):
+    """refine::refine_one (refine.rs:334-386): the moving cloud placed by its pose against the
+    fixed one placed by its own (normals rotated), two point-to-plane rungs from the identity."""
+    tp, sp = pieces[fixed], pieces[moving]
+    if tp.cloud is None or sp.cloud is None:
+        return None
+    sc = scales_for(params, min(tp.thick, sp.thick), max(tp.res, sp.res))
+    source = place_fused(sp.cloud.points, poses[moving])
+    tpts = place_fused(tp.cloud.points, poses[fixed])
+    tnrm = place_fused(tp.cloud.normals, poses[fixed], rotate_only=True)
+    target = Cloud(tpts, tnrm) if len(tpts) and len(source) else None
+    pose = np.eye(4)
+    rungs, dist, last = [], [], None
+    for k in REFINE_RUNGS:
+        d = k * sc.t * sc.icp
+        if target is None:   # an empty side: the rung keeps its start, with no correspondence
+            last = Registration(transform=(C.c_double * 16)(*pose.reshape(16)))
+        else:
+            last = icp_rung(source, target, pose, d, REFINE_ITERATIONS)[0]
+        pose = np.array(last.transform[:]).reshape(4, 4)
+        rungs.append(pose)
+        dist.append(d)
+    return RefinedJoin(fixed, moving, dist, rungs, last.fitness, last.inlier_rmse / sc.t)
+
+
+def refine_joins(pieces, poses, groups, used, params: Params | None = None, one=None):
+    """refine::refine_joins (refine.rs:282-318): per group of two or more, starting from its first
+    fragment, repeatedly the first join of `used` (in `used` order) with exactly one endpoint
+    placed; the placed end is fixed and poses[moving] <- rung2 . poses[moving]. Returns
+    (poses, joins). `one` replaces refine_one (same signature)."""
+    params = params or default_params()
+    one = one or refine_one
+    out = [np.asarray(p, np.float64).reshape(4, 4).copy() for p in poses]
+    joins = []
+    for group in groups:
+        if len(group) < 2:
+            continue
+        done = [group[0]]
+        members = set(group)
+        edges = [(a, b) for a, b in used if a in members and b in members]
+        while True:
+            step = next((i for i, (a, b) in enumerate(edges) if (a in done) != (b in done)), None)
+            if step is None:
+                break
+            a, b = edges.pop(step)
+            fixed, moving = (a, b) if a in done else (b, a)
+            join = one(pieces, out, fixed, moving, params)
+            if join is not None:
+                out[moving] = matmul4(join.rungs[1], out[moving])
+                joins.append(join)
+            done.append(moving)
+    return out, joins

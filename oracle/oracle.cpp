@@ -2165,4 +2165,50 @@ double or_penetration_share(const void *mesh, const double *points, uint32_t n, 
   return double(deeper) / double(n);
 }
 
+// refine::vertex_normals (refine.rs:121-151), Open3D's ComputeVertexNormals:
+// each face's unnormalised normal (v1 - v0) x (v2 - v0) added to its three
+// vertices in face order, then one normalisation; a zero (or NaN) sum becomes
+// (0, 0, 1).
+void or_vertex_normals(const double *v, uint32_t nv, const uint32_t *f, uint32_t nf,
+                       double *out) {
+  std::fill(out, out + 3 * size_t(nv), 0.0);
+  for (uint32_t i = 0; i < nf; ++i) {
+    const uint32_t *tri = f + 3 * size_t(i);
+    const double *o = v + 3 * size_t(tri[0]), *b = v + 3 * size_t(tri[1]),
+                 *c = v + 3 * size_t(tri[2]);
+    double e1[3] = {b[0] - o[0], b[1] - o[1], b[2] - o[2]};
+    double e2[3] = {c[0] - o[0], c[1] - o[1], c[2] - o[2]};
+    double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                   e1[0] * e2[1] - e1[1] * e2[0]};
+    for (int k = 0; k < 3; ++k) {
+      double *s = out + 3 * size_t(tri[k]);
+      for (int a = 0; a < 3; ++a) s[a] += n[a];
+    }
+  }
+  for (uint32_t j = 0; j < nv; ++j) {
+    double *n = out + 3 * size_t(j);
+    double len = std::sqrt((n[0] * n[0] + n[1] * n[1]) + n[2] * n[2]);
+    if (len > 0.0) {
+      for (int a = 0; a < 3; ++a) n[a] /= len;
+    } else {
+      n[0] = 0.0;
+      n[1] = 0.0;
+      n[2] = 1.0;
+    }
+  }
+}
+
+// types::apply_transform_fused / rotate_fused (types.rs:202-214): row i of the
+// row-major pose is fma(t_i2, p2, fma(t_i1, p1, t_i0 p0)), plus t_i3 for a
+// point (rotate_only = 0); a normal takes the rotation block alone.
+void or_place_fused(const double *pts, uint32_t n, const double *t, int rotate_only, double *out) {
+  for (uint32_t i = 0; i < n; ++i) {
+    const double *p = pts + 3 * size_t(i);
+    for (int r = 0; r < 3; ++r) {
+      double s = std::fma(t[4 * r + 2], p[2], std::fma(t[4 * r + 1], p[1], t[4 * r] * p[0]));
+      out[3 * size_t(i) + r] = rotate_only ? s : s + t[4 * r + 3];
+    }
+  }
+}
+
 }  // extern "C"

@@ -184,6 +184,9 @@ _SIGNATURES = {
     "sherd_segment": (C.c_int, [VP, VP, F64P, C.c_uint32, U32P, C.c_uint32, C.c_double,
                                 C.c_double, C.POINTER(SegParams), U8P, C.POINTER(SegInfo),
                                 C.POINTER(SegTrace)]),
+    "sherd_vertex_normals": (C.c_int, [VP, F64P, C.c_uint32, U32P, C.c_uint32, F64P]),
+    "sherd_refine_join": (C.c_int, [VP, F64P, C.c_uint32, F64P, F64P, C.c_uint32, F64P, F64P,
+                                    F64P, C.c_int32, VP]),
 }
 
 

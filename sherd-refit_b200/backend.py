@@ -305,6 +305,29 @@ class Context:
                                             values, grads))
         return values, grads
 
+    # -- R 9 join refinement ----------------------------------------------------------------------
+    def vertex_normals(self, v, f):
+        """refine::vertex_normals (refine.rs:121-151), bit-identical: (nv, 3) f64."""
+        v, f = _f64(v), _u32(f, (-1, 3))
+        out = np.empty((len(v), 3))
+        check(self.h, A.lib().sherd_vertex_normals(self.h, v, len(v), f, len(f), out))
+        return out
+
+    def refine_join(self, source, target, target_normals, pose_fixed, pose_moving, dist,
+                    max_iteration=40):
+        """refine_one's two point-to-plane rungs (refine.rs:334-386) for one join, the clouds
+        placed by their fragments' poses on the device: [rung 1, rung 2] Registrations."""
+        s = _f64(source)
+        t, n = _f64(target), _f64(target_normals)
+        if t.shape != n.shape:
+            raise A.SherdError(A.E_INVALID, "target points and normals differ in shape")
+        d = np.ascontiguousarray(dist, np.float64).reshape(2)
+        out = (A.Registration * 2)()
+        check(self.h, A.lib().sherd_refine_join(self.h, s, len(s), t, n, len(t), _pose(pose_fixed),
+                                                _pose(pose_moving), d, int(max_iteration),
+                                                C.cast(out, C.c_void_p)))
+        return list(out)
+
 
 WORK_ITEM = np.dtype(A.WorkItem)
 CANDIDATE = np.dtype(A.Candidate)

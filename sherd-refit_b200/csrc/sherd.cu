@@ -15,6 +15,7 @@
 #include <array>
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -26,6 +27,7 @@
 #include "kernels.cuh"
 #include "adjoint.cuh"
 #include "segment.cuh"
+#include "refine.cuh"
 
 using namespace sherd;
 
@@ -2041,6 +2043,182 @@ int sherd_segment(sherd_ctx *ctx, const sherd_mesh *mesh, const double *v, uint3
   rc = finish(ctx, "segment", nf, true);
   if (rc) return rc;
   if (info) *info = inf;
+  return SHERD_OK;
+}
+
+
+// ---- R 9: full-resolution join refinement (refine.rs) -------------------------
+
+int sherd_vertex_normals(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f,
+                         uint32_t nf, double *normals) {
+  if (!ctx || ((!v || !normals) && nv) || (!f && nf)) return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (uint64_t(nf) * 3u >= (uint64_t(1) << 31)) return fail(ctx, SHERD_E_INVALID, "too many faces");
+  for (size_t i = 0; i < size_t(3) * nf; ++i)
+    if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
+  if (nv == 0) return SHERD_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  const uint32_t nc = 3u * nf;
+  DBuf<double> dv, dn;
+  DBuf<uint32_t> df, key, key2, face, face2;
+  if ((rc = upload(ctx, dv, v, size_t(3) * nv)) || (rc = upload(ctx, df, f, size_t(nc)))) return rc;
+  CK(dn.alloc(size_t(3) * nv));
+  if (nc) {
+    CK(key.alloc(nc));
+    CK(key2.alloc(nc));
+    CK(face.alloc(nc));
+    CK(face2.alloc(nc));
+    k_incidence<<<blocks_for(nc), 256, 0, s>>>(df.p, nc, key.p, face.p);
+    CK(cudaGetLastError());
+    int bits = 1;  // vertex ids are below nv <= 2^bits
+    while (bits < 32 && (uint64_t(1) << bits) < uint64_t(nv)) ++bits;
+    // LSD radix sort is stable: each vertex keeps its faces in ascending order.
+    if ((rc = radix_sort_pairs(ctx, key.p, key2.p, face.p, face2.p, nc, bits))) return rc;
+  }
+  k_vertex_normals<<<blocks_for(nv), 256, 0, s>>>(dv.p, df.p, key2.p, face2.p, nc, nv, dn.p);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(normals, dn.p, 24 * size_t(nv), cudaMemcpyDeviceToHost, s));
+  return finish(ctx, "vertex_normals", nv, true);
+}
+
+}  // extern "C"
+
+namespace {
+
+bool all_finite(const double *p, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
+// The box padding of a cloud built from `p` placed by the row-major pose t:
+// 1e-6 of a bound on the placed coordinates' magnitude (at least 1), the
+// padding cloud_build gives a cloud of the placed points themselves.
+float placed_pad(const double *p, uint32_t n, const double *t) {
+  double m[3] = {0.0, 0.0, 0.0};
+  for (size_t i = 0; i < size_t(n); ++i)
+    for (int c = 0; c < 3; ++c) m[c] = std::max(m[c], std::fabs(p[3 * i + c]));
+  double mag = 1.0;
+  for (int r = 0; r < 3; ++r) {
+    double b = std::fabs(t[4 * r + 3]);
+    for (int c = 0; c < 3; ++c) b += std::fabs(t[4 * r + c]) * m[c];
+    mag = std::max(mag, b * (1.0 + 1e-9));
+  }
+  return float(1e-6 * mag);
+}
+
+void identity_registration(sherd_registration &r) {
+  std::memset(&r, 0, sizeof r);
+  for (int k = 0; k < 16; k += 5) r.transform[k] = 1.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sherd_refine_join(sherd_ctx *ctx, const double *source, uint32_t n_source,
+                      const double *target, const double *target_normals, uint32_t n_target,
+                      const double pose_fixed[16], const double pose_moving[16],
+                      const double dist[2], int32_t max_iteration, sherd_registration out[2]) {
+  if (!ctx || (!source && n_source) || ((!target || !target_normals) && n_target) || !pose_fixed ||
+      !pose_moving || !dist || !out)
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  if (max_iteration < 0) return fail(ctx, SHERD_E_INVALID, "negative iteration cap");
+  if (!finite_pose(pose_fixed) || !finite_pose(pose_moving))
+    return fail(ctx, SHERD_E_INVALID, "pose is not finite");
+  if (!all_finite(source, size_t(3) * n_source) || !all_finite(target, size_t(3) * n_target) ||
+      !all_finite(target_normals, size_t(3) * n_target))
+    return fail(ctx, SHERD_E_INVALID, "non-finite point or normal");
+  if (n_source == 0 || n_target == 0) {  // nothing to register: both rungs stay at the identity
+    identity_registration(out[0]);
+    identity_registration(out[1]);
+    return SHERD_OK;
+  }
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  const uint32_t ns = n_source, nt = n_target;
+  DBuf<double> raw_s, raw_t, raw_n, placed_s, placed_t, placed_n;
+  if ((rc = upload(ctx, raw_s, source, size_t(3) * ns)) ||
+      (rc = upload(ctx, raw_t, target, size_t(3) * nt)) ||
+      (rc = upload(ctx, raw_n, target_normals, size_t(3) * nt)))
+    return rc;
+  CK(placed_s.alloc(size_t(3) * ns));
+  CK(placed_t.alloc(size_t(3) * nt));
+  CK(placed_n.alloc(size_t(3) * nt));
+  k_place_fused<<<blocks_for(ns), 256, 0, s>>>(raw_s.p, ns, pose_of(pose_moving), 0, placed_s.p);
+  k_place_fused<<<blocks_for(nt), 256, 0, s>>>(raw_t.p, nt, pose_of(pose_fixed), 0, placed_t.p);
+  k_place_fused<<<blocks_for(nt), 256, 0, s>>>(raw_n.p, nt, pose_of(pose_fixed), 1, placed_n.p);
+  CK(cudaGetLastError());
+  sherd_cloud src, tgt;
+  if ((rc = cloud_build_dev(ctx, placed_s.p, nullptr, ns, placed_pad(source, ns, pose_moving), &src)) ||
+      (rc = cloud_build_dev(ctx, placed_t.p, placed_n.p, nt, placed_pad(target, nt, pose_fixed), &tgt)))
+    return rc;
+
+  // A slice of about 256 source points per block, at most 4 blocks per SM.
+  const uint32_t blocks =
+      std::max(1u, std::min<uint32_t>((ns + 255u) / 256u, 4u * uint32_t(std::max(ctx->sm_count, 1))));
+  const uint32_t chunk = (ns + blocks - 1u) / blocks;
+  DBuf<double> partials, identity;
+  DBuf<int> hints;
+  DBuf<WideState> state;
+  DBuf<sherd_registration> dout;
+  CK(partials.alloc(size_t(blocks) * ICP_SUMS));
+  CK(hints.alloc(ns));
+  CK(state.alloc(1));
+  CK(dout.alloc(2));
+  static const double kIdentity[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+  if ((rc = upload(ctx, identity, kIdentity, 16))) return rc;
+  const double *first_pose = reinterpret_cast<const double *>(
+      reinterpret_cast<const char *>(dout.p) + offsetof(sherd_registration, transform));
+  // The rungs alone are timed too (method "refine_join_rungs"; items = passes).
+  cudaEvent_t rungs_begin = nullptr, rungs_end = nullptr;
+  CK(cudaEventCreate(&rungs_begin));
+  if (cudaEventCreate(&rungs_end) != cudaSuccess) {
+    cudaEventDestroy(rungs_begin);
+    return fail(ctx, SHERD_E_DEVICE, "refine_join: cudaEventCreate failed");
+  }
+  struct EventPair {
+    cudaEvent_t a, b;
+    ~EventPair() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } events{rungs_begin, rungs_end};
+  CK(cudaEventRecord(rungs_begin, s));
+  uint32_t done = 0;
+  size_t launched = 0;
+  for (int r = 0; r < 2; ++r) {
+    CK(cudaMemsetAsync(hints.p, 0xFF, sizeof(int) * size_t(ns), s));  // no match yet: -1
+    k_wide_reset<<<1, 32, 0, s>>>(state.p, r == 0 ? identity.p : first_pose);
+    // max_iteration + 1 passes at most; the state says when the rung ended
+    // sooner, looked at every 16 passes.
+    for (int64_t pass = 0; pass <= int64_t(max_iteration); ++pass) {
+      k_wide_pass<<<blocks, ICP_BLOCK, 0, s>>>(src.pts.p, ns, tgt.view, dist[r], max_iteration,
+                                               state.p, hints.p, chunk, partials.p, dout.p + r,
+                                               ctx->d_status);
+      CK(cudaGetLastError());
+      ++launched;
+      if (pass % 16 == 15 && pass < int64_t(max_iteration)) {
+        CK(cudaMemcpyAsync(&done, reinterpret_cast<const char *>(state.p) + offsetof(WideState, done), 4,
+                           cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (done) break;
+      }
+    }
+  }
+  CK(cudaEventRecord(rungs_end, s));
+  CK(cudaMemcpyAsync(out, dout.p, sizeof(sherd_registration) * 2, cudaMemcpyDeviceToHost, s));
+  rc = finish(ctx, "refine_join", ns, true);
+  if (rc) return rc;
+  float ms = 0.0f;
+  MethodStats &m = ctx->stats["refine_join_rungs"];
+  m.calls += 1;
+  m.items += launched;
+  if (cudaEventElapsedTime(&ms, rungs_begin, rungs_end) == cudaSuccess) m.ms += ms;
   return SHERD_OK;
 }
 

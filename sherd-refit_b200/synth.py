@@ -624,6 +624,10 @@ CONFIGS = {
     "thin": lambda seed=0: pot_collection(seed, walls=(2.0,), cells_per_wall=(6,),
                                           edges_per_t=(4.0, 5.0), n_starts=128,
                                           surface_points=500_000, name="thin"),
+    # R 9's input at full resolution: one pot of t = 24 in 8 fragments of 1.1M-2.2M faces (the
+    # size of a 1.2M-face scan), 55k-90k fracture vertices each, 18 adjacent pairs.
+    "scan": lambda seed=0: pot_collection(seed, walls=(24.0,), cells_per_wall=(8,),
+                                          edges_per_t=(64.0, 66.0), n_starts=4, name="scan"),
 }
 
 

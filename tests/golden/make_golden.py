@@ -20,7 +20,12 @@ without the reference tree present:
   `s2.T_reg1..s2.T_frac2`, the scores `s2.scores.json` and the verdicts `s2.accepted`;
 * the coarse breakline score (`executor/cpu.rs:46-68,136-169`) through R 5.4's re-score:
   B's breakline subset `md.brk_sub`, the refined stage-1 poses `s1.T` and their scores
-  `s1.score` against A's whole breakline at `scales.stage1`.
+  `s1.score` against A's whole breakline at `scales.stage1`;
+* R 9's join refinement (`refine.rs:282-386`, `sherd-parity/src/stages/refine.rs`): each
+  fragment's vertex selection `refine/<name>.idx` and its `mesh.stats` (thick, res), the
+  assembly's poses, groups and joins in `used` order (`assembly/*.json`), the joins the
+  refinement walked (`refine/joins.json`: ends, radii, both rung poses, fitness, rmse / t) and
+  the refined poses `refine/poses_final.json`.
 
 Derived arrays are computed here with numpy exactly as the reference's harness computes them:
 the f64 face normals and areas of `mesh::geometry::face_geometry` (`mesh/geometry.rs:70-96`,
@@ -87,6 +92,31 @@ def arrays_at(frag_dir: Path, t: float, surface_points: int) -> Path:
     raise SystemExit(f"no md arrays at t={t!r} under {frag_dir}")
 
 
+def refine_arrays(dump: Path, out: dict) -> None:
+    """R 9's inputs and answers, fragments numbered in PIECES order."""
+    names = list(PIECES)
+
+    def poses(path: Path) -> np.ndarray:
+        value = json.loads(path.read_text())
+        return np.stack([np.array(value[n], dtype=np.float64) for n in names])
+
+    out["refine_before"] = poses(dump / "assembly" / "poses.json")
+    out["refine_after"] = poses(dump / "refine" / "poses_final.json")
+    used = json.loads((dump / "assembly" / "used.json").read_text())
+    out["refine_used"] = np.array([[names.index(u["a"]), names.index(u["b"])] for u in used],
+                                  dtype=np.uint32).reshape(-1, 2)
+    groups = json.loads((dump / "assembly" / "groups.json").read_text())
+    out["refine_group_sizes"] = np.array([len(g) for g in groups], dtype=np.uint32)
+    out["refine_group_members"] = np.array([names.index(n) for g in groups for n in g],
+                                           dtype=np.uint32)
+    joins = json.loads((dump / "refine" / "joins.json").read_text())
+    out["refine_join_ends"] = np.array([[names.index(j["fixed"]), names.index(j["moving"])]
+                                        for j in joins], dtype=np.uint32).reshape(-1, 2)
+    out["refine_join_dist"] = np.array([j["dist"] for j in joins]).reshape(-1, 2)
+    out["refine_join_rungs"] = np.array([j["T_rung"] for j in joins]).reshape(-1, 2, 4, 4)
+    out["refine_join_fit_rmse"] = np.array([[j["fitness"], j["rmse_t"]] for j in joins]).reshape(-1, 2)
+
+
 def main(reference: Path) -> None:
     dump = reference / "fixtures" / "slab" / "dump"
     pair_dir = dump / "pairs" / PAIR
@@ -149,6 +179,9 @@ def main(reference: Path) -> None:
         out[p + "reg_n"] = np.concatenate([nf_[:take_f], nm[:take_m]])
         out[p + "frac_p"] = pf
         out[p + "frac_n"] = nf_
+        out[p + "refine_idx"] = np.load(dump / "refine" / f"{name}.idx.npy").astype(np.uint32)
+        stats = json.loads((fd / "mesh.stats.json").read_text())
+        out[p + "stats_thick_res"] = np.array([float(stats["thick"]), float(stats["res"])])
     scales = json.loads((pair_dir / "scales.json").read_text())
     out["scales"] = np.array([scales[k] for k in (
         "t", "res", "coarse", "stage1", "tight", "facing", "gap", "seam", "near", "pen", "nms",
@@ -166,6 +199,7 @@ def main(reference: Path) -> None:
     out["s2_accepted"] = np.load(pair_dir / "s2.accepted.npy").astype(np.uint8)
     out["params"] = np.array([params[k] for k in (
         "min_tight", "max_gap", "max_pen", "min_seam", "min_cont_n")], dtype=np.float64)
+    refine_arrays(dump, out)
     target = Path(__file__).resolve().parent / "slab.npz"
     np.savez_compressed(target, **out)
     print(f"wrote {target} ({target.stat().st_size / 1e6:.2f} MB, {len(out)} arrays)")
