@@ -16,7 +16,7 @@ reference cannot be built here) on all host cores instead. `--config group` meas
 differentiation workload instead (sherd_adjoint over 4096 perturbed poses of an assembled
 8-fragment pot, and a 50-evaluation joint refinement). `--config refine` measures R 9, the
 full-resolution join refinement of one assembled pot (fracture clouds and the spanning walk of
-two-rung ICP joins).
+two-rung ICP joins). `--config stage1` measures R 5.1-5.5 on the reference's slab pair.
 """
 
 from __future__ import annotations
@@ -396,6 +396,92 @@ def run_refine(args):
     ctx.close()
 
 
+def run_stage1(args):
+    """Stage 1 (R 5.1-5.5) of the reference's own slab pair (tests/golden/slab.npz, extracted
+    from its fixture dump): 16 337 hypotheses scored on a 60-point probe, 250 kept and refined
+    by two point-to-point rungs, re-scored, 10 kept. One step is the whole chain on the device
+    (PairStage1.run with its own walk orders); the oracle runs the same chain on the CPU."""
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    sherd = _pkg()
+    st = _pkg("stage1")
+    with np.load(ROOT / "tests" / "golden" / "slab.npz") as z:
+        slab = {k: z[k] for k in z.files}
+
+    def frames(name):
+        g = lambda k: slab[f"{name}.{k}"]
+        return st.Frames(p=g("brk_P"), ns=g("brk_ns"), f=g("brk_f"), dih=g("brk_dih"),
+                         sub=g("brk_sub"))
+
+    fa, fb = frames("pieceA"), frames("pieceB")
+    ctx = sherd.Context(local)
+    scales = sherd.Scales(*[float(x) for x in slab["scales"]])
+    pair = st.PairStage1(ctx, fa, fb, scales)
+    for _ in range(args.warmup):
+        pair.run(seed=args.seed)
+    stats0 = ctx.stats()["methods"]
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res = pair.run(seed=args.seed)
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    stats1 = ctx.stats()["methods"]
+    device_ms = {k: (v["ms"] - stats0.get(k, {}).get("ms", 0.0)) / args.steps
+                 for k, v in stats1.items() if v["calls"] > stats0.get(k, {}).get("calls", 0)}
+    step = float(np.median(times))
+    n_hyp = len(res.hypotheses)
+    cpu = None
+    if not args.no_cpu:
+        oracle = importlib.import_module("oracle")
+        a = {"p": fa.p, "ns": fa.ns, "f": fa.f, "dih": fa.dih}
+        b = {"p": fb.p, "ns": fb.ns, "f": fb.f, "dih": fb.dih}
+        osc = oracle.scales_from(slab["scales"])
+        t0 = time.perf_counter()
+        pa, pb, poses = oracle.hypotheses(a, b, fa.sub, fb.sub)
+        idx = st.probe_draw(fb.sub, st.COARSE_POINTS, args.seed).astype(np.int64)
+        target = oracle.Cloud(fa.p, fa.ns)
+        cs = oracle.coarse_scores(target, fb.p[idx], fb.ns[idx], poses, osc.coarse)
+        kept = oracle.nms(oracle.order_by_score(cs, oracle.COARSE_ORDER_LIMIT), poses, cs,
+                          osc.nms, st.STAGE1, oracle.COARSE_FLOOR)
+        sub = np.asarray(fb.sub, np.int64)
+        refined = oracle.stage1_ladder(fb.p[sub], target, poses[kept.astype(np.int64)], osc)
+        rescore = oracle.coarse_scores(target, fb.p[sub], fb.ns[sub], refined, osc.stage1)
+        kept2 = oracle.nms(oracle.order_by_score(rescore), refined, rescore, osc.nms, st.STAGE2,
+                           oracle.STAGE1_FLOOR)
+        t_cpu = time.perf_counter() - t0
+        same = (np.array_equal(kept, res.kept) and np.array_equal(kept2, res.kept2)
+                and np.array_equal(cs, res.coarse))
+        cpu = {"value": 1.0 / t_cpu, "unit": "pairs/s", "cores": oracle.lib().or_default_threads(),
+               "kind": "port", "sample": f"the whole chain once, {t_cpu:.2f} s",
+               "same_kept_lists_and_coarse_scores": bool(same)}
+    line = {
+        "metric": "stage-1 pairs/s (R 5.1-5.5)", "value": 1.0 / step, "unit": "pairs/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "the reference's slab fixture pair (tests/golden/slab.npz)",
+        "config": {"workload": (f"slab pair: {n_hyp} hypotheses x {st.COARSE_POINTS} probe points, "
+                                f"{len(res.kept)} refined (2 point-to-point rungs over "
+                                f"{len(fb.sub)} points), {len(res.kept2)} starts"),
+                   "timer": "host wall clock around the chain (median of the steps)"},
+        "hypotheses_per_s": n_hyp / step,
+        "device_ms": device_ms,
+        "gpu_launches": args.steps * 8,
+        "gpu_launches_counts": ("k_hyp_flags, the compaction, k_hyp_poses, k_coarse_scores, 2 "
+                                "k_icp_rung, k_coarse_scores; the LBVH and cloud builds' own "
+                                "launches not counted"),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def _config_dict(wl, args, extra=None):
     d = wl.describe()
     cfg = {"workload": f"{args.config}: {d['fragments']} fragments, {d['pairs']} pairs x "
@@ -432,6 +518,9 @@ def main():
         return
     if args.config == "refine":
         run_refine(args)
+        return
+    if args.config == "stage1":
+        run_stage1(args)
         return
 
     import torch

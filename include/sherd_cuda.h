@@ -469,6 +469,57 @@ int sherd_adjoint(sherd_ctx *ctx, sherd_pair *const *edges, uint32_t n_edges,
                   const double *poses, const double *inverses, uint32_t n_poses,
                   const sherd_adjoint_options *opt, double *values, double *grads);
 
+/* ---- stage 1: hypotheses, coarse score, suppression (R 5.1-5.5) --------- */
+
+/* One fragment's breakline as R 5 reads it (hypotheses.rs:53-82): n points
+ * p, shell macro-normals ns and in-plane axes f (xyz f64 each; the tangent is
+ * ns x f, formed here in f64), and the dihedral of each point in degrees. */
+typedef struct sherd_frames {
+    const double *p;
+    const double *ns;
+    const double *f;
+    const double *dih;
+    uint32_t n;
+} sherd_frames;
+
+/* R 5.1 and R 5.2 in one call (hypotheses.rs:149-211, coarse.rs:113-133):
+ * every (i, j) of the subsets ia (positions into a's points) and ib with
+ * |dih_a[ia[i]] + dih_b[ib[j]] - 180| < dihedral_tol, in row-major (i, j)
+ * order; its pose R = RA RB^T, tau = P_A - R P_B (RA = [t | ns | f] at ia[i],
+ * RB = [-t | ns | -f] at ib[j]); and its coarse score against `target` (A's
+ * whole breakline with its shell normals): the fraction of the probe (q, qn:
+ * n_probe points of B and their shell normals) within `delta` of the target
+ * after the pose, with the matched normal . R qn > normal_agree. The poses stay
+ * on the device between the two stages. Outputs: *count, and when capacity >=
+ * *count, pa[h], pb[h] (positions into ia and ib), poses[16 h..] (row-major
+ * 4x4) and scores[h]. capacity = 0 asks for the count alone; a non-zero
+ * capacity below the count is refused (SHERD_E_INVALID, *count set). n_ia n_ib
+ * must stay below 2^31. Poses and scores are bit-identical to the reference's
+ * sequential restatement. */
+int sherd_hypotheses_coarse(sherd_ctx *ctx, const sherd_frames *a, const sherd_frames *b,
+                            const uint32_t *ia, uint32_t n_ia, const uint32_t *ib, uint32_t n_ib,
+                            double dihedral_tol, const sherd_cloud *target, const double *q,
+                            const double *qn, uint32_t n_probe, double delta,
+                            double normal_agree, uint32_t capacity, uint32_t *pa, uint32_t *pb,
+                            double *poses, double *scores, uint32_t *count);
+
+/* nms::order_by_score (nms.rs:46-59): the indices 0..n-1 by descending score
+ * (f64 total order), ties by ascending index, the first `limit` of them.
+ * `order` has room for min(n, limit); *n_order receives that count. Host code,
+ * no device. */
+int sherd_order_by_score(const double *score, uint32_t n, uint32_t limit, uint32_t *order,
+                         uint32_t *n_order);
+
+/* nms::nms (nms.rs:61-86), R 5.3 and R 5.5's greedy suppression: walk
+ * `order`; stop at the first score below `floor`; keep a pose unless a kept one
+ * is nearer than trans_tol in translation and trace(R^T R') > 2.9; stop once
+ * `topk` are kept (tested after keeping, so topk = 0 keeps one). `poses` holds
+ * n_poses row-major 4x4 poses that order indexes. `kept` has room for
+ * min(n_order, max(topk, 1)); *n_kept receives the count. Host code. */
+int sherd_nms(const uint32_t *order, uint32_t n_order, const double *poses, const double *score,
+              uint32_t n_poses, double trans_tol, uint32_t topk, double floor, uint32_t *kept,
+              uint32_t *n_kept);
+
 /* ---- R 9: full-resolution join refinement (refine.rs) ------------------- */
 
 /* refine::vertex_normals (refine.rs:121-151), Open3D's ComputeVertexNormals:

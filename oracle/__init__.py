@@ -682,3 +682,88 @@ def refine_joins(pieces, poses, groups, used, params: Params | None = None, one=
                 joins.append(join)
             done.append(moving)
     return out, joins
+
+
+# ---- stage 1: R 5.1-5.5 (hypotheses.rs, coarse.rs, nms.rs, ladder.rs, pair.rs:150-238) ----------
+
+STAGE1_RUNGS = (0.2, 0.08)   # ladder.rs:51
+STAGE1_ITERATIONS = 20       # ladder.rs:53
+STAGE1_FLOOR = 0.05          # ladder.rs:61
+COARSE_ORDER_LIMIT = 5000    # pair.rs:50
+COARSE_FLOOR = 0.1           # pair.rs:52
+NMS_ROT_TOL = 2.9            # nms.rs:40
+
+
+def tangents(ns, f):
+    """Breaklines::tangents_f64 (breakline.rs:180-182, 361-363): ns x f in f64."""
+    ns, f = f64(ns).reshape(-1, 3), f64(f).reshape(-1, 3)
+    return np.stack([ns[:, 1] * f[:, 2] - ns[:, 2] * f[:, 1], ns[:, 2] * f[:, 0] - ns[:, 0] * f[:, 2],
+                     ns[:, 0] * f[:, 1] - ns[:, 1] * f[:, 0]], axis=1)
+
+
+def hypotheses(a, b, ia, ib, dihedral_tol=25.0):
+    """hypotheses::build_with + poses (hypotheses.rs:149-211). `a`, `b` are dicts of f64 arrays
+    p, ns, f, dih. Returns (pa, pb, poses (n, 4, 4)) in row-major (i, j) order."""
+    ia, ib = np.asarray(ia, np.int64), np.asarray(ib, np.int64)
+    ok = np.abs(a["dih"][ia][:, None] + b["dih"][ib][None, :] - 180.0) < dihedral_tol
+    pa, pb = np.nonzero(ok)
+    ka, kb = ia[pa], ib[pb]
+    ta, tb = tangents(a["ns"], a["f"])[ka], tangents(b["ns"], b["f"])[kb]
+    axa = (ta, a["ns"][ka], a["f"][ka])
+    axb = (tb, b["ns"][kb], b["f"][kb])
+    n = len(pa)
+    poses = np.zeros((n, 4, 4))
+    poses[:, 3, 3] = 1.0
+    for i in range(3):
+        for k in range(3):
+            poses[:, i, k] = ((axa[0][:, i] * -axb[0][:, k] + axa[1][:, i] * axb[1][:, k])
+                              + axa[2][:, i] * -axb[2][:, k])
+    pA, pB = a["p"][ka], b["p"][kb]
+    for i in range(3):
+        poses[:, i, 3] = pA[:, i] - ((poses[:, i, 0] * pB[:, 0] + poses[:, i, 1] * pB[:, 1])
+                                     + poses[:, i, 2] * pB[:, 2])
+    return pa.astype(np.uint32), pb.astype(np.uint32), poses
+
+
+def order_by_score(score, limit=None):
+    """nms::order_by_score (nms.rs:46-59): descending, ties by ascending index."""
+    score = np.asarray(score, np.float64)
+    order = np.lexsort((np.arange(len(score)), -score))
+    return order[:limit] if limit is not None else order
+
+
+def nms(order, poses, score, trans_tol, topk, floor):
+    """nms::nms (nms.rs:61-86) with trace(A^T B) summed as nms.rs:93-99 sums it."""
+    poses = np.asarray(poses, np.float64)
+    kept = []
+    for h in order:
+        h = int(h)
+        if score[h] < floor:
+            break
+        t = poses[h]
+        duplicate = False
+        for k in kept:
+            u = poses[k]
+            d = t[:3, 3] - u[:3, 3]
+            if np.sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) < trans_tol:
+                tr = 0.0
+                for i in range(3):
+                    tr += (t[0, i] * u[0, i] + t[1, i] * u[1, i]) + t[2, i] * u[2, i]
+                if tr > NMS_ROT_TOL:
+                    duplicate = True
+                    break
+        if not duplicate:
+            kept.append(h)
+        if len(kept) >= topk:
+            break
+    return np.array(kept, np.uint32)
+
+
+def stage1_ladder(source, target: Cloud, inits, scales: Scales):
+    """ladder::climb_all over stage1_rungs (ladder.rs:105-140): two point-to-point rungs."""
+    poses = np.asarray(inits, np.float64).reshape(-1, 4, 4)
+    for k in STAGE1_RUNGS:
+        regs = icp_rung(source, target, poses, k * scales.t * scales.icp, STAGE1_ITERATIONS,
+                        point_to_point=True)
+        poses = np.stack([np.array(r.transform[:]).reshape(4, 4) for r in regs])
+    return poses

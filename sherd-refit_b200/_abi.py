@@ -115,6 +115,12 @@ class SegInfo(C.Structure):
                 ("boundary_angle", C.c_double)]
 
 
+class Frames(C.Structure):
+    """sherd_frames: one fragment's breakline (p, ns, f: xyz f64; dih: degrees)."""
+    _fields_ = [("p", C.c_void_p), ("ns", C.c_void_p), ("f", C.c_void_p), ("dih", C.c_void_p),
+                ("n", C.c_uint32)]
+
+
 class SegTrace(C.Structure):
     _fields_ = [("rep", C.c_void_p), ("near", C.c_void_p), ("ns", C.c_void_p),
                 ("good", C.c_void_p), ("frac_raw", C.c_void_p), ("frac_majority", C.c_void_p),
@@ -184,6 +190,13 @@ _SIGNATURES = {
     "sherd_segment": (C.c_int, [VP, VP, F64P, C.c_uint32, U32P, C.c_uint32, C.c_double,
                                 C.c_double, C.POINTER(SegParams), U8P, C.POINTER(SegInfo),
                                 C.POINTER(SegTrace)]),
+    "sherd_hypotheses_coarse": (C.c_int, [VP, C.POINTER(Frames), C.POINTER(Frames), U32P,
+                                          C.c_uint32, U32P, C.c_uint32, C.c_double, VP, F64P,
+                                          F64P, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
+                                          VP, VP, VP, VP, C.POINTER(C.c_uint32)]),
+    "sherd_order_by_score": (C.c_int, [F64P, C.c_uint32, C.c_uint32, VP, C.POINTER(C.c_uint32)]),
+    "sherd_nms": (C.c_int, [U32P, C.c_uint32, F64P, F64P, C.c_uint32, C.c_double, C.c_uint32,
+                            C.c_double, VP, C.POINTER(C.c_uint32)]),
     "sherd_vertex_normals": (C.c_int, [VP, F64P, C.c_uint32, U32P, C.c_uint32, F64P]),
     "sherd_refine_join": (C.c_int, [VP, F64P, C.c_uint32, F64P, F64P, C.c_uint32, F64P, F64P,
                                     F64P, C.c_int32, VP]),

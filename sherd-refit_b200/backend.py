@@ -35,6 +35,46 @@ def _pose(t) -> np.ndarray:
     return _f64(t, (16,))
 
 
+def _frames(fr):
+    """A sherd_frames over contiguous f64 copies of fr.p, fr.ns, fr.f, fr.dih (kept alive in the
+    returned tuple)."""
+    p, ns, f = _f64(fr.p), _f64(fr.ns), _f64(fr.f)
+    dih = _f64(fr.dih, (-1,))
+    if not (len(p) == len(ns) == len(f) == len(dih)):
+        raise A.SherdError(A.E_INVALID, "frame arrays differ in length")
+    return A.Frames(ptr(p), ptr(ns), ptr(f), ptr(dih), len(p)), (p, ns, f, dih)
+
+
+ALL = 0xFFFFFFFF
+
+
+def order_by_score(score, limit: int = ALL) -> np.ndarray:
+    """nms::order_by_score (nms.rs:46-59): descending (f64 total order), ties by ascending
+    index, the first `limit`."""
+    s = _f64(score, (-1,))
+    m = min(len(s), int(limit))
+    out = np.empty(m, np.uint32)
+    n = C.c_uint32(0)
+    if A.lib().sherd_order_by_score(s, len(s), int(min(limit, ALL)), ptr(out), C.byref(n)):
+        raise A.SherdError(A.E_INVALID, "order_by_score")
+    return out[:n.value]
+
+
+def nms(order, poses, score, trans_tol: float, topk: int, floor: float) -> np.ndarray:
+    """nms::nms (nms.rs:61-86) over row-major 4x4 poses: the kept indices, in keeping order."""
+    order = _u32(order)
+    poses = _f64(poses, (-1, 16))
+    score = _f64(score, (-1,))
+    if len(poses) != len(score):
+        raise A.SherdError(A.E_INVALID, "one score per pose")
+    kept = np.empty(max(min(len(order), max(int(topk), 1)), 1), np.uint32)
+    n = C.c_uint32(0)
+    if A.lib().sherd_nms(order, len(order), poses, score, len(poses), float(trans_tol), int(topk),
+                         float(floor), ptr(kept), C.byref(n)):
+        raise A.SherdError(A.E_INVALID, "nms: an order entry names no pose")
+    return kept[:n.value].copy()
+
+
 class _Handle:
     _free = ""
 
@@ -304,6 +344,30 @@ class Context:
         check(self.h, A.lib().sherd_adjoint(self.h, arr, n_e, poses, inverses, n_p, C.byref(opts),
                                             values, grads))
         return values, grads
+
+    # -- stage 1 ---------------------------------------------------------------------------------
+    def hypotheses_coarse(self, frames_a, frames_b, ia, ib, dihedral_tol, target: "Cloud", q, qn,
+                          delta, normal_agree=0.7):
+        """R 5.1 + R 5.2 (hypotheses.rs:149-211, coarse.rs:113-133) on the device:
+        (pa, pb, poses (n, 4, 4), scores) of every complementary (ia[i], ib[j]) frame pair, in
+        row-major (i, j) order. `frames_*` have p, ns, f (n, 3) and dih (n,) as f64 arrays."""
+        ia, ib = _u32(ia), _u32(ib)
+        q, qn = _f64(q), _f64(qn)
+        fa, fb = _frames(frames_a), _frames(frames_b)
+        count = C.c_uint32(0)
+        check(self.h, A.lib().sherd_hypotheses_coarse(
+            self.h, C.byref(fa[0]), C.byref(fb[0]), ia, len(ia), ib, len(ib), float(dihedral_tol),
+            target.h, q, qn, len(q), float(delta), float(normal_agree), 0, None, None, None, None,
+            C.byref(count)))
+        n = count.value
+        pa, pb = np.empty(n, np.uint32), np.empty(n, np.uint32)
+        poses, scores = np.empty((n, 4, 4)), np.empty(n)
+        if n:
+            check(self.h, A.lib().sherd_hypotheses_coarse(
+                self.h, C.byref(fa[0]), C.byref(fb[0]), ia, len(ia), ib, len(ib),
+                float(dihedral_tol), target.h, q, qn, len(q), float(delta), float(normal_agree),
+                n, ptr(pa), ptr(pb), ptr(poses), ptr(scores), C.byref(count)))
+        return pa, pb, poses, scores
 
     # -- R 9 join refinement ----------------------------------------------------------------------
     def vertex_normals(self, v, f):

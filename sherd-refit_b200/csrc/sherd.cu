@@ -28,6 +28,7 @@
 #include "adjoint.cuh"
 #include "segment.cuh"
 #include "refine.cuh"
+#include "stage1.cuh"
 
 using namespace sherd;
 
@@ -2219,6 +2220,153 @@ int sherd_refine_join(sherd_ctx *ctx, const double *source, uint32_t n_source,
   m.calls += 1;
   m.items += launched;
   if (cudaEventElapsedTime(&ms, rungs_begin, rungs_end) == cudaSuccess) m.ms += ms;
+  return SHERD_OK;
+}
+
+
+// ---- stage 1: hypotheses, coarse score, suppression (R 5.1-5.5) ---------------
+
+int sherd_hypotheses_coarse(sherd_ctx *ctx, const sherd_frames *a, const sherd_frames *b,
+                            const uint32_t *ia, uint32_t n_ia, const uint32_t *ib, uint32_t n_ib,
+                            double dihedral_tol, const sherd_cloud *target, const double *q,
+                            const double *qn, uint32_t n_probe, double delta,
+                            double normal_agree, uint32_t capacity, uint32_t *pa, uint32_t *pb,
+                            double *poses, double *scores, uint32_t *count) {
+  if (!ctx || !a || !b || !target || !count || (!ia && n_ia) || (!ib && n_ib) ||
+      ((!q || !qn) && n_probe) || (capacity && (!pa || !pb || !poses || !scores)))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  *count = 0;
+  if ((a->n && (!a->p || !a->ns || !a->f || !a->dih)) || (b->n && (!b->p || !b->ns || !b->f || !b->dih)))
+    return fail(ctx, SHERD_E_INVALID, "null frame array");
+  if (!target->view.nrm) return fail(ctx, SHERD_E_INVALID, "the target carries no normals");
+  if (uint64_t(n_ia) * n_ib >= (uint64_t(1) << 31))
+    return fail(ctx, SHERD_E_INVALID, "n_ia * n_ib must stay below 2^31");
+  for (uint32_t i = 0; i < n_ia; ++i)
+    if (ia[i] >= a->n) return fail(ctx, SHERD_E_INVALID, "ia names a point beyond a's frames");
+  for (uint32_t j = 0; j < n_ib; ++j)
+    if (ib[j] >= b->n) return fail(ctx, SHERD_E_INVALID, "ib names a point beyond b's frames");
+  if (n_ia == 0 || n_ib == 0) return SHERD_OK;  // no hypothesis (R 5.1's empty return)
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  DBuf<double> ap, ans, af, adih, bp, bns, bf, bdih, dq, dqn, dposes, dscores;
+  DBuf<uint32_t> dia, dib, lin, sel, nsel, dpa, dpb;
+  DBuf<uint8_t> flags;
+  if ((rc = upload(ctx, ap, a->p, size_t(3) * a->n)) || (rc = upload(ctx, ans, a->ns, size_t(3) * a->n)) ||
+      (rc = upload(ctx, af, a->f, size_t(3) * a->n)) || (rc = upload(ctx, adih, a->dih, size_t(a->n))) ||
+      (rc = upload(ctx, bp, b->p, size_t(3) * b->n)) || (rc = upload(ctx, bns, b->ns, size_t(3) * b->n)) ||
+      (rc = upload(ctx, bf, b->f, size_t(3) * b->n)) || (rc = upload(ctx, bdih, b->dih, size_t(b->n))) ||
+      (rc = upload(ctx, dia, ia, size_t(n_ia))) || (rc = upload(ctx, dib, ib, size_t(n_ib))) ||
+      (rc = upload(ctx, dq, q, size_t(3) * n_probe)) || (rc = upload(ctx, dqn, qn, size_t(3) * n_probe)))
+    return rc;
+  const uint32_t grid = n_ia * n_ib;
+  CK(flags.alloc(grid));
+  CK(lin.alloc(grid));
+  CK(sel.alloc(grid));
+  CK(nsel.alloc(1));
+  k_hyp_flags<<<blocks_for(grid), 256, 0, s>>>(adih.p, dia.p, n_ia, bdih.p, dib.p, n_ib, dihedral_tol,
+                                               flags.p, lin.p);
+  CK(cudaGetLastError());
+  {
+    size_t bytes = 0;
+    CK(cub::DeviceSelect::Flagged(nullptr, bytes, lin.p, flags.p, sel.p, nsel.p, int(grid), s));
+    DBuf<unsigned char> tmp;
+    CK(tmp.alloc(bytes));
+    CK(cub::DeviceSelect::Flagged(tmp.p, bytes, lin.p, flags.p, sel.p, nsel.p, int(grid), s));
+    CK(cudaStreamSynchronize(s));
+  }
+  uint32_t n = 0;
+  CK(cudaMemcpy(&n, nsel.p, 4, cudaMemcpyDeviceToHost));
+  *count = n;
+  if (n == 0 || capacity == 0) return finish(ctx, "hypotheses_coarse", 0, true);
+  if (capacity < n) {
+    rc = finish(ctx, "hypotheses_coarse", 0, true);
+    if (rc) return rc;
+    return fail(ctx, SHERD_E_INVALID, "capacity below the hypothesis count");
+  }
+  CK(dpa.alloc(n));
+  CK(dpb.alloc(n));
+  CK(dposes.alloc(size_t(16) * n));
+  CK(dscores.alloc(n));
+  FramesView fa{ap.p, ans.p, af.p, adih.p, a->n}, fb{bp.p, bns.p, bf.p, bdih.p, b->n};
+  k_hyp_poses<<<blocks_for(n), 256, 0, s>>>(fa, fb, dia.p, dib.p, n_ib, sel.p, n, dpa.p, dpb.p,
+                                            dposes.p);
+  CK(cudaGetLastError());
+  if (n_probe) {
+    unsigned cgrid = std::min(blocks_for(size_t(n) * 32, 128), unsigned(ctx->sm_count) * 16u);
+    k_coarse_scores<<<cgrid, 128, 0, s>>>(target->view, dq.p, dqn.p, n_probe, dposes.p, n, delta,
+                                          normal_agree, dscores.p, ctx->d_status);
+    CK(cudaGetLastError());
+  } else {
+    CK(cudaMemsetAsync(dscores.p, 0, sizeof(double) * n, s));  // 0 / 0 probe points: 0
+  }
+  CK(cudaMemcpyAsync(pa, dpa.p, 4 * size_t(n), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(pb, dpb.p, 4 * size_t(n), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(poses, dposes.p, sizeof(double) * 16 * size_t(n), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(scores, dscores.p, sizeof(double) * size_t(n), cudaMemcpyDeviceToHost, s));
+  return finish(ctx, "hypotheses_coarse", size_t(n) * n_probe, true);
+}
+
+}  // extern "C"
+
+namespace {
+
+// f64::total_cmp's key (a signed integer order equal to IEEE 754 totalOrder).
+int64_t total_key(double x) {
+  int64_t bits;
+  std::memcpy(&bits, &x, 8);
+  return bits ^ int64_t(uint64_t(bits >> 63) >> 1);
+}
+
+// nms::trace_of_transpose_product (nms.rs:93-99) on row-major 4x4 poses:
+// trace(A^T B) summed over columns i as (a0i b0i + a1i b1i) + a2i b2i.
+double trace_tp(const double *a, const double *b) {
+  double trace = 0.0;
+  for (int i = 0; i < 3; ++i) trace += (a[i] * b[i] + a[4 + i] * b[4 + i]) + a[8 + i] * b[8 + i];
+  return trace;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sherd_order_by_score(const double *score, uint32_t n, uint32_t limit, uint32_t *order,
+                         uint32_t *n_order) {
+  if (!n_order || ((!score || (!order && limit)) && n)) return SHERD_E_INVALID;
+  std::vector<uint32_t> idx(n);
+  for (uint32_t i = 0; i < n; ++i) idx[i] = i;
+  std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
+    int64_t kx = total_key(score[x]), ky = total_key(score[y]);
+    return kx != ky ? kx > ky : x < y;
+  });
+  uint32_t m = std::min(n, limit);
+  std::copy(idx.begin(), idx.begin() + m, order);
+  *n_order = m;
+  return SHERD_OK;
+}
+
+int sherd_nms(const uint32_t *order, uint32_t n_order, const double *poses, const double *score,
+              uint32_t n_poses, double trans_tol, uint32_t topk, double floor, uint32_t *kept,
+              uint32_t *n_kept) {
+  if (!n_kept || ((!order || !poses || !score || !kept) && n_order)) return SHERD_E_INVALID;
+  for (uint32_t o = 0; o < n_order; ++o)
+    if (order[o] >= n_poses) return SHERD_E_INVALID;
+  uint32_t m = 0;
+  for (uint32_t o = 0; o < n_order; ++o) {
+    const uint32_t h = order[o];
+    if (score[h] < floor) break;
+    const double *t = poses + 16 * size_t(h);
+    bool duplicate = false;
+    for (uint32_t k = 0; k < m && !duplicate; ++k) {
+      const double *u = poses + 16 * size_t(kept[k]);
+      const double dx = t[3] - u[3], dy = t[7] - u[7], dz = t[11] - u[11];
+      duplicate = std::sqrt((dx * dx + dy * dy) + dz * dz) < trans_tol && trace_tp(t, u) > 2.9;
+    }
+    if (!duplicate) kept[m++] = h;
+    if (m >= topk) break;
+  }
+  *n_kept = m;
   return SHERD_OK;
 }
 

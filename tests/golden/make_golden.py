@@ -18,6 +18,10 @@ without the reference tree present:
   at the pair's own `t` (`md.Pf`, `md.fp`, `md.S`, `md.sp`, `md.margin_idx`, `md.brk_P`,
   `md.brk_ns`), the pair's `scales.json`, the starts `s1.T[nms2.kept]`, the four rung poses
   `s2.T_reg1..s2.T_frac2`, the scores `s2.scores.json` and the verdicts `s2.accepted`;
+* stage 1 (R 5.1-5.5, `hypotheses.rs`, `coarse.rs`, `nms.rs`, `ladder.rs`): the breakline
+  frames' in-plane axes `md.brk_f` and dihedrals `md.brk_dih`, the subsets and kept pairs
+  `hyp.ia/ib/pa/pb`, the probe `coarse.idx` and every hypothesis's score `coarse.cs`, both
+  suppressions' walk orders and kept lists `nms1.*`, `nms2.*`;
 * the coarse breakline score (`executor/cpu.rs:46-68,136-169`) through R 5.4's re-score:
   B's breakline subset `md.brk_sub`, the refined stage-1 poses `s1.T` and their scores
   `s1.score` against A's whole breakline at `scales.stage1`;
@@ -169,6 +173,8 @@ def main(reference: Path) -> None:
         out[p + "brk_P"] = np.load(md / "md.brk_P.npy")
         out[p + "brk_ns"] = np.load(md / "md.brk_ns.npy")
         out[p + "brk_sub"] = np.load(md / "md.brk_sub.npy").astype(np.uint32)
+        out[p + "brk_f"] = np.load(md / "md.brk_f.npy")
+        out[p + "brk_dih"] = np.load(md / "md.brk_dih.npy")
         nf_ = fn[fp]
         pm = s[margin_idx]
         nm = fn[sp[margin_idx]]
@@ -186,6 +192,10 @@ def main(reference: Path) -> None:
     out["scales"] = np.array([scales[k] for k in (
         "t", "res", "coarse", "stage1", "tight", "facing", "gap", "seam", "near", "pen", "nms",
         "icp")], dtype=np.float64)
+    for k in ("hyp.ia", "hyp.ib", "hyp.pa", "hyp.pb", "coarse.idx", "nms1.order", "nms1.kept",
+              "nms2.order", "nms2.kept"):
+        out[k.replace(".", "_")] = np.load(pair_dir / f"{k}.npy").astype(np.uint32)
+    out["coarse_cs"] = np.load(pair_dir / "coarse.cs.npy")
     out["s1_T"] = np.load(pair_dir / "s1.T.npy")
     out["s1_score"] = np.load(pair_dir / "s1.score.npy")
     kept = np.load(pair_dir / "nms2.kept.npy").astype(np.int64)
