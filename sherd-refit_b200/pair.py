@@ -1,0 +1,79 @@
+"""R 5's whole pair chain on the device: matching/pair.rs:375-440 (`match_pair`).
+
+Stage 1 (`stage1.PairStage1.run`: hypotheses, coarse score, suppression, the breakline ladder
+and its re-score, the second suppression) gives at most `stage2` starts; each start goes through
+the batched stage-2 path (sherd_ladder_verify_batch: the four point-to-plane rungs, R 6's scores
+and R 6.5's verdict, one work item per start); R 5.7 then ranks the candidates by seam * tight,
+descending and stable (ties keep the second suppression's order), writes the pair's best stage-1
+score on every one and keeps the first `keep`. A pair whose best stage-1 score is under a
+non-zero `stage1_floor` returns its best stage-1 pose alone, marked partial and refused
+(pair.rs:413-432).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi as A
+from .backend import Context
+from .stage1 import PairStage1, Stage1Result
+
+KEEP_PER_PAIR = 5  # pipeline.rs:173
+
+
+@dataclass
+class PairResult:
+    """match_pair's candidates (sherd_candidate records, R 5.7's order, at most `keep`) and the
+    stage-1 result they came from. `starts[i]` is the start candidate i was refined from."""
+    candidates: list
+    stage1: Stage1Result
+    starts: list = field(default_factory=list)
+
+    @property
+    def transforms(self) -> list:
+        """Each candidate's pose: the last rung's (the R 5.6 ladder's result)."""
+        return [np.array(c.rungs[3].transform[:]).reshape(4, 4) for c in self.candidates]
+
+
+def _partial(scales: A.Scales, transform, brk: float) -> A.Candidate:
+    """Scores::partial (verify.rs:183-195): nothing computed, the two limits filled in, `brk`
+    and `brk_best` set, partial and refused."""
+    c = A.Candidate()
+    c.scores.gap_limit = scales.gap / scales.t
+    c.scores.tight_delta = scales.tight / scales.t
+    c.scores.partial = 1
+    c.scores.brk = brk
+    c.scores.brk_best = brk
+    c.accepted = 0
+    t = np.ascontiguousarray(transform, np.float64).reshape(16)
+    for r in range(4):
+        c.rungs[r].transform[:] = t.tolist()
+    return c
+
+
+def match_pair(ctx: Context, pair, stage1: PairStage1, params: A.Params,
+               keep: int = KEEP_PER_PAIR, seed: int = 0, stage1_floor: float = 0.0,
+               order1=None, order2=None) -> PairResult:
+    """Pair::match_pair (pair.rs:375-440) for one device pair (`pair`, a backend.Pair over the
+    same two fragments as `stage1`). `order1` / `order2` replace the two suppressions' walk
+    orders (the reference's Python pipeline's unstable ones, for parity runs)."""
+    s1 = stage1.run(seed=seed, order1=order1, order2=order2)
+    if not len(s1.scores):
+        return PairResult([], s1)
+    best1 = s1.best
+    if stage1_floor > 0.0 and best1 < stage1_floor:
+        k = int(np.flatnonzero(s1.scores == best1)[0])   # pair.rs:793-796, the first maximum
+        return PairResult([_partial(stage1.scales, s1.transforms[k], best1)], s1, [k])
+    starts = s1.starts
+    brk = s1.scores[s1.kept2.astype(np.int64)]
+    out = ctx.ladder_verify_batch([pair], [(0, k, starts[k]) for k in range(len(starts))], params)
+    cands = [A.Candidate.from_buffer_copy(out[k]) for k in range(len(starts))]
+    for c, b in zip(cands, brk):
+        c.scores.brk = float(b)
+    order = sorted(range(len(cands)), key=lambda k: -(cands[k].scores.seam * cands[k].scores.tight))
+    cands = [cands[k] for k in order]
+    for c in cands:
+        c.scores.brk_best = best1
+    return PairResult(cands[:keep], s1, order[:keep])

@@ -21,7 +21,8 @@ without the reference tree present:
 * stage 1 (R 5.1-5.5, `hypotheses.rs`, `coarse.rs`, `nms.rs`, `ladder.rs`): the breakline
   frames' in-plane axes `md.brk_f` and dihedrals `md.brk_dih`, the subsets and kept pairs
   `hyp.ia/ib/pa/pb`, the probe `coarse.idx` and every hypothesis's score `coarse.cs`, both
-  suppressions' walk orders and kept lists `nms1.*`, `nms2.*`;
+  suppressions' walk orders and kept lists `nms1.*`, `nms2.*`, and R 5.7's ranked result
+  `result.candidates.json` (pose, verdict, brk, brk_best, seam, tight of each of the 5 kept);
 * the coarse breakline score (`executor/cpu.rs:46-68,136-169`) through R 5.4's re-score:
   B's breakline subset `md.brk_sub`, the refined stage-1 poses `s1.T` and their scores
   `s1.score` against A's whole breakline at `scales.stage1`;
@@ -196,6 +197,11 @@ def main(reference: Path) -> None:
               "nms2.order", "nms2.kept"):
         out[k.replace(".", "_")] = np.load(pair_dir / f"{k}.npy").astype(np.uint32)
     out["coarse_cs"] = np.load(pair_dir / "coarse.cs.npy")
+    result = json.loads((pair_dir / "result.candidates.json").read_text())
+    out["result_T"] = np.array([c["T"] for c in result], dtype=np.float64).reshape(-1, 4, 4)
+    out["result_accepted"] = np.array([bool(c["accepted"]) for c in result], dtype=np.uint8)
+    out["result_brk"] = np.array([[c["brk"], c["brk_best"]] for c in result]).reshape(-1, 2)
+    out["result_seam_tight"] = np.array([[c["seam"], c["tight"]] for c in result]).reshape(-1, 2)
     out["s1_T"] = np.load(pair_dir / "s1.T.npy")
     out["s1_score"] = np.load(pair_dir / "s1.score.npy")
     kept = np.load(pair_dir / "nms2.kept.npy").astype(np.int64)
