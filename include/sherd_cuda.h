@@ -469,6 +469,29 @@ int sherd_adjoint(sherd_ctx *ctx, sherd_pair *const *edges, uint32_t n_edges,
                   const double *poses, const double *inverses, uint32_t n_poses,
                   const sherd_adjoint_options *opt, double *values, double *grads);
 
+/* ---- R 3.5.3-3.5.5: breaklines and their frames (fragment/breakline.rs) --- */
+
+/* breakline::build (breakline.rs:207-300) in f64 on one labelled working mesh
+ * (v: nv xyz f64; f: nf faces; frac: 1 for a fracture face): the midpoints of
+ * the edges whose two faces differ in label, in the face adjacency's
+ * ascending edge-key order; the shell (ns) and fracture (nf) macro normals,
+ * area-weighted ball normals over the mask's faces between macro_inner t and
+ * macro_outer t of the point (the whole macro_outer ball where that is empty
+ * or gives a normal shorter than 0.5; zero where the mask has no face); the
+ * frame f = nf - (nf . ns) ns normalised; valid = |ns|, |nf|, |ns x f| > 0.5;
+ * the dihedral acos(ns . nf) in degrees; and the hypothesis subset `sub`, the
+ * valid lowest-index representatives of the brk_voxel t voxels, ascending.
+ * Outputs: *count points, and when capacity >= *count: p, ns, nf, f (xyz
+ * each), dih, valid, sub (room for *count; *n_sub written). capacity = 0
+ * asks for the count alone; a non-zero capacity below it is refused. Points,
+ * normals, frames, validity and subset are bit-identical to the sequential
+ * restatement (ball sums in ascending face order); dih to the device acos. */
+int sherd_breaklines(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f, uint32_t nf,
+                     const uint8_t *frac, double t, double macro_inner, double macro_outer,
+                     double brk_voxel, uint32_t capacity, double *p, double *ns, double *nfr,
+                     double *fr, double *dih, uint8_t *valid, uint32_t *sub, uint32_t *n_sub,
+                     uint32_t *count);
+
 /* ---- stage 1: hypotheses, coarse score, suppression (R 5.1-5.5) --------- */
 
 /* One fragment's breakline as R 5 reads it (hypotheses.rs:53-82): n points

@@ -156,6 +156,9 @@ def lib() -> C.CDLL:
                               C.POINTER(SegParams), vp, U8P, C.POINTER(SegInfo),
                               C.POINTER(SegTrace)]),
         "or_vertex_normals": (None, [F64P, C.c_uint32, U32P, C.c_uint32, F64P]),
+        "or_ball_normals": (None, [F64P, C.c_uint32, F64P, F64P, F64P, C.c_uint32, C.c_double,
+                                   F64P, U8P]),
+        "or_voxel_representatives": (C.c_uint32, [F64P, C.c_uint32, C.c_double, U32P]),
         "or_place_fused": (None, [F64P, C.c_uint32, F64P, C.c_int, F64P]),
     }
     for name, (res, args) in sig.items():
@@ -767,3 +770,152 @@ def stage1_ladder(source, target: Cloud, inits, scales: Scales):
                         point_to_point=True)
         poses = np.stack([np.array(r.transform[:]).reshape(4, 4) for r in regs])
     return poses
+
+
+# ---- R 3.5: breaklines, frames and samples (breakline.rs, samples.rs) --------------------------
+
+MACRO_INNER, MACRO_OUTER, BRK_VOXEL = 0.15, 0.60, 0.5   # breakline.rs:72-76
+FRAME_FLOOR, VALID_MIN = 1e-9, 0.5                      # breakline.rs:78-80
+MARGIN_INNER, MARGIN_OUTER = 0.12, 1.5                  # samples.rs:82-84
+
+
+def _dot3(a, b):
+    return (a[:, 0] * b[:, 0] + a[:, 1] * b[:, 1]) + a[:, 2] * b[:, 2]
+
+
+def _norm3(a):
+    return np.sqrt(_dot3(a, a))
+
+
+def face_adjacency_edges(f):
+    """face_adjacency (adjacency.rs:43-51, 138-160): the face pairs (fa, fb) sharing an edge and
+    the edge's two vertices (lo, hi), in ascending edge-key order (slot-major, stable)."""
+    f = np.asarray(f, np.int64).reshape(-1, 3)
+    nf = len(f)
+    keys, ends = [], []
+    for x, y in ((0, 1), (1, 2), (2, 0)):
+        lo, hi = np.minimum(f[:, x], f[:, y]), np.maximum(f[:, x], f[:, y])
+        keys.append(lo * (1 << 32) + hi)
+        ends.append(np.stack([lo, hi], axis=1))
+    keys, ends = np.concatenate(keys), np.concatenate(ends)
+    order = np.argsort(keys, kind="stable")
+    k = keys[order]
+    w = np.flatnonzero(k[:-1] == k[1:])
+    return order[w] % nf, order[w + 1] % nf, ends[order[w], 0], ends[order[w], 1]
+
+
+def ball_normals(points, normals, areas, queries, radius):
+    """ball_normals (segment.rs:267-296) of `queries` over `points`: (unit normals, non-empty)."""
+    p, q = f64(points).reshape(-1, 3), f64(queries).reshape(-1, 3)
+    out = np.zeros((len(q), 3))
+    has = np.zeros(len(q), np.uint8)
+    if len(p) and len(q):
+        lib().or_ball_normals(p, len(p), f64(normals).reshape(-1, 3), f64(areas).reshape(-1), q,
+                              len(q), float(radius), out, has)
+    return out, has
+
+
+def voxel_representatives(points, spacing):
+    """voxel_representatives (segment.rs:217-259): the lowest index per voxel, ascending."""
+    p = f64(points).reshape(-1, 3)
+    out = np.empty(max(len(p), 1), np.uint32)
+    k = lib().or_voxel_representatives(p, len(p), float(spacing), out) if len(p) else 0
+    return out[:k].copy()
+
+
+def breaklines(v, f, frac, t, macro_inner=MACRO_INNER, macro_outer=MACRO_OUTER,
+               brk_voxel=BRK_VOXEL):
+    """breakline::build (breakline.rs:207-300) in f64: the midpoints of the edges whose two faces
+    differ in label, in adjacency order; the shell and fracture macro normals over the faces
+    between macro_inner t and macro_outer t of each point (the whole macro_outer ball where the
+    annulus is empty); f = nf - (nf.ns) ns normalised; the validity mask; the hypothesis subset
+    (voxel representatives at brk_voxel t that are valid); and the dihedral in degrees
+    (breakline.rs:189-195). Returns a dict of arrays."""
+    v = f64(v).reshape(-1, 3)
+    f = np.asarray(f, np.int64).reshape(-1, 3)
+    frac = np.asarray(frac).astype(bool)
+    normals, areas, cent = face_geometry(v, f)
+    fa, fb, lo, hi = face_adjacency_edges(f)
+    change = frac[fa] != frac[fb]
+    a, b = v[lo[change]], v[hi[change]]
+    p = 0.5 * (a + b)
+    n = len(p)
+    empty = {"p": p, "ns": np.zeros((n, 3)), "nf": np.zeros((n, 3)), "f": np.zeros((n, 3)),
+             "valid": np.zeros(n, bool), "sub": np.zeros(0, np.uint32), "dih": np.zeros(n)}
+    if n == 0:
+        return empty
+    inner, outer = macro_inner * t, macro_outer * t
+    _, dist = Cloud(p).nearest_below(cent, inner)
+
+    def macro(fracture):
+        every = np.flatnonzero(frac == fracture)
+        out = np.zeros((n, 3))
+        if len(every) == 0:
+            return out
+        far = every[dist[every] >= inner]
+        if len(far):
+            out, _ = ball_normals(cent[far], normals[far], areas[far], p, outer)
+        bad = np.flatnonzero(_norm3(out) < VALID_MIN)
+        if len(bad):
+            out[bad], _ = ball_normals(cent[every], normals[every], areas[every], p[bad], outer)
+        return out
+
+    ns, nf = macro(False), macro(True)
+    d = _dot3(nf, ns)
+    fr = nf - d[:, None] * ns
+    fr = fr / np.maximum(_norm3(fr), FRAME_FLOOR)[:, None]
+    t_ = np.stack([ns[:, 1] * fr[:, 2] - ns[:, 2] * fr[:, 1], ns[:, 2] * fr[:, 0] - ns[:, 0] * fr[:, 2],
+                   ns[:, 0] * fr[:, 1] - ns[:, 1] * fr[:, 0]], axis=1)
+    valid = (_norm3(ns) > VALID_MIN) & (_norm3(nf) > VALID_MIN) & (_norm3(t_) > VALID_MIN)
+    rep = voxel_representatives(p, brk_voxel * t)
+    sub = rep[valid[rep]]
+    dih = np.degrees(np.arccos(np.clip(_dot3(ns, nf), -1.0, 1.0)))
+    return {"p": p, "ns": ns, "nf": nf, "f": fr, "valid": valid, "sub": sub.astype(np.uint32),
+            "dih": dih}
+
+
+def sample_on_faces(rng, v, f, areas, faces, n):
+    """samples::sample_on_faces (samples.rs:281-305) with numpy's generator: the face picks
+    (searchsorted of the normalised cumulative areas, side right, n uniforms), then n uniforms
+    for u and n for v, folded where u + v > 1. Returns (points, picks, u, v) (u, v unfolded)."""
+    faces = np.asarray(faces, np.int64)
+    if len(faces) == 0 or n == 0:
+        return np.zeros((0, 3)), np.zeros(0, np.int64), np.zeros(0), np.zeros(0)
+    w = areas[faces] / areas[faces].sum()
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    picks = faces[np.minimum(np.searchsorted(cdf, rng.random(n), side="right"), len(faces) - 1)]
+    u, vv = rng.random(n), rng.random(n)
+    fold = u + vv > 1.0
+    al, be = np.where(fold, 1.0 - u, u), np.where(fold, 1.0 - vv, vv)
+    o, pu, pv = v[f[picks, 0]], v[f[picks, 1]], v[f[picks, 2]]
+    pts = (o + al[:, None] * (pu - o)) + be[:, None] * (pv - o)
+    return pts, picks, u, vv
+
+
+def samples(v, f, frac, brk_points, t, seed=0, surface_points=20000, frac_per_t2=150.0,
+            min_frac=5000, max_frac=12000, margin_points=6000):
+    """samples::build (samples.rs:201-248) with the reference's one numpy stream per fragment
+    (samples.rs:33-42): the surface samples, the fracture samples
+    clip(150 A_frac / t^2, 5000, 12000), and the shell margin 0.12 t < d_brk < 1.5 t thinned to
+    margin_points by choice(..., replace=False), sorted."""
+    v = f64(v).reshape(-1, 3)
+    f = np.asarray(f, np.int64).reshape(-1, 3)
+    frac = np.asarray(frac).astype(bool)
+    _, areas, _ = face_geometry(v, f)
+    rng = np.random.default_rng(seed)
+    s, sp, su, sv = sample_on_faces(rng, v, f, areas, np.arange(len(f)), surface_points)
+    fr = np.flatnonzero(frac)
+    raw = frac_per_t2 * areas[fr].sum() / (t * t)
+    n_frac = min_frac if np.isnan(raw) else int(np.clip(raw, min_frac, max_frac))
+    pf, fp, fu, fv = sample_on_faces(rng, v, f, areas, fr, n_frac)
+    bp = f64(brk_points).reshape(-1, 3)
+    if len(bp):
+        _, d_brk = Cloud(bp).nearest_below(s, MARGIN_OUTER * t)
+    else:
+        d_brk = np.full(len(s), np.inf)
+    margin = np.flatnonzero(~frac[sp] & (d_brk > MARGIN_INNER * t) & (d_brk < MARGIN_OUTER * t))
+    if margin_points and len(margin) > margin_points:
+        margin = np.sort(rng.choice(margin, margin_points, replace=False))
+    return {"S": s, "sp": sp, "S_u": su, "S_v": sv, "Pf": pf, "fp": fp, "Pf_u": fu, "Pf_v": fv,
+            "margin_idx": margin}

@@ -2211,4 +2211,30 @@ void or_place_fused(const double *pts, uint32_t n, const double *t, int rotate_o
   }
 }
 
+// ball_normals (segment.rs:267-296) of arbitrary query points over the n
+// points `p` (with their unit normals and areas): the balls of radius r, each
+// summed in ascending point order; has[q] = 0 for an empty ball.
+void or_ball_normals(const double *p, uint32_t n, const double *normals, const double *areas,
+                     const double *queries, uint32_t nq, double radius, double *out3,
+                     uint8_t *has) {
+  BallGrid grid(p, n, std::max(radius, 1e-300));
+  std::vector<std::array<double, 3>> q(nq), out;
+  for (uint32_t i = 0; i < nq; ++i)
+    for (int k = 0; k < 3; ++k) q[i][k] = queries[3 * size_t(i) + k];
+  std::vector<uint8_t> h;
+  ball_normals(grid, q, normals, areas, radius, out, h);
+  for (uint32_t i = 0; i < nq; ++i) {
+    for (int k = 0; k < 3; ++k) out3[3 * size_t(i) + k] = out[i][k];
+    has[i] = h[i];
+  }
+}
+
+// voxel_representatives (segment.rs:217-259): writes the ascending
+// representatives (room for n) and returns their count.
+uint32_t or_voxel_representatives(const double *p, uint32_t n, double spacing, uint32_t *out) {
+  std::vector<uint32_t> rep = voxel_representatives(p, n, spacing);
+  std::copy(rep.begin(), rep.end(), out);
+  return uint32_t(rep.size());
+}
+
 }  // extern "C"

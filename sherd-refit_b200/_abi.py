@@ -194,6 +194,9 @@ _SIGNATURES = {
                                           C.c_uint32, U32P, C.c_uint32, C.c_double, VP, F64P,
                                           F64P, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
                                           VP, VP, VP, VP, C.POINTER(C.c_uint32)]),
+    "sherd_breaklines": (C.c_int, [VP, F64P, C.c_uint32, U32P, C.c_uint32, U8P, C.c_double,
+                                   C.c_double, C.c_double, C.c_double, C.c_uint32, VP, VP, VP, VP,
+                                   VP, VP, VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "sherd_order_by_score": (C.c_int, [F64P, C.c_uint32, C.c_uint32, VP, C.POINTER(C.c_uint32)]),
     "sherd_nms": (C.c_int, [U32P, C.c_uint32, F64P, F64P, C.c_uint32, C.c_double, C.c_uint32,
                             C.c_double, VP, C.POINTER(C.c_uint32)]),

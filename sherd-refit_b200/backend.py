@@ -345,6 +345,32 @@ class Context:
                                             values, grads))
         return values, grads
 
+    # -- R 3.5 -----------------------------------------------------------------------------------
+    def breaklines(self, v, f, frac, t, macro_inner=0.15, macro_outer=0.60, brk_voxel=0.5):
+        """breakline::build (breakline.rs:207-300) on the device: a dict of p, ns, nf, f (n, 3),
+        dih (n,), valid (n,) bool and sub (ascending)."""
+        v, f = _f64(v), _u32(f, (-1, 3))
+        frac = np.ascontiguousarray(np.asarray(frac).astype(bool), np.uint8).reshape(-1)
+        if len(frac) != len(f):
+            raise A.SherdError(A.E_INVALID, "one label per face")
+        args = (self.h, v, len(v), f, len(f), frac, float(t), float(macro_inner),
+                float(macro_outer), float(brk_voxel))
+        count, n_sub = C.c_uint32(0), C.c_uint32(0)
+        check(self.h, A.lib().sherd_breaklines(*args, 0, None, None, None, None, None, None,
+                                               None, C.byref(n_sub), C.byref(count)))
+        n = count.value
+        out = {"p": np.zeros((n, 3)), "ns": np.zeros((n, 3)), "nf": np.zeros((n, 3)),
+               "f": np.zeros((n, 3)), "dih": np.zeros(n), "valid": np.zeros(n, np.uint8),
+               "sub": np.zeros(max(n, 1), np.uint32)}
+        if n:
+            check(self.h, A.lib().sherd_breaklines(
+                *args, n, ptr(out["p"]), ptr(out["ns"]), ptr(out["nf"]), ptr(out["f"]),
+                ptr(out["dih"]), ptr(out["valid"]), ptr(out["sub"]), C.byref(n_sub),
+                C.byref(count)))
+        out["sub"] = out["sub"][:n_sub.value].copy()
+        out["valid"] = out["valid"].astype(bool)
+        return out
+
     # -- stage 1 ---------------------------------------------------------------------------------
     def hypotheses_coarse(self, frames_a, frames_b, ia, ib, dihedral_tol, target: "Cloud", q, qn,
                           delta, normal_agree=0.7):

@@ -29,6 +29,7 @@
 #include "segment.cuh"
 #include "refine.cuh"
 #include "stage1.cuh"
+#include "preprocess.cuh"
 
 using namespace sherd;
 
@@ -2368,6 +2369,257 @@ int sherd_nms(const uint32_t *order, uint32_t n_order, const double *poses, cons
   }
   *n_kept = m;
   return SHERD_OK;
+}
+
+
+}  // extern "C"
+
+// ---- R 3.5.3-3.5.5: breaklines and their frames --------------------------------
+
+namespace {
+
+// The entries of `in` (or 0..n-1 when `in` is null) whose flag is set, in
+// order; `count` receives how many.
+int select_flagged(sherd_ctx *ctx, const uint32_t *in, const uint8_t *flags, uint32_t n,
+                   DBuf<uint32_t> &out, uint32_t &count) {
+  cudaStream_t s = ctx->stream;
+  count = 0;
+  CK(out.alloc(std::max<uint32_t>(n, 1)));
+  if (n == 0) return SHERD_OK;
+  DBuf<uint32_t> iota, cnt;
+  if (!in) {
+    CK(iota.alloc(n));
+    k_iota<<<blocks_for(n), 256, 0, s>>>(iota.p, n);
+    CK(cudaGetLastError());
+    in = iota.p;
+  }
+  CK(cnt.alloc(1));
+  size_t bytes = 0;
+  CK(cub::DeviceSelect::Flagged(nullptr, bytes, in, flags, out.p, cnt.p, int(n), s));
+  DBuf<unsigned char> tmp;
+  CK(tmp.alloc(std::max<size_t>(bytes, 1)));
+  CK(cub::DeviceSelect::Flagged(tmp.p, bytes, in, flags, out.p, cnt.p, int(n), s));
+  CK(cudaMemcpyAsync(&count, cnt.p, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return SHERD_OK;
+}
+
+// voxel_representatives (segment.rs:217-259) of n device points at `spacing`:
+// the lowest index of every occupied voxel, ascending (segmentation's grid).
+int voxel_reps(sherd_ctx *ctx, const double *pts, uint32_t n, double spacing,
+               DBuf<uint32_t> &rep, uint32_t &n_rep) {
+  cudaStream_t s = ctx->stream;
+  n_rep = 0;
+  CK(rep.alloc(std::max<uint32_t>(n, 1)));
+  if (n == 0) return SHERD_OK;
+  DBuf<unsigned long long> mb, keys, keys2;
+  DBuf<uint32_t> idx, idx2, unsorted;
+  DBuf<uint8_t> heads;
+  CK(mb.alloc(3));
+  CK(cudaMemsetAsync(mb.p, 0xFF, 3 * sizeof(unsigned long long), s));
+  k_min_bound<<<std::min(blocks_for(n), 1024u), 256, 0, s>>>(pts, n, mb.p);
+  CK(keys.alloc(n));
+  CK(keys2.alloc(n));
+  CK(idx.alloc(n));
+  CK(idx2.alloc(n));
+  k_voxel_keys<<<blocks_for(n), 256, 0, s>>>(pts, n, mb.p, spacing, keys.p, idx.p, ctx->d_status);
+  CK(cudaGetLastError());
+  int rc = radix_sort_pairs(ctx, keys.p, keys2.p, idx.p, idx2.p, n, 63);
+  if (rc) return rc;
+  CK(heads.alloc(n));
+  k_run_heads<<<blocks_for(n), 256, 0, s>>>(keys2.p, n, heads.p);
+  CK(cudaGetLastError());
+  if ((rc = select_flagged(ctx, idx2.p, heads.p, n, unsorted, n_rep))) return rc;
+  if (n_rep == 0) return SHERD_OK;
+  size_t bytes = 0;
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, unsorted.p, rep.p, int(n_rep), 0, 32, s));
+  DBuf<unsigned char> tmp;
+  CK(tmp.alloc(std::max<size_t>(bytes, 1)));
+  CK(cub::DeviceRadixSort::SortKeys(tmp.p, bytes, unsorted.p, rep.p, int(n_rep), 0, 32, s));
+  CK(cudaStreamSynchronize(s));
+  return SHERD_OK;
+}
+
+// One macro normal (breakline.rs:307-337) of the n breakline points `p` into
+// out3: the area-weighted ball normals over the faces of the mask at distance
+// >= inner, then, for the points that got a normal shorter than 0.5, over
+// every face of the mask; zeros when the mask is empty.
+int macro_normals(sherd_ctx *ctx, const double *p, uint32_t n, const double *cent,
+                  const double *normals, const double *areas, const uint8_t *frac, uint32_t nf,
+                  const double *dist, uint8_t fracture, double inner, double outer, float pad,
+                  double *out3) {
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemsetAsync(out3, 0, sizeof(double) * 3 * size_t(n), s));
+  DBuf<uint8_t> every, far, flag, bad_flag;
+  CK(every.alloc(nf));
+  CK(far.alloc(nf));
+  k_macro_masks<<<blocks_for(nf), 256, 0, s>>>(frac, fracture, dist, inner, nf, every.p, far.p);
+  CK(cudaGetLastError());
+  DBuf<uint32_t> all_idx, far_idx, queries, bad_idx;
+  uint32_t n_all = 0, n_far = 0, n_bad = 0;
+  int rc = select_flagged(ctx, nullptr, every.p, nf, all_idx, n_all);
+  if (rc) return rc;
+  if (n_all == 0) return SHERD_OK;
+  if ((rc = select_flagged(ctx, nullptr, far.p, nf, far_idx, n_far))) return rc;
+  CK(flag.alloc(n));
+  // One ball pass over the faces `sel` (k of them) for the queries q_idx.
+  auto pass = [&](const uint32_t *sel, uint32_t k, const uint32_t *q_idx, uint32_t nq,
+                  double *res3) -> int {
+    DBuf<double> c, nn, a;
+    CK(c.alloc(size_t(3) * k));
+    CK(nn.alloc(size_t(3) * k));
+    CK(a.alloc(k));
+    k_gather_points<<<blocks_for(k), 256, 0, s>>>(cent, sel, k, c.p);
+    k_gather_points<<<blocks_for(k), 256, 0, s>>>(normals, sel, k, nn.p);
+    k_gather1<<<blocks_for(k), 256, 0, s>>>(areas, sel, k, a.p);
+    CK(cudaGetLastError());
+    sherd_cloud sub;
+    int r = cloud_build_dev(ctx, c.p, nullptr, k, pad, &sub);
+    if (r) return r;
+    if ((r = ball_pass(ctx, sub.view, p, q_idx, nq, outer, BALL_NORMALS, nn.p, a.p, nullptr, res3,
+                       flag.p)))
+      return r;
+    CK(cudaStreamSynchronize(s));
+    return SHERD_OK;
+  };
+  CK(queries.alloc(n));
+  k_iota<<<blocks_for(n), 256, 0, s>>>(queries.p, n);
+  CK(cudaGetLastError());
+  if (n_far && (rc = pass(far_idx.p, n_far, queries.p, n, out3))) return rc;
+  CK(bad_flag.alloc(n));
+  k_short_normals<<<blocks_for(n), 256, 0, s>>>(out3, n, bad_flag.p);
+  CK(cudaGetLastError());
+  if ((rc = select_flagged(ctx, nullptr, bad_flag.p, n, bad_idx, n_bad))) return rc;
+  if (n_bad == 0) return SHERD_OK;
+  DBuf<double> fallback;
+  CK(fallback.alloc(size_t(3) * n_bad));
+  if ((rc = pass(all_idx.p, n_all, bad_idx.p, n_bad, fallback.p))) return rc;
+  k_scatter3<<<blocks_for(n_bad), 256, 0, s>>>(fallback.p, bad_idx.p, n_bad, out3);
+  CK(cudaGetLastError());
+  return SHERD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sherd_breaklines(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f, uint32_t nf,
+                     const uint8_t *frac, double t, double macro_inner, double macro_outer,
+                     double brk_voxel, uint32_t capacity, double *p, double *ns, double *nfr,
+                     double *fr, double *dih, uint8_t *valid, uint32_t *sub, uint32_t *n_sub,
+                     uint32_t *count) {
+  if (!ctx || !count || !n_sub || ((!v || !f || !frac) && nf) ||
+      (capacity && (!p || !ns || !nfr || !fr || !dih || !valid || !sub)))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  *count = 0;
+  *n_sub = 0;
+  if (!(t > 0.0) || !std::isfinite(t) || !(macro_inner >= 0.0) || !(macro_outer > 0.0) ||
+      !(brk_voxel > 0.0))
+    return fail(ctx, SHERD_E_INVALID, "t, the macro radii and the voxel must be positive");
+  if (uint64_t(nf) * 3u >= (uint64_t(1) << 31)) return fail(ctx, SHERD_E_INVALID, "too many faces");
+  for (size_t i = 0; i < size_t(3) * nf; ++i)
+    if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
+  double mag = 1.0;
+  for (size_t i = 0; i < size_t(3) * nv; ++i) {
+    if (!std::isfinite(v[i])) return fail(ctx, SHERD_E_INVALID, "non-finite vertex");
+    mag = std::max(mag, std::fabs(v[i]));
+  }
+  if (nf == 0) return SHERD_OK;
+  const float pad = float(1e-6 * mag);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int rc = begin(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  DBuf<double> dv, normals, areas, cent;
+  DBuf<uint32_t> df;
+  DBuf<uint8_t> dfrac;
+  if ((rc = upload(ctx, dv, v, size_t(3) * nv)) || (rc = upload(ctx, df, f, size_t(3) * nf)) ||
+      (rc = upload(ctx, dfrac, frac, size_t(nf))))
+    return rc;
+  CK(normals.alloc(size_t(3) * nf));
+  CK(areas.alloc(nf));
+  CK(cent.alloc(size_t(3) * nf));
+  k_face_geometry<<<blocks_for(nf), 256, 0, s>>>(dv.p, df.p, nf, normals.p, areas.p, cent.p);
+  CK(cudaGetLastError());
+
+  // R 3.5.3 the points: the edges whose two faces differ in label, in the
+  // adjacency's ascending edge-key order, at their midpoints.
+  const uint32_t m = 3 * nf, n_pairs = m - 1;
+  DBuf<unsigned long long> ek, ek2;
+  DBuf<uint32_t> ep, ep2, fa, fb, edges;
+  CK(ek.alloc(m));
+  CK(ek2.alloc(m));
+  CK(ep.alloc(m));
+  CK(ep2.alloc(m));
+  k_edge_keys<<<blocks_for(nf), 256, 0, s>>>(df.p, nf, ek.p, ep.p);
+  CK(cudaGetLastError());
+  if ((rc = radix_sort_pairs(ctx, ek.p, ek2.p, ep.p, ep2.p, m, 64))) return rc;
+  CK(fa.alloc(n_pairs));
+  CK(fb.alloc(n_pairs));
+  k_face_pairs<<<blocks_for(m), 256, 0, s>>>(ek2.p, ep2.p, m, nf, fa.p, fb.p);
+  DBuf<uint8_t> bflag;
+  CK(bflag.alloc(n_pairs));
+  k_brk_flags<<<blocks_for(n_pairs), 256, 0, s>>>(fa.p, fb.p, n_pairs, dfrac.p, bflag.p);
+  CK(cudaGetLastError());
+  uint32_t n = 0;
+  if ((rc = select_flagged(ctx, nullptr, bflag.p, n_pairs, edges, n))) return rc;
+  *count = n;
+  if (n == 0 || capacity == 0) return finish(ctx, "breaklines", nf, true);
+  if (capacity < n) {
+    rc = finish(ctx, "breaklines", nf, true);
+    if (rc) return rc;
+    return fail(ctx, SHERD_E_INVALID, "capacity below the breakline point count");
+  }
+  DBuf<double> dp, dns, dnf, dfr, ddih, dist;
+  DBuf<uint32_t> nn_idx;
+  CK(dp.alloc(size_t(3) * n));
+  k_brk_points<<<blocks_for(n), 256, 0, s>>>(ek2.p, edges.p, n, dv.p, dp.p);
+  CK(cudaGetLastError());
+
+  // R 3.5.4 each centroid's distance to the breakline, needed only below
+  // `inner` (the bounded search reports +inf beyond it), then the macro
+  // normals of the shell and of the fracture, and the frames.
+  const double inner = macro_inner * t, outer = macro_outer * t;
+  sherd_cloud brk;
+  if ((rc = cloud_build_dev(ctx, dp.p, nullptr, n, pad, &brk))) return rc;
+  CK(dist.alloc(nf));
+  CK(nn_idx.alloc(nf));
+  k_nn_below<<<blocks_for(nf, 128), 128, 0, s>>>(brk.view, cent.p, nf, inner, nn_idx.p, dist.p,
+                                                  ctx->d_status);
+  CK(cudaGetLastError());
+  CK(dns.alloc(size_t(3) * n));
+  CK(dnf.alloc(size_t(3) * n));
+  if ((rc = macro_normals(ctx, dp.p, n, cent.p, normals.p, areas.p, dfrac.p, nf, dist.p, 0, inner,
+                          outer, pad, dns.p)) ||
+      (rc = macro_normals(ctx, dp.p, n, cent.p, normals.p, areas.p, dfrac.p, nf, dist.p, 1, inner,
+                          outer, pad, dnf.p)))
+    return rc;
+  DBuf<uint8_t> dvalid, rflag;
+  CK(dfr.alloc(size_t(3) * n));
+  CK(ddih.alloc(n));
+  CK(dvalid.alloc(n));
+  k_brk_frames<<<blocks_for(n), 256, 0, s>>>(dns.p, dnf.p, n, dfr.p, dvalid.p, ddih.p);
+  CK(cudaGetLastError());
+
+  // R 3.5.5 the hypothesis subset: the valid voxel representatives.
+  DBuf<uint32_t> rep, dsub;
+  uint32_t n_rep = 0, ns_count = 0;
+  if ((rc = voxel_reps(ctx, dp.p, n, brk_voxel * t, rep, n_rep))) return rc;
+  CK(rflag.alloc(std::max<uint32_t>(n_rep, 1)));
+  if (n_rep) {
+    k_valid_reps<<<blocks_for(n_rep), 256, 0, s>>>(rep.p, n_rep, dvalid.p, rflag.p);
+    CK(cudaGetLastError());
+  }
+  if ((rc = select_flagged(ctx, rep.p, rflag.p, n_rep, dsub, ns_count))) return rc;
+  *n_sub = ns_count;
+  CK(cudaMemcpyAsync(p, dp.p, sizeof(double) * 3 * size_t(n), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ns, dns.p, sizeof(double) * 3 * size_t(n), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(nfr, dnf.p, sizeof(double) * 3 * size_t(n), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(fr, dfr.p, sizeof(double) * 3 * size_t(n), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(dih, ddih.p, sizeof(double) * size_t(n), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(valid, dvalid.p, size_t(n), cudaMemcpyDeviceToHost, s));
+  if (ns_count) CK(cudaMemcpyAsync(sub, dsub.p, 4 * size_t(ns_count), cudaMemcpyDeviceToHost, s));
+  return finish(ctx, "breaklines", nf, true);
 }
 
 }  // extern "C"

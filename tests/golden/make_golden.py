@@ -18,6 +18,9 @@ without the reference tree present:
   at the pair's own `t` (`md.Pf`, `md.fp`, `md.S`, `md.sp`, `md.margin_idx`, `md.brk_P`,
   `md.brk_ns`), the pair's `scales.json`, the starts `s1.T[nms2.kept]`, the four rung poses
   `s2.T_reg1..s2.T_frac2`, the scores `s2.scores.json` and the verdicts `s2.accepted`;
+* R 3.5 at the pair's t (`fragment/breakline.rs`, `fragment/samples.rs`): the breakline's
+  fracture macro normals `md.brk_nf` and validity `md.valid`, the sample faces `md.sp`, `md.fp`,
+  the uniforms `md.S_u/S_v`, `md.Pf_u/Pf_v`, the margin `md.margin_idx` and `md.params.json`;
 * stage 1 (R 5.1-5.5, `hypotheses.rs`, `coarse.rs`, `nms.rs`, `ladder.rs`): the breakline
   frames' in-plane axes `md.brk_f` and dihedrals `md.brk_dih`, the subsets and kept pairs
   `hyp.ia/ib/pa/pb`, the probe `coarse.idx` and every hypothesis's score `coarse.cs`, both
@@ -50,6 +53,8 @@ from pathlib import Path
 import numpy as np
 
 PIECES = ("pieceA", "pieceB")
+MD_PARAMS = ("t", "seed", "surface_points", "frac_per_t2", "min_frac_points", "max_frac_points",
+             "margin_points", "macro_inner", "macro_outer", "brk_voxel")
 PAIR = "pieceA__pieceB"
 SCORE_KEYS = (
     "tightA", "tightB", "tight", "gapA", "gapB", "gap", "contactA", "contactB", "contact",
@@ -176,6 +181,15 @@ def main(reference: Path) -> None:
         out[p + "brk_sub"] = np.load(md / "md.brk_sub.npy").astype(np.uint32)
         out[p + "brk_f"] = np.load(md / "md.brk_f.npy")
         out[p + "brk_dih"] = np.load(md / "md.brk_dih.npy")
+        out[p + "brk_nf"] = np.load(md / "md.brk_nf.npy")
+        out[p + "brk_valid"] = np.load(md / "md.valid.npy").astype(np.uint8)
+        out[p + "sp"] = np.load(md / "md.sp.npy").astype(np.uint32)
+        out[p + "fp"] = np.load(md / "md.fp.npy").astype(np.uint32)
+        out[p + "S_uv"] = np.stack([np.load(md / "md.S_u.npy"), np.load(md / "md.S_v.npy")])
+        out[p + "Pf_uv"] = np.stack([np.load(md / "md.Pf_u.npy"), np.load(md / "md.Pf_v.npy")])
+        out[p + "margin_idx"] = np.load(md / "md.margin_idx.npy").astype(np.uint32)
+        mdp = json.loads((md / "md.params.json").read_text())
+        out[p + "md_params"] = np.array([mdp[k] for k in MD_PARAMS], dtype=np.float64)
         nf_ = fn[fp]
         pm = s[margin_idx]
         nm = fn[sp[margin_idx]]
