@@ -469,6 +469,25 @@ int sherd_adjoint(sherd_ctx *ctx, sherd_pair *const *edges, uint32_t n_edges,
                   const double *poses, const double *inverses, uint32_t n_poses,
                   const sherd_adjoint_options *opt, double *values, double *grads);
 
+/* ---- io::load_mesh (io/mod.rs:114-137, io/ply.rs, mesh/clean.rs) -------- */
+
+/* A mesh read from a file, in host memory. */
+typedef struct sherd_host_mesh sherd_host_mesh;
+
+/* Reads a PLY file (ASCII, binary little- or big-endian; any numeric property
+ * types; x, y, z widened to f64; the vertex_indices or vertex_index list,
+ * polygons as the fan (i0, i_{k-1}, i_k), faces under three corners dropped;
+ * other elements and properties read past) and cleans it as mesh/clean.rs:
+ * 138-142: duplicate vertices merged onto their first occurrence (+0 = -0, NaN
+ * never equal), faces with a repeated corner dropped, unreferenced vertices
+ * removed. *nv, *nf receive the sizes; SHERD_E_EMPTY when no triangle is
+ * left, SHERD_E_INVALID on a malformed file (message in
+ * sherd_last_error(NULL)). Host code, no device. */
+int sherd_mesh_read(const char *path, sherd_host_mesh **out, uint32_t *nv, uint32_t *nf);
+/* Copies the mesh out: v receives 3 nv doubles, f 3 nf indices. */
+int sherd_host_mesh_copy(const sherd_host_mesh *m, double *v, uint32_t *f);
+int sherd_host_mesh_free(sherd_host_mesh *m);
+
 /* ---- R 3.5.3-3.5.5: breaklines and their frames (fragment/breakline.rs) --- */
 
 /* breakline::build (breakline.rs:207-300) in f64 on one labelled working mesh

@@ -12,7 +12,7 @@ from ._abi import (AdjointOptions, Candidate, IcpOptions, InsideOutcome, Params,
                    REDUCE_MIN, SCHED_BATCHED, SCHED_PLAIN, exported_symbols, lib)
 from .backend import (CANDIDATE, WORK_ITEM, Batch, Cloud, CoarseBatch, Context, CudaExecutor,
                       DistBatch, IcpBatch, InsideBatch, Mesh, Pair, Surfaces, accept, candidates,
-                      default_params, scales_for_pair, work_item_array, work_items)
+                      default_params, read_mesh, scales_for_pair, work_item_array, work_items)
 
 __all__ = [
     "AdjointOptions", "Batch", "CANDIDATE", "WORK_ITEM", "candidates", "work_item_array",
@@ -20,7 +20,8 @@ __all__ = [
     "IcpOptions",
     "InsideBatch", "InsideOutcome", "Mesh", "Pair", "Params", "Registration", "Scales", "Scores",
     "SegInfo", "SegParams", "SherdError", "Surfaces", "WorkItem", "REDUCE_ALL", "REDUCE_MIN", "SCHED_BATCHED",
-    "SCHED_PLAIN", "accept", "default_params", "exported_symbols", "lib", "scales_for_pair",
+    "SCHED_PLAIN", "accept", "default_params", "exported_symbols", "lib", "read_mesh",
+    "scales_for_pair",
     "seg_params_default", "work_items",
 ]
 

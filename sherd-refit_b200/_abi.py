@@ -194,6 +194,10 @@ _SIGNATURES = {
                                           C.c_uint32, U32P, C.c_uint32, C.c_double, VP, F64P,
                                           F64P, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
                                           VP, VP, VP, VP, C.POINTER(C.c_uint32)]),
+    "sherd_mesh_read": (C.c_int, [C.c_char_p, C.POINTER(VP), C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint32)]),
+    "sherd_host_mesh_copy": (C.c_int, [VP, F64P, U32P]),
+    "sherd_host_mesh_free": (C.c_int, [VP]),
     "sherd_breaklines": (C.c_int, [VP, F64P, C.c_uint32, U32P, C.c_uint32, U8P, C.c_double,
                                    C.c_double, C.c_double, C.c_double, C.c_uint32, VP, VP, VP, VP,
                                    VP, VP, VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),

@@ -75,6 +75,23 @@ def nms(order, poses, score, trans_tol: float, topk: int, floor: float) -> np.nd
     return kept[:n.value].copy()
 
 
+def read_mesh(path) -> tuple[np.ndarray, np.ndarray]:
+    """io::load_mesh (io/mod.rs:114-137) for a PLY file: the cleaned (v f64 (nv, 3), f u32
+    (nf, 3)). Raises SherdError on a malformed file or one with no triangle."""
+    h, nv, nf = C.c_void_p(), C.c_uint32(0), C.c_uint32(0)
+    rc = A.lib().sherd_mesh_read(str(path).encode(), C.byref(h), C.byref(nv), C.byref(nf))
+    if rc:
+        msg = A.lib().sherd_last_error(None)
+        raise A.SherdError(rc, msg.decode() if msg else "sherd_mesh_read")
+    try:
+        v = np.empty((nv.value, 3))
+        f = np.empty((nf.value, 3), np.uint32)
+        A.lib().sherd_host_mesh_copy(h, v, f)
+    finally:
+        A.lib().sherd_host_mesh_free(h)
+    return v, f
+
+
 class _Handle:
     _free = ""
 

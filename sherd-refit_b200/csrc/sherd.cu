@@ -30,6 +30,7 @@
 #include "refine.cuh"
 #include "stage1.cuh"
 #include "preprocess.cuh"
+#include "meshio.h"
 
 using namespace sherd;
 
@@ -2620,6 +2621,56 @@ int sherd_breaklines(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_
   CK(cudaMemcpyAsync(valid, dvalid.p, size_t(n), cudaMemcpyDeviceToHost, s));
   if (ns_count) CK(cudaMemcpyAsync(sub, dsub.p, 4 * size_t(ns_count), cudaMemcpyDeviceToHost, s));
   return finish(ctx, "breaklines", nf, true);
+}
+
+
+// ---- io::load_mesh (io/mod.rs:114-137): PLY in, cleaned mesh out -----------------
+
+struct sherd_host_mesh {
+  sherd::meshio::HostMesh m;
+};
+
+int sherd_mesh_read(const char *path, sherd_host_mesh **out, uint32_t *nv, uint32_t *nf) {
+  if (!path || !out || !nv || !nf) return fail(nullptr, SHERD_E_INVALID, "null argument");
+  *out = nullptr;
+  *nv = 0;
+  *nf = 0;
+  auto *h = new sherd_host_mesh;
+  std::string err;
+  try {
+    err = sherd::meshio::read_ply(path, h->m);
+  } catch (const std::bad_alloc &) {
+    err = "out of host memory";
+  }
+  if (!err.empty()) {
+    delete h;
+    return fail(nullptr, SHERD_E_INVALID, std::string(path) + ": " + err);
+  }
+  if (h->m.v.size() / 3 >= (uint64_t(1) << 32) || h->m.f.size() / 3 >= (uint64_t(1) << 32)) {
+    delete h;
+    return fail(nullptr, SHERD_E_INVALID, std::string(path) + ": more than 2^32 vertices or faces");
+  }
+  sherd::meshio::clean(h->m);
+  if (h->m.f.empty()) {
+    delete h;
+    return fail(nullptr, SHERD_E_EMPTY, std::string(path) + ": no triangles");
+  }
+  *nv = uint32_t(h->m.v.size() / 3);
+  *nf = uint32_t(h->m.f.size() / 3);
+  *out = h;
+  return SHERD_OK;
+}
+
+int sherd_host_mesh_copy(const sherd_host_mesh *m, double *v, uint32_t *f) {
+  if (!m || !v || !f) return fail(nullptr, SHERD_E_INVALID, "null argument");
+  std::copy(m->m.v.begin(), m->m.v.end(), v);
+  std::copy(m->m.f.begin(), m->m.f.end(), f);
+  return SHERD_OK;
+}
+
+int sherd_host_mesh_free(sherd_host_mesh *m) {
+  delete m;
+  return SHERD_OK;
 }
 
 }  // extern "C"
