@@ -10,6 +10,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <array>
@@ -84,6 +85,15 @@ cudaError_t noalloc_address(int device, int **out) {
   *out = static_cast<int *>(p);
   return cudaSuccess;
 }
+
+// An NVTX range over one host-side scope (the enqueue of a stage or an entry
+// point), for nsys / ncu --nvtx; a no-op unless a tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 int fail(const sherd_ctx *ctx, int code, const std::string &msg) {
   t_errors[ctx] = msg;
@@ -1598,10 +1608,15 @@ int batch_run(sherd_batch *b, float *ms) {
   int rc = begin(ctx);
   if (rc) return rc;
   cudaStream_t s = ctx->stream;
+  NvtxRange range(b->sched == SHERD_SCHED_BATCHED ? "sherd batch (batched)" : "sherd batch (plain)");
   if (b->sched == SHERD_SCHED_BATCHED) {
+    static const char *const kStage[sherd_batch::STAGES] = {
+        "sherd stage ladder", "sherd stage verify", "sherd stage pen_inside", "sherd stage pen_min",
+        "sherd stage finalize"};
     if ((rc = capture(b))) return rc;
     CK(cudaEventRecord(b->ev[0], s));
     for (int k = 0; k < sherd_batch::STAGES; ++k) {
+      NvtxRange stage(kStage[k]);
       CK(cudaGraphLaunch(b->exec[k], s));
       CK(cudaEventRecord(b->ev[k + 1], s));
     }
@@ -1742,6 +1757,7 @@ int sherd_adjoint(sherd_ctx *ctx, sherd_pair *const *edges, uint32_t n_edges, co
     if (!views[e].frac_tgt.nrm) return fail(ctx, SHERD_E_INVALID, "edge target without normals");
   }
   std::lock_guard<std::mutex> lock(ctx->mu);
+  NvtxRange range("sherd adjoint");
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<PairView> dv;
@@ -1872,6 +1888,7 @@ int sherd_segment(sherd_ctx *ctx, const sherd_mesh *mesh, const double *v, uint3
   }
   const float pad = float(1e-6 * mag);
   std::lock_guard<std::mutex> lock(ctx->mu);
+  NvtxRange range("sherd segment");
   int rc = begin(ctx);
   if (rc) return rc;
   cudaStream_t s = ctx->stream;
@@ -2060,6 +2077,7 @@ int sherd_vertex_normals(sherd_ctx *ctx, const double *v, uint32_t nv, const uin
     if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
   if (nv == 0) return SHERD_OK;
   std::lock_guard<std::mutex> lock(ctx->mu);
+  NvtxRange range("sherd vertex_normals");
   int rc = begin(ctx);
   if (rc) return rc;
   cudaStream_t s = ctx->stream;
@@ -2140,6 +2158,7 @@ int sherd_refine_join(sherd_ctx *ctx, const double *source, uint32_t n_source,
     return SHERD_OK;
   }
   std::lock_guard<std::mutex> lock(ctx->mu);
+  NvtxRange range("sherd refine_join");
   int rc = begin(ctx);
   if (rc) return rc;
   cudaStream_t s = ctx->stream;
@@ -2249,6 +2268,7 @@ int sherd_hypotheses_coarse(sherd_ctx *ctx, const sherd_frames *a, const sherd_f
     if (ib[j] >= b->n) return fail(ctx, SHERD_E_INVALID, "ib names a point beyond b's frames");
   if (n_ia == 0 || n_ib == 0) return SHERD_OK;  // no hypothesis (R 5.1's empty return)
   std::lock_guard<std::mutex> lock(ctx->mu);
+  NvtxRange range("sherd hypotheses_coarse");
   int rc = begin(ctx);
   if (rc) return rc;
   cudaStream_t s = ctx->stream;
@@ -2528,6 +2548,7 @@ int sherd_breaklines(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_
   if (nf == 0) return SHERD_OK;
   const float pad = float(1e-6 * mag);
   std::lock_guard<std::mutex> lock(ctx->mu);
+  NvtxRange range("sherd breaklines");
   int rc = begin(ctx);
   if (rc) return rc;
   cudaStream_t s = ctx->stream;
