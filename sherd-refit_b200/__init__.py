@@ -4,7 +4,10 @@ The package wraps the C ABI of include/sherd_cuda.h (built into `_lib/libsherd_c
 device LBVHs over fragment meshes and point clouds, first-hit and parity rays, bounded
 point-to-mesh distances, exact nearest neighbours, the point-to-plane ICP ladder, the R 6
 verification and the batched persistent stage-2 path, plus the differentiable pose objective
-(`adjoint`). There is no CPU fallback: if the library is missing, using it raises.
+(`adjoint`). Around it, with the reference's names: `preprocess` (R 3.5 breaklines and samples
+of a labelled mesh), `stage1` (R 5.1-5.5), `pair` (`match_pair` through R 5.7), `refine`
+(R 9's join refinement) and `read_mesh` (PLY). There is no CPU fallback: if the library is
+missing, using it raises.
 """
 
 from ._abi import (AdjointOptions, Candidate, IcpOptions, InsideOutcome, Params, Registration,
