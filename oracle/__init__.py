@@ -159,6 +159,8 @@ def lib() -> C.CDLL:
         "or_ball_normals": (None, [F64P, C.c_uint32, F64P, F64P, F64P, C.c_uint32, C.c_double,
                                    F64P, U8P]),
         "or_voxel_representatives": (C.c_uint32, [F64P, C.c_uint32, C.c_double, U32P]),
+        "or_nms": (C.c_uint32, [U32P, C.c_uint32, F64P, F64P, C.c_double, C.c_uint32, C.c_double,
+                                U32P]),
         "or_place_fused": (None, [F64P, C.c_uint32, F64P, C.c_int, F64P]),
     }
     for name, (res, args) in sig.items():
@@ -736,30 +738,14 @@ def order_by_score(score, limit=None):
 
 
 def nms(order, poses, score, trans_tol, topk, floor):
-    """nms::nms (nms.rs:61-86) with trace(A^T B) summed as nms.rs:93-99 sums it."""
-    poses = np.asarray(poses, np.float64)
-    kept = []
-    for h in order:
-        h = int(h)
-        if score[h] < floor:
-            break
-        t = poses[h]
-        duplicate = False
-        for k in kept:
-            u = poses[k]
-            d = t[:3, 3] - u[:3, 3]
-            if np.sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) < trans_tol:
-                tr = 0.0
-                for i in range(3):
-                    tr += (t[0, i] * u[0, i] + t[1, i] * u[1, i]) + t[2, i] * u[2, i]
-                if tr > NMS_ROT_TOL:
-                    duplicate = True
-                    break
-        if not duplicate:
-            kept.append(h)
-        if len(kept) >= topk:
-            break
-    return np.array(kept, np.uint32)
+    """nms::nms (nms.rs:61-86) with trace(A^T B) summed as nms.rs:93-99 sums it (or_nms)."""
+    order = u32(order)
+    poses = f64(poses).reshape(-1, 16)
+    score = f64(score).reshape(-1)
+    kept = np.empty(max(len(order), 1), np.uint32)
+    m = lib().or_nms(order, len(order), poses, score, float(trans_tol), int(topk), float(floor),
+                     kept) if len(order) else 0
+    return kept[:m].copy()
 
 
 def stage1_ladder(source, target: Cloud, inits, scales: Scales):

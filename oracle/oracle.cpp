@@ -2237,4 +2237,31 @@ uint32_t or_voxel_representatives(const double *p, uint32_t n, double spacing, u
   return uint32_t(rep.size());
 }
 
+// nms::nms (nms.rs:61-99) over row-major 4x4 poses: walk `order`, stop at the
+// first score below `floor`, keep a pose unless a kept one is nearer than
+// trans_tol in translation ((dx dx + dy dy) + dz dz under the root) and
+// trace(A^T B) > 2.9 (summed per column as (a0 b0 + a1 b1) + a2 b2), stop once
+// topk are kept (tested after keeping). Returns the count written to kept.
+uint32_t or_nms(const uint32_t *order, uint32_t n_order, const double *poses, const double *score,
+                double trans_tol, uint32_t topk, double floor, uint32_t *kept) {
+  uint32_t m = 0;
+  for (uint32_t o = 0; o < n_order; ++o) {
+    const uint32_t h = order[o];
+    if (score[h] < floor) break;
+    const double *t = poses + 16 * size_t(h);
+    bool duplicate = false;
+    for (uint32_t k = 0; k < m && !duplicate; ++k) {
+      const double *u = poses + 16 * size_t(kept[k]);
+      const double dx = t[3] - u[3], dy = t[7] - u[7], dz = t[11] - u[11];
+      if (!(std::sqrt((dx * dx + dy * dy) + dz * dz) < trans_tol)) continue;
+      double trace = 0.0;
+      for (int c = 0; c < 3; ++c) trace += (t[c] * u[c] + t[4 + c] * u[4 + c]) + t[8 + c] * u[8 + c];
+      duplicate = trace > 2.9;
+    }
+    if (!duplicate) kept[m++] = h;
+    if (m >= topk) break;
+  }
+  return m;
+}
+
 }  // extern "C"
