@@ -121,6 +121,20 @@ def _max_over_ranks(world, x):
     return x if world == 1 else _pkg("shard").max_over_ranks(x, device="cuda")
 
 
+def nn_query_rates(sbytes: dict, stage_ms: dict, step_ms: float, world: int) -> dict:
+    """NN queries/s of the batched path: every ICP point-iteration of k_ladder is one bounded
+    nearest-neighbour query (48 algorithmic bytes each), so the ladder stage's queries are its
+    bytes / 48; the rate over the ladder stage's device time, and over the whole step (all
+    ranks' queries over the slowest rank's step)."""
+    q = sbytes["ladder"] / 48.0
+    ms = stage_ms.get("ladder", 0.0)
+    return {"ladder_queries_per_step": q,
+            "nn_queries_per_s": q / (ms / 1000.0) if ms > 0 else None,
+            "nn_queries_per_s_whole_step": world * q / (step_ms / 1000.0) if step_ms > 0 else None,
+            "unit": "queries/s",
+            "what": "one bounded nearest-neighbour query per ICP point-iteration (k_ladder)"}
+
+
 def cpu_baseline(wl, seconds, params_fn):
     """The oracle (reference algorithm, f64, all host threads) on a bounded, deterministic
     sample of the workload's items: returns (verifications/s, threads, sample description)."""
@@ -635,6 +649,7 @@ def main():
                 "timer": "host wall clock around the synchronous C-ABI call",
                 "matches_resident_run": same},
         "gpu_launches": 7 * args.steps,
+        "nn_queries": nn_query_rates(sbytes, stage_ms, step_ms, world),
         "roofline": roofline,
         "clocks": clocks,
         "cpu_baseline": cpu,
