@@ -566,7 +566,8 @@ def _pairs_and_starts(rng, frags, n_starts, all_pairs=True):
 def pot_collection(seed, walls, cells_per_wall, edges_per_t, n_starts, frac_per_t2=150.0,
                    frac_range=(5000, 12000), noise_amp=0.25, surface_points=20000,
                    margin_points=6000, reg_points=6000, all_pairs=True, name="pot"):
-    """Fragments of pots broken by seeded spherical Voronoi partitions (configs 2, 3 and 5)."""
+    """Fragments of pots broken by seeded spherical Voronoi partitions (the pot, collection,
+    thin and scan workloads)."""
     rng = np.random.default_rng(seed)
     frags = []
     densities = frac_per_t2 if isinstance(frac_per_t2, tuple) else (frac_per_t2,) * len(walls)
@@ -591,7 +592,8 @@ def pot_collection(seed, walls, cells_per_wall, edges_per_t, n_starts, frac_per_
 
 
 def slab_collection(seed=0, t=10.0, edges_per_t=7.0, n_starts=16, noise_amp=0.3):
-    """Config 1: a 200 x 100 curved slab of wall t cut in two, B perturbed <= 30 deg, <= 2 t."""
+    """The slab pair: a 200 x 100 curved slab of wall t cut in two, B perturbed <= 30 deg,
+    <= 2 t."""
     rng = np.random.default_rng(seed)
     wall = SlabWall(t)
     part = SlabCut(wall)
@@ -609,12 +611,12 @@ def slab_collection(seed=0, t=10.0, edges_per_t=7.0, n_starts=16, noise_amp=0.3)
 
 
 CONFIGS = {
-    # 1 slab, 2 pot (8 fragments, 28 pairs x 64 starts), 3 collection
-    # (40 fragments of 3 pots, t = 5, 8, 12; 780 pairs x 128 starts; 1k-60k fracture points),
-    # 5 thin pot (t = 2 at 4-6 edges per t, 6 fragments of about 1M faces, 500k surface
+    # The workloads: a slab pair; a pot (8 fragments, 28 pairs x 64 starts); a collection
+    # (40 fragments of 3 pots, t = 5, 8, 12; 780 pairs x 128 starts; 1k-60k fracture points);
+    # a thin pot (t = 2 at 4-6 edges per t, 6 fragments of about 1M faces, 500k surface
     # samples per fragment: 1M penetration samples per pair).
     # The ring meshing spends about twice the faces of an isotropic mesh at the same edge
-    # length, so the edge lengths are set to land on each config's stated face counts.
+    # length, so the edge lengths are set to land on each workload's face counts.
     "slab": lambda seed=0: slab_collection(seed, edges_per_t=7.0),
     "pot": lambda seed=0: pot_collection(seed, walls=(8.0,), cells_per_wall=(8,),
                                          edges_per_t=(5.5, 7.5), n_starts=64, name="pot"),
