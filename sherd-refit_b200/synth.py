@@ -448,7 +448,7 @@ def fragment_from_cell(rng, name, cm: CellMesh, t, frac_per_t2, frac_range, surf
 
 
 # ---------------------------------------------------------------------------------------------
-# collections (the configs)
+# collections (the workloads)
 # ---------------------------------------------------------------------------------------------
 
 
