@@ -77,3 +77,97 @@ def match_pair(ctx: Context, pair, stage1: PairStage1, params: A.Params,
     for c in cands:
         c.scores.brk_best = best1
     return PairResult(cands[:keep], s1, order[:keep])
+
+
+@dataclass
+class FragmentInput:
+    """One labelled working mesh as the matching stage reads it: f64 vertices, faces, the
+    fracture label per face, R 3.2's thickness, R 3.3's res and its watertightness."""
+    v: np.ndarray
+    f: np.ndarray
+    frac: np.ndarray
+    t: float
+    res: float
+    watertight: bool = True
+
+
+def match_collection(ctx: Context, fragments, pairs, params: A.Params,
+                     keep: int = KEEP_PER_PAIR, seed: int = 0, stage1_floor: float = 0.0,
+                     timings: dict | None = None) -> list:
+    """R 5 over a list of pairs (a, b) of `fragments` (FragmentInput), the collection form of
+    match_pair: each fragment's R 3.5 arrays at each t a pair asks for (t_pair = min(t_a, t_b),
+    R 4.2), stage 1 per pair, ONE batched stage-2 call over every pair's starts (the items are
+    independent, batch.rs:417-423), then R 5.7 per pair. Returns one PairResult per pair, in
+    order. `timings`, when given, receives the host seconds of each phase."""
+    import time
+
+    from . import preprocess
+    from .backend import scales_for_pair
+    clock = time.perf_counter
+    t0 = clock()
+    scales = [scales_for_pair(params, min(fragments[a].t, fragments[b].t),
+                              max(fragments[a].res, fragments[b].res)) for a, b in pairs]
+    data, dev = {}, {}
+    meshes = {}
+    for (a, b), sc in zip(pairs, scales):
+        for k in (a, b):
+            key = (k, sc.t)
+            if key in data:
+                continue
+            fr = fragments[k]
+            md = preprocess.match_data(ctx, fr.v, fr.f, fr.frac, sc.t, seed)
+            if k not in meshes:
+                mesh = ctx.mesh(fr.v, fr.f)
+                meshes[k] = (mesh, mesh.subset(fr.frac))
+            mesh, fm = meshes[k]
+            surf = ctx.surfaces(fm, mesh, int(bool(fr.watertight)), md.frac_area, md.samples.pf,
+                                md.samples.s, md.brk.p, md.brk.ns, md.margin_p, md.margin_n)
+            data[key] = md
+            dev[key] = (surf, ctx.cloud(md.reg_p, md.reg_n), ctx.cloud(md.samples.pf, md.pf_n))
+    t1 = clock()
+    results, items, handles, owner = [], [], [], []
+    for k, ((a, b), sc) in enumerate(zip(pairs, scales)):
+        ma, mb = data[(a, sc.t)], data[(b, sc.t)]
+        if not all(len(m.samples.pf) and len(m.brk) for m in (ma, mb)):
+            results.append(None)   # not matchable (pair.rs:161-165): no candidate
+            continue
+        s1 = PairStage1(ctx, ma.frames, mb.frames, sc).run(seed=seed)
+        results.append(PairResult([], s1))
+        if not len(s1.scores) or (stage1_floor > 0.0 and s1.best < stage1_floor):
+            continue
+        sa, reg_t, frac_t = dev[(a, sc.t)]
+        sb = dev[(b, sc.t)][0]
+        handles.append(ctx.pair(sa, sb, reg_t, frac_t, mb.reg_p, mb.samples.pf, sc))
+        owner.append(k)
+        items += [(len(handles) - 1, j, start) for j, start in enumerate(s1.starts)]
+    t2 = clock()
+    out = ctx.ladder_verify_batch(handles, items, params) if items else []
+    t3 = clock()
+    per = [[] for _ in pairs]
+    for i in range(len(items)):
+        c = A.Candidate.from_buffer_copy(out[i])
+        per[owner[c.pair]].append(c)
+    for k, (res, sc) in enumerate(zip(results, scales)):
+        if res is None:
+            results[k] = PairResult([], None)
+            continue
+        s1 = res.stage1
+        if not len(s1.scores):
+            continue
+        if stage1_floor > 0.0 and s1.best < stage1_floor:
+            j = int(np.flatnonzero(s1.scores == s1.best)[0])
+            res.candidates, res.starts = [_partial(sc, s1.transforms[j], s1.best)], [j]
+            continue
+        cands = sorted(per[k], key=lambda c: c.start)
+        brk = s1.scores[s1.kept2.astype(np.int64)]
+        for c in cands:
+            c.scores.brk = float(brk[c.start])
+        order = sorted(range(len(cands)),
+                       key=lambda i: -(cands[i].scores.seam * cands[i].scores.tight))
+        ranked = [cands[i] for i in order]
+        for c in ranked:
+            c.scores.brk_best = s1.best
+        res.candidates, res.starts = ranked[:keep], [cands[i].start for i in order[:keep]]
+    if timings is not None:
+        timings.update(preprocess=t1 - t0, stage1=t2 - t1, stage2=t3 - t2, rank=clock() - t3)
+    return results

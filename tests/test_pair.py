@@ -121,3 +121,64 @@ def test_match_pair_on_the_device_reproduces_the_fixture(sherd, gpu_ctx, gpu_sla
     best = np.array(own.candidates[0].rungs[3].transform[:]).reshape(4, 4)
     assert own.candidates[0].accepted == 1
     assert trace_deg(best, slab["result_T"][0]) <= 0.2
+
+
+class _OracleCollectionDevice(_OracleDevice):
+    """_OracleDevice plus the object constructors match_collection uses, on the oracle."""
+
+    def face_geometry(self, v, f):
+        return self.o.face_geometry(v, f)
+
+    def breaklines(self, v, f, frac, t, macro_inner=0.15, macro_outer=0.6, brk_voxel=0.5):
+        return self.o.breaklines(v, f, frac, t, macro_inner, macro_outer, brk_voxel)
+
+    def mesh(self, v, f):
+        return self.o.Mesh(v, f)
+
+    def surfaces(self, fracture, mesh, watertight, frac_area, pf, s, brk_p, brk_ns, margin_p,
+                 margin_n):
+        return self.o.Surfaces(fracture, mesh, watertight, frac_area, pf, s, brk_p, brk_ns,
+                               margin_p, margin_n)
+
+    def pair(self, a, b, reg_t, frac_t, reg_p, frac_p, scales):
+        return self.o.Pair(a, b, reg_t, frac_t, reg_p, frac_p,
+                           self.o.Scales.from_buffer_copy(scales))
+
+
+def test_match_collection_is_match_pair_per_pair(sherd, oracle, slab):
+    """The collection form (one batched stage 2 over every pair's starts) gives each pair what
+    match_pair gives it, and on the slab the fixture's accepted join first."""
+    pm = importlib.import_module("sherd-refit_b200.pair")
+    pre = importlib.import_module("sherd-refit_b200.preprocess")
+    st = importlib.import_module("sherd-refit_b200.stage1")
+    dev = _OracleCollectionDevice(oracle)
+    params = _params(sherd, slab)
+    frags = []
+    for name in ("pieceA", "pieceB"):
+        p = piece(slab, name)
+        frags.append(pm.FragmentInput(p["V"], p["F"], p["frac"], float(p["thick_t"]),
+                                      float(p["res"]), bool(p["watertight"])))
+    timings = {}
+    (res,) = pm.match_collection(dev, frags, [(0, 1)], params, timings=timings)
+    assert set(timings) == {"preprocess", "stage1", "stage2", "rank"}
+    sc = sherd.scales_for_pair(params, min(f.t for f in frags), max(f.res for f in frags))
+    assert np.array_equal(np.array([getattr(sc, k) for k, _ in sc._fields_]), slab["scales"])
+    mds = [pre.match_data(dev, f.v, f.f, f.frac, sc.t, 0) for f in frags]
+    surf = []
+    for f, md in zip(frags, mds):
+        mesh = oracle.Mesh(f.v, f.f)
+        fm = mesh.subset(f.frac)
+        surf.append((mesh, fm, oracle.Surfaces(fm, mesh, int(f.watertight), md.frac_area,
+                                               md.samples.pf, md.samples.s, md.brk.p, md.brk.ns,
+                                               md.margin_p, md.margin_n)))
+    a, b = mds
+    pair = oracle.Pair(surf[0][2], surf[1][2], oracle.Cloud(a.reg_p, a.reg_n),
+                       oracle.Cloud(a.samples.pf, a.pf_n), b.reg_p, b.samples.pf,
+                       oracle.Scales.from_buffer_copy(sc))
+    want = pm.match_pair(dev, pair, st.PairStage1(dev, a.frames, b.frames, sc), params)
+    assert len(res.candidates) == len(want.candidates) == 5
+    for g, w in zip(res.candidates, want.candidates):
+        assert bytes(g.rungs) == bytes(w.rungs) and g.accepted == w.accepted
+        assert g.scores.brk == w.scores.brk and g.scores.brk_best == w.scores.brk_best
+    best = np.array(res.candidates[0].rungs[3].transform[:]).reshape(4, 4)
+    assert res.candidates[0].accepted == 1 and trace_deg(best, slab["result_T"][0]) <= 0.05
