@@ -247,3 +247,23 @@ def test_device_native_pair_chain_accepts_the_fixtures_join(sherd, gpu_ctx, orac
     best = np.array(res.candidates[0].rungs[3].transform[:]).reshape(4, 4)
     assert res.candidates[0].accepted == 1
     assert trace_deg(best, slab["result_T"][0]) <= 0.2 and origin_t(best, slab["result_T"][0], t) <= 0.05
+
+
+@pytest.mark.gpu
+def test_device_match_collection_accepts_the_fixtures_join(sherd, gpu_ctx, slab):
+    """pair.match_collection on the device from the two labelled slab meshes: the pair's best
+    candidate is the fixture's accepted join."""
+    pm = importlib.import_module("sherd-refit_b200.pair")
+    params = sherd.default_params()
+    for k, val in zip(("min_tight", "max_gap", "max_pen", "min_seam", "min_cont_n"), slab["params"]):
+        setattr(params, k, float(val))
+    frags = []
+    for name in ("pieceA", "pieceB"):
+        p = piece(slab, name)
+        frags.append(pm.FragmentInput(p["V"], p["F"], p["frac"], float(p["thick_t"]),
+                                      float(p["res"]), bool(p["watertight"])))
+    (res,) = pm.match_collection(gpu_ctx, frags, [(0, 1)], params)
+    best = np.array(res.candidates[0].rungs[3].transform[:]).reshape(4, 4)
+    t = float(slab["scales"][0])
+    assert res.candidates[0].accepted == 1
+    assert trace_deg(best, slab["result_T"][0]) <= 0.2 and origin_t(best, slab["result_T"][0], t) <= 0.05
