@@ -182,3 +182,23 @@ def test_match_collection_is_match_pair_per_pair(sherd, oracle, slab):
         assert g.scores.brk == w.scores.brk and g.scores.brk_best == w.scores.brk_best
     best = np.array(res.candidates[0].rungs[3].transform[:]).reshape(4, 4)
     assert res.candidates[0].accepted == 1 and trace_deg(best, slab["result_T"][0]) <= 0.05
+
+
+def test_match_collection_under_the_stage1_floor(sherd, oracle, slab):
+    """match_collection's stage1_floor branch is match_pair's: the best stage-1 pose alone,
+    partial and refused, and no stage-2 item."""
+    pm = importlib.import_module("sherd-refit_b200.pair")
+
+    class NoStage2(_OracleCollectionDevice):
+        def ladder_verify_batch(self, *a, **k):
+            raise AssertionError("no stage-2 item should run under the floor")
+
+    frags = []
+    for name in ("pieceA", "pieceB"):
+        p = piece(slab, name)
+        frags.append(pm.FragmentInput(p["V"], p["F"], p["frac"], float(p["thick_t"]),
+                                      float(p["res"]), bool(p["watertight"])))
+    (res,) = pm.match_collection(NoStage2(oracle), frags, [(0, 1)], _params(sherd, slab),
+                                 stage1_floor=0.9)
+    (c,) = res.candidates
+    assert c.scores.partial == 1 and c.accepted == 0 and c.scores.brk == res.stage1.best
