@@ -372,9 +372,10 @@ def run_refine(args):
         cpu = {"value": n_joins / cpu_stage, "unit": "joins/s",
                "cores": oracle.lib().or_default_threads(), "kind": "port",
                "sample": (f"the oracle on the walk's first join ({len(o_pieces[1].points)} source, "
-                          f"{len(o_pieces[0].points)} target points; {t_join_cpu:.2f} s, one "
-                          f"thread: one pose) and its two fragments' clouds ({t_cloud_cpu:.2f} s "
-                          f"each, all threads), scaled to {len(frags)} clouds and {n_joins} joins"),
+                          f"{len(o_pieces[0].points)} target points; {t_join_cpu:.2f} s, each "
+                          f"pass's searches on all threads) and its two fragments' clouds "
+                          f"({t_cloud_cpu:.2f} s each, all threads), scaled to {len(frags)} "
+                          f"clouds and {n_joins} joins"),
                "join_s": t_join_cpu, "cloud_s": t_cloud_cpu,
                "first_join_device_vs_oracle": {"rung_rot_deg_trans_t": vs,
                                                "fitness": [first.fitness, oj.fitness]}}

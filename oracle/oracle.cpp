@@ -42,6 +42,31 @@ constexpr float F_INF = std::numeric_limits<float>::infinity();
 constexpr double D_INF = std::numeric_limits<double>::infinity();
 constexpr uint32_t MISS = 0xFFFFFFFFu;
 
+// Runs fn(0..n-1) on `threads` threads (in order on one).
+template <class F>
+void parallel_for(uint32_t n, int threads, F &&fn) {
+  if (threads <= 1 || n < 2) {
+    for (uint32_t i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::atomic<uint32_t> next{0};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([&] {
+      for (;;) {
+        uint32_t i = next.fetch_add(1);
+        if (i >= n) break;
+        fn(i);
+      }
+    });
+  for (auto &th : pool) th.join();
+}
+
+int default_threads() {
+  unsigned h = std::thread::hardware_concurrency();
+  return h ? int(h) : 1;
+}
+
 struct V3f {
   float x, y, z;
 };
@@ -681,7 +706,7 @@ struct Corr {
 
 // icp::correspondences (icp.rs:361-392).
 void correspondences(const std::vector<double> &moved, const Cloud &tgt, double distance,
-                     std::vector<Corr> &out, double *fit, double *rmse) {
+                     std::vector<Corr> &out, double *fit, double *rmse, int threads = 1) {
   out.clear();
   *fit = 0.0;
   *rmse = 0.0;
@@ -690,13 +715,29 @@ void correspondences(const std::vector<double> &moved, const Cloud &tgt, double 
   double r2 = distance * distance;
   double err = 0.0;
   size_t n = moved.size() / 3;
-  for (size_t i = 0; i < n; ++i) {
-    uint32_t j;
-    double d2;
-    if (!tgt.nearest_within_sq(&moved[3 * i], r2, &j, &d2)) continue;
-    if (d2 >= r2) continue;
-    err += d2;
-    out.push_back({uint32_t(i), j});
+  if (threads > 1 && n >= 4096) {
+    // The searches on `threads` threads, the sum afterwards in point order: the same
+    // correspondences and the same rounding as the loop below.
+    std::vector<uint32_t> js(n);
+    std::vector<double> d2s(n);
+    std::vector<uint8_t> ok(n);
+    parallel_for(uint32_t(n), threads, [&](uint32_t i) {
+      ok[i] = tgt.nearest_within_sq(&moved[3 * size_t(i)], r2, &js[i], &d2s[i]) && d2s[i] < r2;
+    });
+    for (size_t i = 0; i < n; ++i) {
+      if (!ok[i]) continue;
+      err += d2s[i];
+      out.push_back({uint32_t(i), js[i]});
+    }
+  } else {
+    for (size_t i = 0; i < n; ++i) {
+      uint32_t j;
+      double d2;
+      if (!tgt.nearest_within_sq(&moved[3 * i], r2, &j, &d2)) continue;
+      if (d2 >= r2) continue;
+      err += d2;
+      out.push_back({uint32_t(i), j});
+    }
   }
   if (out.empty()) return;
   double nc = double(out.size()), ns = double(n);
@@ -905,7 +946,8 @@ void transform_points(std::vector<double> &pts, const double *m) {
 
 // icp::register (icp.rs:308-356), point-to-plane.
 sherd_registration icp_register(const double *src, uint32_t ns, const Cloud &tgt,
-                                const double *init, const sherd_icp_options &opt) {
+                                const double *init, const sherd_icp_options &opt,
+                                int threads = 1) {
   sherd_registration out{};
   std::memcpy(out.transform, init, sizeof out.transform);
   if (ns == 0 || tgt.size() == 0) return out;
@@ -915,7 +957,7 @@ sherd_registration icp_register(const double *src, uint32_t ns, const Cloud &tgt
   transform_points(moved, init);
   std::vector<Corr> corr;
   double fit, rmse;
-  correspondences(moved, tgt, opt.max_correspondence_distance, corr, &fit, &rmse);
+  correspondences(moved, tgt, opt.max_correspondence_distance, corr, &fit, &rmse, threads);
   uint32_t iterations = 0;
   bool converged = false;
   for (int it = 0; it < opt.max_iteration; ++it) {
@@ -928,7 +970,7 @@ sherd_registration icp_register(const double *src, uint32_t ns, const Cloud &tgt
     transform_points(moved, u);
     ++iterations;
     double nfit, nrmse;
-    correspondences(moved, tgt, opt.max_correspondence_distance, corr, &nfit, &nrmse);
+    correspondences(moved, tgt, opt.max_correspondence_distance, corr, &nfit, &nrmse, threads);
     converged = std::fabs(nfit - fit) < 1e-6 && std::fabs(nrmse - rmse) < 1e-6;
     fit = nfit;
     rmse = nrmse;
@@ -1456,29 +1498,6 @@ uint8_t cone_vote(const Mesh &m, const double *c, const double *fnv, const doubl
   return good;
 }
 
-template <class F>
-void parallel_for(uint32_t n, int threads, F &&fn) {
-  if (threads <= 1 || n < 2) {
-    for (uint32_t i = 0; i < n; ++i) fn(i);
-    return;
-  }
-  std::atomic<uint32_t> next{0};
-  std::vector<std::thread> pool;
-  for (int t = 0; t < threads; ++t)
-    pool.emplace_back([&] {
-      for (;;) {
-        uint32_t i = next.fetch_add(1);
-        if (i >= n) break;
-        fn(i);
-      }
-    });
-  for (auto &th : pool) th.join();
-}
-
-int default_threads() {
-  unsigned h = std::thread::hardware_concurrency();
-  return h ? int(h) : 1;
-}
 
 }  // namespace
 
@@ -1890,6 +1909,10 @@ void or_nearest_below(const void *cloud, const double *q, uint32_t n, double bou
 void or_icp_rung(const double *src, uint32_t ns, const void *target, const double *inits,
                  uint32_t k, sherd_icp_options opt, sherd_registration *out, int threads) {
   const Cloud *c = static_cast<const Cloud *>(target);
+  if (k < uint32_t(std::max(threads, 1))) {  // few poses: the threads share each pass instead
+    for (uint32_t i = 0; i < k; ++i) out[i] = icp_register(src, ns, *c, inits + 16 * size_t(i), opt, threads);
+    return;
+  }
   parallel_for(k, threads, [&](uint32_t i) {
     out[i] = icp_register(src, ns, *c, inits + 16 * size_t(i), opt);
   });
