@@ -69,3 +69,47 @@ def gather_records(records: np.ndarray, device=None) -> list:
     dist.all_gather(bufs, buf)
     return [np.frombuffer(b.cpu().numpy()[:c * item].tobytes(), records.dtype)
             for b, c in zip(bufs, counts)]
+
+
+def partition_pairs(cost, world: int) -> list:
+    """Pairs over ranks by estimated cost, longest first onto the least-loaded rank (ties to the
+    lower rank): a list per rank of pair indices, ascending. Deterministic, so every rank
+    computes the same partition without talking to the others."""
+    load = [0.0] * max(int(world), 1)
+    out = [[] for _ in load]
+    for k in sorted(range(len(cost)), key=lambda k: (-float(cost[k]), k)):
+        r = min(range(len(load)), key=lambda r: (load[r], r))
+        load[r] += float(cost[k])
+        out[r].append(k)
+    return [sorted(o) for o in out]
+
+
+def match_collection_sharded(ctx, fragments, pairs, params, keep: int = 5, seed: int = 0,
+                             stage1_floor: float = 0.0, device=None) -> list:
+    """pair.match_collection with the pairs shared out over the ranks by estimated cost (the
+    fragments' face counts): each rank builds the arrays of only the fragments its pairs touch,
+    matches its pairs, and one all-gather of fixed-size candidate records (sherd_candidate, the
+    pair field rewritten to the collection's pair index) hands every rank every pair's ranked
+    candidates. Returns, per pair, its candidate records in R 5.7's order."""
+    import torch.distributed as dist
+
+    from . import pair as pair_mod
+    from .backend import CANDIDATE
+    on = dist.is_available() and dist.is_initialized()
+    rank, world = (dist.get_rank(), dist.get_world_size()) if on else (0, 1)
+    cost = [len(fragments[a].f) + len(fragments[b].f) for a, b in pairs]
+    mine = partition_pairs(cost, world)[rank]
+    res = pair_mod.match_collection(ctx, fragments, [pairs[k] for k in mine], params, keep, seed,
+                                    stage1_floor)
+    recs = []
+    for k, r in zip(mine, res):
+        for c in r.candidates:
+            rec = np.frombuffer(bytes(c), CANDIDATE).copy()
+            rec["pair"] = k
+            recs.append(rec)
+    mine_recs = np.concatenate(recs) if recs else np.zeros(0, CANDIDATE)
+    out = [[] for _ in pairs]
+    for part in gather_records(mine_recs, device):
+        for rec in part:
+            out[int(rec["pair"])].append(rec)
+    return out

@@ -61,3 +61,52 @@ def _rank_main(rank, world, port):
 def test_two_gloo_ranks_shard_the_starts_and_gather_the_records():
     import torch.multiprocessing as mp
     mp.spawn(_rank_main, args=(2, _free_port()), nprocs=2, join=True)
+
+
+def test_partition_pairs_balances_and_covers():
+    shard = importlib.import_module("sherd-refit_b200.shard")
+    parts = shard.partition_pairs([5, 1, 4, 2, 3, 3], 2)
+    assert sorted(k for p in parts for k in p) == list(range(6))
+    assert parts == [[0, 1, 5], [2, 3, 4]]          # longest first: loads 9 and 9
+    assert shard.partition_pairs([1, 1], 3) == [[0], [1], []]
+
+
+def _rank_match(rank, world, port):
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "tests"))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=300))
+    try:
+        oracle = importlib.import_module("oracle")
+        sherd = importlib.import_module("sherd-refit_b200")
+        shard = importlib.import_module("sherd-refit_b200.shard")
+        pm = importlib.import_module("sherd-refit_b200.pair")
+        from _slab import piece
+        from test_pair import _OracleCollectionDevice, _params
+        with np.load(ROOT / "tests" / "golden" / "slab.npz") as z:
+            slab = {k: z[k] for k in z.files}
+        frags = []
+        for name in ("pieceA", "pieceB"):
+            p = piece(slab, name)
+            frags.append(pm.FragmentInput(p["V"], p["F"], p["frac"], float(p["thick_t"]),
+                                          float(p["res"]), bool(p["watertight"])))
+        dev = _OracleCollectionDevice(oracle)
+        pairs = [(0, 1), (0, 1), (0, 1)]
+        out = shard.match_collection_sharded(dev, frags, pairs, _params(sherd, slab))
+        assert [len(o) for o in out] == [5, 5, 5]
+        for o in out:                                   # every rank's copy of the same pair
+            assert bytes(o[0]["rungs"]) == bytes(out[0][0]["rungs"]) and o[0]["accepted"] == 1
+            s = [r["scores"]["seam"] * r["scores"]["tight"] for r in o]
+            assert all(x >= y for x, y in zip(s, s[1:]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_share_the_pairs_of_a_collection():
+    import torch.multiprocessing as mp
+    mp.spawn(_rank_match, args=(2, _free_port()), nprocs=2, join=True)
