@@ -40,10 +40,11 @@ sys.path.insert(0, str(ROOT))
 METRIC = "pair-pose verifications/s"
 UNIT = "verifications/s"
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (read + write) of one k_ladder launch on the default collection workload (seed 0),
-# from one ncu capture of `python bench.py --steps 1 --warmup 3 --no-cpu`
-# (profiles/k_ladder_collection_dram.md).
-LADDER_TRAFFIC = {("collection", 0): (539.88 + 270.85) * 1e9}
+# DRAM bytes (read + write) of one launch of a stage's dominant kernel, per (workload, seed,
+# kernel, ranks), from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of
+# `python bench.py --steps 1 --warmup 3 --no-cpu --no-plain`, with the digest of the CUDA sources
+# it was taken on: a capture of other sources is not reported.
+TRAFFIC = {}
 
 
 def _pkg(name=""):
@@ -122,88 +123,122 @@ def _max_over_ranks(world, x):
     return x if world == 1 else _pkg("shard").max_over_ranks(x, device="cuda")
 
 
-def nn_query_rates(sbytes: dict, stage_ms: dict, step_ms: float, world: int) -> dict:
+def nn_query_rates(sbytes: dict, stage_ms: dict, step_ms: float, total_q: float) -> dict:
     """NN queries/s of the batched path: every ICP point-iteration of k_ladder is one bounded
     nearest-neighbour query (48 algorithmic bytes each), so the ladder stage's queries are its
-    bytes / 48; the rate over the ladder stage's device time, and over the whole step (all
-    ranks' queries over the slowest rank's step)."""
+    bytes / 48; the rate over this rank's ladder stage device time, and over the whole step
+    (all ranks' queries, `total_q`, over the slowest rank's step)."""
     q = sbytes["ladder"] / 48.0
     ms = stage_ms.get("ladder", 0.0)
-    return {"ladder_queries_per_step": q,
+    return {"ladder_queries_per_step": total_q,
             "nn_queries_per_s": q / (ms / 1000.0) if ms > 0 else None,
-            "nn_queries_per_s_whole_step": world * q / (step_ms / 1000.0) if step_ms > 0 else None,
+            "nn_queries_per_s_whole_step": total_q / (step_ms / 1000.0) if step_ms > 0 else None,
             "unit": "queries/s",
             "what": "one bounded nearest-neighbour query per ICP point-iteration (k_ladder)"}
 
 
-def cpu_baseline(wl, seconds, params_fn):
-    """The oracle (reference algorithm, f64, all host threads) on a bounded, deterministic
-    sample of the workload's items: returns (verifications/s, threads, sample description)."""
+CPU_ITEMS = 512
+
+
+def oracle_sample(wl, k: int) -> np.ndarray:
+    """The CPU legs' sample: k items evenly spaced over the pair-major item list (ascending item
+    indices). The same sample serves the CUDA arm's cpu_baseline and parity legs and every step
+    of the reference arm, so the two CPU figures are of one workload."""
+    n = wl.n_items
+    return np.unique(np.linspace(0, n - 1, min(int(k), n)).round().astype(np.int64))
+
+
+def oracle_run(oracle, wl, pairs, idx, params):
+    """The oracle over the items idx on all host threads: (candidates in idx order, seconds).
+    The items are handed over most expensive first (the threads take them in list order), the
+    order the device queue takes them in, so the last thread to finish is not left holding the
+    largest item."""
+    workload = _pkg("workload")
+    shard = _pkg("shard")
+    pair, start, inits = workload.item_arrays(wl)
+    cost = shard.pair_costs(wl)[pair[idx].astype(np.int64)]
+    order = np.argsort(-cost, kind="stable")
+    sel = idx[order]
+    items = oracle.work_items_from(pair[sel], start[sel], inits[sel])
+    t0 = time.perf_counter()
+    out, _ = oracle.ladder_verify_items(pairs, items, params, 0)
+    dt = time.perf_counter() - t0
+    got = np.ctypeslib.as_array(out)[: len(idx)].copy()
+    cands = np.empty_like(got)
+    cands[order] = got
+    return cands, dt
+
+
+def cpu_baseline_and_parity(wl, k, gpu_cands):
+    """The oracle (reference algorithm, f64, all host threads) on the deterministic sample:
+    its rate as cpu_baseline, and its candidates compared with the CUDA path's at the same
+    items (oracle.parity: verdicts, status and the final pose against the f64 answer, with the
+    reference's one-ULP chaos probe for any item outside the bound)."""
     oracle = importlib.import_module("oracle")
+    parity = importlib.import_module("oracle.parity")
     workload = _pkg("workload")
     pairs, keep = oracle.collection(wl)
-    pair, start, inits = workload.item_arrays(wl)
-    n = len(pair)
     params = oracle.default_params()
     threads = oracle.lib().or_default_threads()
-
-    def run(k):
-        idx = np.linspace(0, n - 1, k).round().astype(np.int64)
-        items = oracle.work_items_from(pair[idx], start[idx], inits[idx])
+    idx = oracle_sample(wl, k)
+    ref, dt = oracle_run(oracle, wl, pairs, idx, params)
+    sample = (f"{len(idx)} of the {wl.n_items} (pair, start) items, evenly spaced over the "
+              f"pair-major item list, on {threads} threads, {dt:.1f} s")
+    cpu = {"value": len(idx) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": sample}
+    par = None
+    if gpu_cands is not None:
+        arrays = workload.item_arrays(wl)
+        t, c = parity.item_scale(wl, arrays[0][idx])
+        probe = parity.collection_probe(oracle, pairs, params, arrays, idx, ref, t, c)
         t0 = time.perf_counter()
-        oracle.ladder_verify_items(pairs, items, params, 0)
-        return time.perf_counter() - t0
-
-    k = max(threads, 8)
-    dt = run(k)
-    while dt < 0.5 * seconds and k < 4096:
-        k = min(4096, int(k * max(2.0, 0.5 * seconds / max(dt, 1e-3))))
-        dt = run(k)
-    sample = (f"{k} of the {n} (pair, start) items, evenly spaced over the pair-major item "
-              f"list, on {threads} threads, {dt:.1f} s")
-    return k / dt, threads, sample
+        par = parity.compare(gpu_cands[idx], ref, t, c, pair_ids=arrays[0][idx], probe=probe)
+        par["probe_s"] = round(time.perf_counter() - t0, 1)
+        par["sample"] = "the cpu_baseline sample: " + sample
+        par["oracle"] = "oracle/oracle.cpp, the reference algorithm in f64 (source-order sums)"
+    del keep
+    return cpu, par
 
 
 def run_reference(args):
+    """The reference arm: the reference algorithm's CPU restatement (the oracle; the Rust
+    reference cannot be built here) on all host cores, each timed step the whole deterministic
+    sample (oracle_sample) of the same workload, most expensive item first. The warm-up steps
+    run one item per thread of the same sample, untimed."""
     world, rank, _ = _dist()
     if rank != 0:
         return
     synth = _pkg("synth")
     wl = synth.make(args.config, args.seed)
     oracle = importlib.import_module("oracle")
-    workload = _pkg("workload")
     pairs, keep = oracle.collection(wl)
-    pair, start, inits = workload.item_arrays(wl)
-    n = len(pair)
     params = oracle.default_params()
     threads = oracle.lib().or_default_threads()
-    per_step = args.reference_items or max(threads * 2, 16)
-    rng = np.random.default_rng(args.seed)
+    idx = oracle_sample(wl, args.cpu_items)
+    for _ in range(args.warmup):
+        oracle_run(oracle, wl, pairs, idx[:: max(1, len(idx) // threads)], params)
     times = []
-    for step in range(args.warmup + args.steps):
-        idx = np.sort(rng.choice(n, per_step, replace=False))
-        items = oracle.work_items_from(pair[idx], start[idx], inits[idx])
-        t0 = time.perf_counter()
-        oracle.ladder_verify_items(pairs, items, params, 0)
-        dt = time.perf_counter() - t0
-        if step >= args.warmup:
-            times.append(dt)
-    value = per_step * len(times) / sum(times)
-    sample = (f"{per_step} random (pair, start) items per step (seed {args.seed}) of the "
-              f"{n}-item workload, {threads} threads")
+    for _ in range(args.steps):
+        _, dt = oracle_run(oracle, wl, pairs, idx, params)
+        times.append(dt)
+    value = len(idx) * len(times) / sum(times)
+    sample = (f"{len(idx)} of the {wl.n_items} (pair, start) items per step, evenly spaced over "
+              f"the pair-major item list (the CUDA arm's cpu_baseline sample), {threads} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(times)),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": _config_dict(wl, args),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, sherd-refit_b200/synth.py)",
+        "config": _config_dict(wl, args),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": ("the reference's Rust CPU backend cannot be built in this image (no cargo); "
                  "this is its C++ restatement (oracle/oracle.cpp), pinned to the reference's "
-                 "fixture to 1e-14 t, f64 point loops as the reference's Numerics::REFERENCE"),
+                 "fixture, f64 point loops as the reference's Numerics::REFERENCE"),
     }
     print(json.dumps(line), flush=True)
+    del keep
 
 
 def run_group(args):
@@ -559,16 +594,62 @@ def run_chain(args):
     ctx.close()
 
 
-def _config_dict(wl, args, extra=None):
+def _config_dict(wl, args):
+    """The workload the line is quoted on; both arms print the same dictionary."""
     d = wl.describe()
-    cfg = {"workload": f"{args.config}: {d['fragments']} fragments, {d['pairs']} pairs x "
-                       f"{d['starts_per_pair']} starts = {d['items']} (pair, start) items",
-           **d, "sched": args.sched,
-           "parallelism": (f"{int(os.environ.get('WORLD_SIZE', '1'))} ranks, one GPU each; every "
-                           "rank verifies its own starts for every pair (weak scaling)")}
-    if extra:
-        cfg.update(extra)
-    return cfg
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"workload": f"{args.config}: {d['fragments']} fragments, {d['pairs']} pairs x "
+                        f"{d['starts_per_pair']} starts = {d['items']} (pair, start) items",
+            **d, "sched": args.sched,
+            "l2": (f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MB write); the resident "
+                   "fragment data also exceeds L2"),
+            "parallelism": (f"{world} rank(s), one GPU each; the collection's pairs partitioned "
+                            "over the ranks by estimated cost, each rank holding only its pairs' "
+                            "fragments, one batched call per rank, one all-gather of candidate "
+                            "records (strong scaling)")}
+
+
+def _source_hash() -> str:
+    """A digest of the CUDA sources, naming the build a recorded ncu capture belongs to."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in sorted((ROOT / "sherd-refit_b200" / "csrc").glob("*.cu*")):
+        h.update(f.name.encode())
+        h.update(f.read_bytes())
+    return h.hexdigest()[:12]
+
+
+def _plain_leg(ctx, sherd, dev, wl, params, n_pairs, full_cands):
+    """SHERD_SCHED_PLAIN (one k_ladder + k_verify_items launch per pair, synchronised after each
+    pair) on n_pairs pairs evenly spaced over the collection with all their starts, and the
+    batched schedule on the same items, on the resident data (device time, CUDA events)."""
+    workload = _pkg("workload")
+    sub = np.unique(np.linspace(0, len(dev.pairs) - 1, n_pairs).round().astype(np.int64))
+    pair, start, inits = workload.item_arrays(wl)
+    where = np.full(len(dev.pairs), -1, np.int64)
+    where[sub] = np.arange(len(sub))
+    sel = np.flatnonzero(where[pair] >= 0)
+    items = sherd.work_item_array(where[pair[sel]].astype(np.uint32), start[sel], inits[sel])
+    pairs = [dev.pairs[k] for k in sub]
+    out = {}
+    for name, sched in (("plain", sherd.SCHED_PLAIN), ("batched", sherd.SCHED_BATCHED)):
+        b = ctx.batch(pairs, items, params, sched)
+        b.run()
+        out[name] = (b.run()["total"], sherd.candidates(b.results()).copy())
+        del b
+    n = len(sel)
+    plain_ms, plain_c = out["plain"]
+    batched_ms, batched_c = out["batched"]
+    want = full_cands[sel].copy()
+    want["pair"] = where[want["pair"].astype(np.int64)]
+    return {"value": n / (plain_ms / 1000.0), "unit": UNIT, "ms": plain_ms, "items": int(n),
+            "pairs": int(len(sub)),
+            "sample": (f"{len(sub)} of the {len(dev.pairs)} pairs, evenly spaced over the pair "
+                       f"list, with all their starts ({n} items)"),
+            "batched_same_items": {"value": n / (batched_ms / 1000.0), "ms": batched_ms},
+            "batched_over_plain_same_items": plain_ms / batched_ms,
+            "identical_candidates": bool(plain_c.tobytes() == batched_c.tobytes()
+                                         == want.tobytes())}
 
 
 def main():
@@ -581,9 +662,10 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--sched", default="batched", choices=("batched", "plain"))
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--reference-items", type=int, default=0)
+    ap.add_argument("--cpu-items", type=int, default=CPU_ITEMS)
+    ap.add_argument("--plain-pairs", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--group-poses", type=int, default=4096)
     ap.add_argument("--refine-workload", default="scan")
     ap.add_argument("--chain-workload", default="pot")
@@ -607,25 +689,24 @@ def main():
     import torch
 
     world, rank, local = _dist()
+    torch.cuda.set_device(local)
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(local)
     sherd = _pkg()
     synth = _pkg("synth")
     workload = _pkg("workload")
     shard = _pkg("shard")
     t_gen = time.perf_counter()
-    wl = shard.rank_workload(synth.make(args.config, args.seed), rank, args.seed)
+    wl = synth.make(args.config, args.seed)
     t_gen = time.perf_counter() - t_gen
+    mine = shard.rank_pairs(wl, rank, world) if world > 1 else None
     ctx = sherd.Context(local)
     params = sherd.default_params()
     t_up = time.perf_counter()
-    dev = workload.to_device(ctx, wl, params)
+    dev = workload.to_device(ctx, wl, params, pairs=mine)
     t_up = time.perf_counter() - t_up
     sched = sherd.SCHED_BATCHED if args.sched == "batched" else sherd.SCHED_PLAIN
     batch = ctx.batch(dev.pairs, dev.items, params, sched)
@@ -648,28 +729,33 @@ def main():
     clocks = sampler.stop()
     stage_ms = {k: float(np.mean([r[k] for r in runs])) for k in runs[0]}
     step_ms = _max_over_ranks(world, stage_ms["total"])
-    n_items = dev.n_items
-    value = world * n_items / (step_ms / 1000.0)
+    n_items = wl.n_items
+    value = n_items / (step_ms / 1000.0)
 
-    cands = sherd.candidates(batch.results())
-    sbytes = workload.stage_bytes(wl, cands, dev.n_src)
-    accepted = int(cands["accepted"].sum())
-    status_bad = int((cands["status"] != 0).sum())
+    local_cands = sherd.candidates(batch.results()).copy()
+    local_cands["pair"] = np.asarray(dev.pair_index)[local_cands["pair"].astype(np.int64)]
+    sbytes = workload.stage_bytes(wl, local_cands)
+    total_q = shard.sum_over_ranks(sbytes["ladder"] / 48.0, device="cuda")
 
-    # End to end through the host-buffer C-ABI call: work items in, candidates out.
+    # End to end through the host-buffer C-ABI call: work items in, candidates out, then the
+    # one all-gather that puts every item's candidate on every rank.
     e2e_ms = []
     for k in range(args.e2e_steps + 1):
         flush.zero_()
         torch.cuda.synchronize()
+        _barrier(world)
         t0 = time.perf_counter()
         out = ctx.ladder_verify_batch(dev.pairs, dev.items, params, sched)
+        full = shard.gather_candidates(wl, dev, sherd.candidates(out), device="cuda")
         t1 = time.perf_counter()
         if k:
             e2e_ms.append(1000 * (t1 - t0))
     e2e_step = _max_over_ranks(world, float(np.mean(e2e_ms)))
-    h2d = n_items * sherd.WORK_ITEM.itemsize
-    d2h = n_items * sherd.CANDIDATE.itemsize
+    h2d = dev.n_items * sherd.WORK_ITEM.itemsize
+    d2h = dev.n_items * sherd.CANDIDATE.itemsize
     same = bytes(out) == bytes(batch.results())
+    accepted = int(full["accepted"].sum())
+    status_bad = int((full["status"] != 0).sum())
 
     peak, peak_kind = _peaks()
     kernel_of = {"ladder": "k_ladder", "verify": "k_verify_items", "pen_inside": "k_pen_inside",
@@ -681,12 +767,15 @@ def main():
                      "gbs": sbytes[k] / (ms / 1000.0) / 1e9 if ms > 0 else None}
     dom = max(("ladder", "verify", "pen_inside", "pen_min"), key=lambda k: stage_ms[k])
     achieved = stages[dom]["gbs"]
-    traffic = LADDER_TRAFFIC.get((args.config, args.seed)) if dom == "ladder" else None
+    src = _source_hash()
+    rec = TRAFFIC.get((args.config, args.seed, kernel_of[dom], world))
+    traffic = rec[0] if rec and rec[1] == src else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                   "full-size launch (profiles/k_ladder_collection_dram.md)"
-                                   if traffic else None),
+                "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                   f"full-size launch of this build (CUDA sources {src})"
+                                   if traffic else
+                                   f"no ncu capture recorded for this build (CUDA sources {src})"),
                 "kernel": stages[dom]["kernel"],
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "per_unit": ("48 B per ICP point-iteration (16 B source point + 32 B matched "
@@ -694,30 +783,39 @@ def main():
                              if dom == "ladder" else "24 B per query point"),
                 "stages": stages}
 
+    plain = None
+    if world == 1 and not args.no_plain and sched == sherd.SCHED_BATCHED:
+        plain = _plain_leg(ctx, sherd, dev, wl, params, args.plain_pairs, full)
+        plain["value_over_plain"] = value / plain["value"]
+
     if rank != 0:
         ctx.close()
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
-    cpu = None
+    cpu, par = None, None
     if not args.no_cpu:
-        v_cpu, threads, sample = cpu_baseline(wl, args.cpu_seconds, None)
-        cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        cpu, par = cpu_baseline_and_parity(wl, args.cpu_items, full)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator, sherd-refit_b200/synth.py)",
-        "config": _config_dict(wl, args, {
-            "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MB write); the resident "
-                  "fragment data also exceeds L2",
-            "accepted": accepted, "item_errors": status_bad,
-            "generate_s": round(t_gen, 1), "upload_s": round(t_up, 1)}),
-        "e2e": {"value": world * n_items / (e2e_step / 1000.0), "unit": UNIT,
+        "config": _config_dict(wl, args),
+        "run": {"accepted": accepted, "item_errors": status_bad, "generate_s": round(t_gen, 1),
+                "upload_s": round(t_up, 1),
+                "rank_items": int(dev.n_items), "rank_pairs": len(dev.pairs)},
+        "e2e": {"value": n_items / (e2e_step / 1000.0), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "timer": "host wall clock around the synchronous C-ABI call",
+                "timer": ("host wall clock around the synchronous C-ABI call and the candidate "
+                          "all-gather (max over ranks); bytes per rank"),
                 "matches_resident_run": same},
         "gpu_launches": 7 * args.steps,
-        "nn_queries": nn_query_rates(sbytes, stage_ms, step_ms, world),
+        "nn_queries": nn_query_rates(sbytes, stage_ms, step_ms, total_q),
         "roofline": roofline,
+        "plain": plain,
+        "parity": par,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }

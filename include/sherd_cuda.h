@@ -292,9 +292,15 @@ int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source,
  * cudaMalloc/cudaFree while other streams are in flight (both can block or
  * synchronise the whole device). No counterpart in the reference.
  *
- * The same rung as sherd_icp_rung, with every buffer already on the device:
- * `source` holds n_source points as 4 doubles each (x, y, z, unused; 16-byte
- * aligned), `inits` k row-major 4x4 poses, `out` room for k registrations.
+ * The same rung as sherd_icp_rung (point-to-plane or point-to-point), with
+ * every buffer already on the device: `source` holds n_source points as 4
+ * doubles each (x, y, z, unused; 16-byte aligned), `inits` k row-major 4x4
+ * poses, `out` room for k registrations (both 8-byte aligned). Each buffer
+ * must be device memory of the context's GPU (or managed memory): a host
+ * pointer or a misaligned one is refused with SHERD_E_INVALID before anything
+ * is launched. The poses are read on the device only, so a non-finite one is
+ * not refused up front: its rung finds no correspondence and the call returns
+ * SHERD_E_INVALID after it ran; pass finite poses.
  * The per-point working memory (each source point's last match) lives in one
  * array inside this library, sized at SHERD_NOALLOC_CAPACITY entries and held
  * by every GPU that loads the library until the process exits; a call with

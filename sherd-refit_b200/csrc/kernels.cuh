@@ -274,7 +274,14 @@ __global__ void __launch_bounds__(ICP_BLOCK, 4) k_icp_rung(const double4 *src, u
                                                         sherd_registration *out, uint32_t *status) {
   __shared__ IcpShared sh;
   uint32_t st = 0;
-  if (threadIdx.x < 16) sh.t[threadIdx.x] = inits[16 * blockIdx.x + threadIdx.x];
+  if (threadIdx.x < 16) {
+    double v = inits[16 * blockIdx.x + threadIdx.x];
+    sh.t[threadIdx.x] = v;
+    // A non-finite start (which only a caller passing device-resident poses can hand over,
+    // the host-buffer entry refusing it first) is reported; the rung itself stays in bounds
+    // (no distance compares below a NaN radius, so it finds no correspondence).
+    if (!isfinite(v)) st |= ST_RANGE;
+  }
   __syncthreads();
   icp_rung_block(src, ns, tgt, opt.max_correspondence_distance, opt.max_iteration, sh,
                  hints + size_t(ns) * blockIdx.x, out + blockIdx.x, st,

@@ -168,10 +168,10 @@ int finish(sherd_ctx *ctx, const char *method, size_t items, bool timed) {
   }
   if (st & ST_ABORTED) return fail(ctx, SHERD_E_ABORTED, std::string(method) + ": aborted");
   if (st & ST_TIMEOUT) return fail(ctx, SHERD_E_TIMEOUT, std::string(method) + ": time budget spent");
-  if (st & ST_STACK) return fail(ctx, SHERD_E_DEVICE, std::string(method) + ": traversal stack overflow");
-  if (st & ST_SCRATCH) return fail(ctx, SHERD_E_INVALID, std::string(method) + ": scratch too small");
   if (st & ST_RANGE)
     return fail(ctx, SHERD_E_INVALID, std::string(method) + ": input outside the supported range");
+  if (st & ST_STACK) return fail(ctx, SHERD_E_DEVICE, std::string(method) + ": traversal stack overflow");
+  if (st & ST_SCRATCH) return fail(ctx, SHERD_E_INVALID, std::string(method) + ": scratch too small");
   return SHERD_OK;
 }
 
@@ -1093,7 +1093,26 @@ int sherd_icp_rung_noalloc(sherd_ctx *ctx, const double *source, uint32_t n_sour
                 "over several calls or use sherd_icp_rung");
   if ((reinterpret_cast<uintptr_t>(source) & 15u) != 0)
     return fail(ctx, SHERD_E_INVALID, "source must be 16-byte aligned (4 doubles per point)");
+  if ((reinterpret_cast<uintptr_t>(inits) & 7u) != 0 || (reinterpret_cast<uintptr_t>(out) & 7u) != 0)
+    return fail(ctx, SHERD_E_INVALID, "inits and out must be 8-byte aligned");
   if (k == 0) return SHERD_OK;
+  // Every buffer must be memory this context's GPU can address as device memory: a host
+  // pointer would fault inside the kernel, so it is refused here, before any launch. The
+  // query allocates nothing.
+  const void *bufs[3] = {inits, out, n_source ? source : nullptr};
+  for (const void *b : bufs) {
+    if (!b) continue;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, b) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, SHERD_E_INVALID, "source, inits and out must be device memory");
+    }
+    bool ok = at.type == cudaMemoryTypeManaged ||
+              (at.type == cudaMemoryTypeDevice && at.device == ctx->device);
+    if (!ok)
+      return fail(ctx, SHERD_E_INVALID,
+                  "source, inits and out must be device (or managed) memory of the context's GPU");
+  }
   std::lock_guard<std::mutex> lock(ctx->mu);
   int rc = begin(ctx);  // makes the context's device current
   if (rc) return rc;

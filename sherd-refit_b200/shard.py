@@ -1,40 +1,72 @@
 """One process per GPU: how the batched stage-2 path is spread over ranks.
 
-(pair, start) items are independent, so the path shards without a collective on its data
-path. Rank r verifies its own start set for every pair of the collection: the same fragments
-and pairs, starts drawn from the seed (seed, r), so each rank carries one collection's worth of
-work and the whole job grows with the rank count (weak scaling). Around that:
-  * `max_over_ranks`, the job's step time (a one-element MAX all-reduce);
-  * `gather_records`, one all-gather of fixed-size result records (sherd_candidate, 808 B) in
-    rank order, for a caller that wants every rank's candidates on every rank.
-Nothing here reads peer memory; the collectives go through torch.distributed (NCCL on GPUs,
-gloo on the CPU).
+(pair, start) items are independent, so the path shards without a collective on its data path
+(the collection plan of the reference's matching stage, crates/sherd-core/src/pipeline.rs:1615-1690,
+`match_all` over blocks of pairs). A collection is split by pairs:
+  * `pair_costs` estimates each pair's device time from its point and sample counts;
+  * `partition_pairs` shares the pairs out, longest first onto the least-loaded rank, the same
+    on every rank without a message;
+  * each rank makes resident only the fragments its pairs touch (workload.to_device with
+    `pairs`) and runs one batched call over its pairs' items;
+  * `gather_candidates` ends the job with one all-gather of fixed-size candidate records
+    (sherd_candidate, 808 B) rewritten to the collection's pair indices, which puts every item's
+    candidate, in the collection's item order, on every rank.
+Around that, `max_over_ranks` gives the job's step time (a one-element MAX all-reduce). The
+total work is fixed whatever the rank count (strong scaling). Nothing here reads peer memory;
+the collectives go through torch.distributed (NCCL on GPUs, gloo on the CPU).
 """
 
 from __future__ import annotations
 
 import numpy as np
 
-from . import synth
+# Device seconds per algorithmic byte of the two halves of an item, from the batched path on the
+# 40-fragment collection: the ICP ladder moves about 800 GB/s of its 48 B point-iterations, the
+# penetration wavefront about 60 GB/s of its 24 B surface-sample queries. Only the ratio matters.
+LADDER_S_PER_BYTE = 1.0 / 800e9
+PEN_S_PER_BYTE = 1.0 / 60e9
+PASSES_PER_RUNG = 12.0
 
 
-def rank_workload(wl, rank: int, seed: int):
-    """The workload rank `rank` verifies: wl itself on rank 0, else the same fragments and pairs
-    with starts drawn from the seed (seed, rank)."""
-    if rank == 0:
-        return wl
-    n_starts = len(wl.starts[0]) if wl.starts else 0
-    rng = np.random.default_rng((seed, rank))
-    pairs, starts = synth._pairs_and_starts(rng, wl.fragments, n_starts,
-                                            all_pairs=len(wl.pairs) == _all_pairs(wl))
-    assert [(p.a, p.b) for p in pairs] == [(p.a, p.b) for p in wl.pairs]
-    return synth.Workload(name=wl.name, fragments=wl.fragments, pairs=pairs, starts=starts,
-                          seed=wl.seed)
+def pair_costs(wl) -> np.ndarray:
+    """Estimated device seconds of each pair's items: per start, the four rungs over B's
+    registration and fracture clouds (PASSES_PER_RUNG passes of 48 B per point) and the
+    penetration queries of both sides' surface samples (24 B each)."""
+    out = np.empty(len(wl.pairs))
+    for k, (p, st) in enumerate(zip(wl.pairs, wl.starts)):
+        a, b = wl.fragments[p.a], wl.fragments[p.b]
+        ladder = 2.0 * (len(b.reg_p) + len(b.pf)) * PASSES_PER_RUNG * 48.0
+        pen = (len(a.s) + len(b.s)) * 24.0
+        out[k] = len(st) * (ladder * LADDER_S_PER_BYTE + pen * PEN_S_PER_BYTE)
+    return out
 
 
-def _all_pairs(wl):
-    n = len(wl.fragments)
-    return n * (n - 1) // 2
+def rank_pairs(wl, rank: int, world: int) -> list:
+    """The pairs (indices into wl.pairs, ascending) rank `rank` of `world` verifies."""
+    return partition_pairs(pair_costs(wl), world)[rank]
+
+
+def gather_candidates(wl, dev, cands, device=None) -> np.ndarray:
+    """Every item's candidate in the collection's item order, on every rank: this rank's
+    candidates (a structured sherd_candidate array over dev's items) get the collection's pair
+    index and travel with their item index in one all-gather of fixed-size records."""
+    from .backend import CANDIDATE
+    cands = np.asarray(cands)
+    mine = cands.copy()
+    mine["pair"] = np.asarray(dev.pair_index, np.int64)[cands["pair"].astype(np.int64)]
+    rec = np.dtype([("item", np.uint64), ("cand", CANDIDATE)])
+    recs = np.zeros(len(mine), rec)
+    recs["item"] = np.asarray(dev.item_index, np.uint64)
+    recs["cand"] = mine
+    out = np.zeros(wl.n_items, CANDIDATE)
+    seen = np.zeros(wl.n_items, bool)
+    for part in gather_records(recs, device):
+        idx = part["item"].astype(np.int64)
+        out[idx] = part["cand"]
+        seen[idx] = True
+    if not seen.all():
+        raise RuntimeError(f"{int((~seen).sum())} items were verified by no rank")
+    return out
 
 
 def max_over_ranks(x: float, device=None) -> float:
@@ -45,6 +77,17 @@ def max_over_ranks(x: float, device=None) -> float:
         return float(x)
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, device=None) -> float:
+    """The sum of x over all ranks (x itself without a process group)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 

@@ -26,8 +26,10 @@ class DeviceCollection:
     frac_targets: list
     pairs: list
     scales: list
-    items: object          # ctypes WorkItem array
+    items: object          # ctypes WorkItem array (pair = index into `pairs`)
     n_src: np.ndarray      # (n_pairs, 2): |pc_reg of B|, |pc_frac of B|
+    pair_index: np.ndarray | None = None  # per device pair, its index in the workload's pairs
+    item_index: np.ndarray | None = None  # per work item, its index in the workload's item list
 
     @property
     def n_items(self):
@@ -51,37 +53,65 @@ def item_arrays(wl):
     return pair, start, inits
 
 
-def to_device(ctx: Context, wl, params: A.Params | None = None) -> DeviceCollection:
-    meshes, fractures, surfaces, reg_t, frac_t = [], [], [], [], []
-    for fr in wl.fragments:
+def to_device(ctx: Context, wl, params: A.Params | None = None, pairs=None) -> DeviceCollection:
+    """The workload made resident through `ctx`. `pairs` (indices into wl.pairs, ascending)
+    restricts it to those pairs' items and to the fragments they touch, as one rank of a
+    cost-partitioned collection holds them; the device pair index of a work item is then its
+    position in `pairs`, and `item_index` maps each work item back to the workload's item list."""
+    keep = np.arange(len(wl.pairs)) if pairs is None else np.asarray(pairs, np.int64)
+    used = sorted({f for k in keep for f in (wl.pairs[k].a, wl.pairs[k].b)})
+    meshes, fractures, surfaces, reg_t, frac_t = ({}, {}, {}, {}, {})
+    for i in used:
+        fr = wl.fragments[i]
         m = ctx.mesh(fr.v, fr.f)
         fm = m.subset(fr.frac)
-        meshes.append(m)
-        fractures.append(fm)
-        surfaces.append(ctx.surfaces(fm, m, True, fr.frac_area, fr.pf, fr.s, fr.brk_p, fr.brk_ns,
-                                     fr.margin_p, fr.margin_n))
-        reg_t.append(ctx.cloud(fr.reg_p, fr.reg_n))
-        frac_t.append(ctx.cloud(fr.pf, fr.pf_n))
-    scales = pair_scales(wl, params)
-    pairs = []
-    n_src = np.zeros((len(wl.pairs), 2), np.int64)
-    for k, (p, sc) in enumerate(zip(wl.pairs, scales)):
+        meshes[i] = m
+        fractures[i] = fm
+        surfaces[i] = ctx.surfaces(fm, m, True, fr.frac_area, fr.pf, fr.s, fr.brk_p, fr.brk_ns,
+                                   fr.margin_p, fr.margin_n)
+        reg_t[i] = ctx.cloud(fr.reg_p, fr.reg_n)
+        frac_t[i] = ctx.cloud(fr.pf, fr.pf_n)
+    all_scales = pair_scales(wl, params)
+    scales = [all_scales[k] for k in keep]
+    dev_pairs = []
+    n_src = np.zeros((len(keep), 2), np.int64)
+    for j, k in enumerate(keep):
+        p = wl.pairs[k]
         b = wl.fragments[p.b]
-        pairs.append(ctx.pair(surfaces[p.a], surfaces[p.b], reg_t[p.a], frac_t[p.a], b.reg_p, b.pf,
-                              sc))
-        n_src[k] = (len(b.reg_p), len(b.pf))
-    items = work_item_array(*item_arrays(wl))
-    return DeviceCollection(ctx, meshes, fractures, surfaces, reg_t, frac_t, pairs, scales, items,
-                            n_src)
+        dev_pairs.append(ctx.pair(surfaces[p.a], surfaces[p.b], reg_t[p.a], frac_t[p.a], b.reg_p,
+                                  b.pf, all_scales[k]))
+        n_src[j] = (len(b.reg_p), len(b.pf))
+    pair, start, inits = item_arrays(wl)
+    if pairs is None:
+        sel = np.arange(len(pair))
+        local = pair
+    else:
+        where = np.full(len(wl.pairs), -1, np.int64)
+        where[keep] = np.arange(len(keep))
+        sel = np.flatnonzero(where[pair] >= 0)
+        local = where[pair[sel]].astype(np.uint32)
+    items = work_item_array(local, start[sel], inits[sel])
+    order = lambda d: [d[i] for i in used]
+    return DeviceCollection(ctx, order(meshes), order(fractures), order(surfaces), order(reg_t),
+                            order(frac_t), dev_pairs, scales, items, n_src, keep, sel)
 
 
-def stage_bytes(wl, cands, n_src):
-    """Compulsory bytes of each stage of the batched path over the units in `cands`:
+def pair_n_src(wl) -> np.ndarray:
+    """(n_pairs, 2): |pc_reg of B|, |pc_frac of B| of every pair of the workload."""
+    return np.array([(len(wl.fragments[p.b].reg_p), len(wl.fragments[p.b].pf)) for p in wl.pairs],
+                    np.int64).reshape(-1, 2)
+
+
+def stage_bytes(wl, cands, n_src=None):
+    """Compulsory bytes of each stage of the batched path over the units in `cands` (their pair
+    field indexing wl.pairs, and n_src by default that of every workload pair):
     ladder: 48 B per ICP point-iteration (16 B source point, 32 B matched target point and
     normal) over the passes each rung ran (iterations + 1); verify: 24 B per query of
     |Pf_A| + |Pf_B| + |brk_A| + |Pm_B|; pen_inside: 24 B per surface sample |S_A| + |S_B|;
     pen_min: 24 B per surface sample of the items whose two sides had nothing inside
     (pen_depth <= 0; a lower bound of the points that pass scans)."""
+    if n_src is None:
+        n_src = pair_n_src(wl)
     pair = cands["pair"].astype(np.int64)
     passes = cands["rungs"]["iterations"].astype(np.int64) + 1
     src = np.stack([n_src[pair, 0], n_src[pair, 0], n_src[pair, 1], n_src[pair, 1]], axis=1)

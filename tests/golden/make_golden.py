@@ -236,4 +236,6 @@ def main(reference: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference checkout>")
+    main(Path(sys.argv[1]))

@@ -208,3 +208,21 @@ def test_the_stage1_rung_holds_the_fixture_poses(slab, oracle):
     for r, pose in zip(regs, slab["s1_T"]):
         mine = np.array(r.transform[:]).reshape(4, 4)
         assert trace_deg(mine, pose) < 1e-3 and origin_t(mine, pose, t) < 1e-6
+
+
+@pytest.mark.parametrize("point_to_point", [False, True])
+def test_a_single_pose_rung_is_the_same_on_one_thread_and_on_eight(slab, oracle, point_to_point):
+    """With one pose, the oracle splits each pass's correspondence searches over its threads and
+    still sums in point order: the registration is the same bytes on one thread and on eight."""
+    a, b = piece(slab, "pieceA"), piece(slab, "pieceB")
+    t, icp = float(slab["scales"][0]), float(slab["scales"][11])
+    target = oracle.Cloud(a["reg_p"], a["reg_n"])
+    src = b["reg_p"]
+    assert len(src) >= 4096
+    for k in (0, 1, 2):
+        init = slab["starts"][k].reshape(1, 16)
+        one = oracle.icp_rung(src, target, init, 0.2 * t * icp, 30, threads=1,
+                              point_to_point=point_to_point)
+        eight = oracle.icp_rung(src, target, init, 0.2 * t * icp, 30, threads=8,
+                                point_to_point=point_to_point)
+        assert bytes(one[0]) == bytes(eight[0]), k

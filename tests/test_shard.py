@@ -1,8 +1,11 @@
 """The multi-rank host logic of the batched path, on two gloo ranks on the CPU.
 
-Each rank verifies its own start set for the same pairs (weak scaling); the job's step time
-is the maximum over ranks; results travel as fixed-size records in one all-gather. No GPU is
-needed: the collectives run on gloo with world size 2.
+A collection is split by pairs over the ranks by estimated cost (the survey's collection plan,
+crates/sherd-core/src/pipeline.rs:1615-1690); each rank holds only the fragments its pairs touch
+and verifies its pairs' items; one all-gather of fixed-size candidate records gives every rank
+every item's candidate. The job's step time is the maximum over ranks. No GPU is needed: the
+collectives run on gloo with world size 2, and the verification runs on an oracle-backed stand-in
+for the device context.
 """
 
 from __future__ import annotations
@@ -24,6 +27,40 @@ def _free_port():
         return s.getsockname()[1]
 
 
+class _OracleContext:
+    """The constructors workload.to_device calls and the batched call, answered by the oracle."""
+
+    def __init__(self, oracle):
+        self.o = oracle
+
+    def mesh(self, v, f):
+        return self.o.Mesh(v, f)
+
+    def surfaces(self, fracture, mesh, watertight, frac_area, pf, s, brk_p, brk_ns, margin_p,
+                 margin_n):
+        return self.o.Surfaces(fracture, mesh, watertight, frac_area, pf, s, brk_p, brk_ns,
+                               margin_p, margin_n)
+
+    def cloud(self, p, n):
+        return self.o.Cloud(p, n)
+
+    def pair(self, a, b, reg_t, frac_t, reg_p, frac_p, scales):
+        return self.o.Pair(a, b, reg_t, frac_t, reg_p, frac_p,
+                           self.o.Scales.from_buffer_copy(scales))
+
+    def ladder_verify_batch(self, pairs, items, params, sched=0):
+        out, _ = self.o.ladder_verify_items(pairs, items, self.o.Params.from_buffer_copy(params))
+        return out
+
+
+def small_collection():
+    """Six pairs of the pot workload (seven fragments), two starts each."""
+    synth = importlib.import_module("sherd-refit_b200.synth")
+    wl = synth.make("pot", 0)
+    return synth.Workload(name="pot6", fragments=wl.fragments, pairs=wl.pairs[:6],
+                          starts=[s[:2] for s in wl.starts[:6]], seed=0)
+
+
 def _rank_main(rank, world, port):
     import datetime
 
@@ -32,33 +69,39 @@ def _rank_main(rank, world, port):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world,
-                            timeout=datetime.timedelta(seconds=120))
+                            timeout=datetime.timedelta(seconds=300))
     try:
-        synth = importlib.import_module("sherd-refit_b200.synth")
+        oracle = importlib.import_module("oracle")
         shard = importlib.import_module("sherd-refit_b200.shard")
         backend = importlib.import_module("sherd-refit_b200.backend")
         workload = importlib.import_module("sherd-refit_b200.workload")
-        base = synth.make("slab", 0)
-        wl = shard.rank_workload(base, rank, 0)
-        assert [(p.a, p.b) for p in wl.pairs] == [(p.a, p.b) for p in base.pairs]
-        items = np.frombuffer(bytes(backend.work_item_array(*workload.item_arrays(wl))),
-                              backend.WORK_ITEM)
-        assert len(items) == base.n_items
-        everyone = shard.gather_records(items)
-        assert len(everyone) == world and np.array_equal(everyone[rank], items)
-        assert np.array_equal(everyone[0]["init"], np.frombuffer(bytes(backend.work_item_array(
-            *workload.item_arrays(base))), backend.WORK_ITEM)["init"])
-        for other in range(world):
-            if other != rank:
-                assert not np.array_equal(everyone[other]["init"], items["init"])
-        ragged = shard.gather_records(items[:rank + 1])
-        assert [len(r) for r in ragged] == [r + 1 for r in range(world)]
+        wl = small_collection()
+        ctx = _OracleContext(oracle)
+        params = backend.default_params()
+        parts = shard.partition_pairs(shard.pair_costs(wl), world)
+        assert all(parts) and sorted(k for p in parts for k in p) == list(range(len(wl.pairs)))
+        mine = shard.rank_pairs(wl, rank, world)
+        assert mine == parts[rank]
+        dev = workload.to_device(ctx, wl, params, pairs=mine)
+        touched = {f for k in mine for f in (wl.pairs[k].a, wl.pairs[k].b)}
+        assert len(dev.meshes) == len(touched) < len(wl.fragments)
+        assert dev.n_items == sum(len(wl.starts[k]) for k in mine)
+        got = backend.candidates(ctx.ladder_verify_batch(dev.pairs, dev.items, params))
+        full = shard.gather_candidates(wl, dev, got)
+        # one rank over the whole collection, byte for byte
+        one = workload.to_device(ctx, wl, params)
+        want = backend.candidates(ctx.ladder_verify_batch(one.pairs, one.items, params))
+        assert full.tobytes() == want[: wl.n_items].tobytes()
+        assert np.array_equal(full["pair"], workload.item_arrays(wl)[0])
         assert shard.max_over_ranks(1.5 + rank) == 1.5 + (world - 1)
+        assert shard.sum_over_ranks(1.0 + rank) == world * (world + 1) / 2
+        ragged = shard.gather_records(np.asarray(got)[:rank + 1])
+        assert [len(r) for r in ragged] == [r + 1 for r in range(world)]
     finally:
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_shard_the_starts_and_gather_the_records():
+def test_two_gloo_ranks_split_a_collection_by_pairs_and_gather_every_candidate():
     import torch.multiprocessing as mp
     mp.spawn(_rank_main, args=(2, _free_port()), nprocs=2, join=True)
 
@@ -96,13 +139,25 @@ def _rank_match(rank, world, port):
             frags.append(pm.FragmentInput(p["V"], p["F"], p["frac"], float(p["thick_t"]),
                                           float(p["res"]), bool(p["watertight"])))
         dev = _OracleCollectionDevice(oracle)
-        pairs = [(0, 1), (0, 1), (0, 1)]
-        out = shard.match_collection_sharded(dev, frags, pairs, _params(sherd, slab))
+        # The swapped pair is a different question (B fixed, A moving), so the ranks' shares
+        # differ: two pairs on rank 0, one on rank 1.
+        pairs = [(0, 1), (1, 0), (0, 1)]
+        assert shard.partition_pairs([1, 1, 1], world) == [[0, 2], [1]]
+        params = _params(sherd, slab)
+        out = shard.match_collection_sharded(dev, frags, pairs, params)
         assert [len(o) for o in out] == [5, 5, 5]
-        for o in out:                                   # every rank's copy of the same pair
-            assert bytes(o[0]["rungs"]) == bytes(out[0][0]["rungs"]) and o[0]["accepted"] == 1
+        for o in out:
             s = [r["scores"]["seam"] * r["scores"]["tight"] for r in o]
             assert all(x >= y for x, y in zip(s, s[1:]))
+        assert out[0][0]["accepted"] == 1
+        # Against one process matching the whole pair list: the same records, byte for byte.
+        whole = pm.match_collection(dev, frags, pairs, params)
+        for k, (o, w) in enumerate(zip(out, whole)):
+            assert len(o) == len(w.candidates)
+            for rec, c in zip(o, w.candidates):
+                want = np.frombuffer(bytes(c), rec.dtype).copy()
+                want["pair"] = k
+                assert rec.tobytes() == want.tobytes()
     finally:
         dist.destroy_process_group()
 

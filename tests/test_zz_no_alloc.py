@@ -26,7 +26,8 @@ def _call(sherd, ctx, src, n, target, inits, k, opt, out):
                                               C.c_void_p(inits), k, opt, C.c_void_p(out))
 
 
-def test_the_allocation_free_rung_matches_the_allocating_one(sherd, gpu_ctx, slab):
+@pytest.mark.parametrize("estimation", [1, 0], ids=["point_to_plane", "point_to_point"])
+def test_the_allocation_free_rung_matches_the_allocating_one(sherd, gpu_ctx, slab, estimation):
     import torch
 
     a, b = piece(slab, "pieceA"), piece(slab, "pieceB")
@@ -35,14 +36,14 @@ def test_the_allocation_free_rung_matches_the_allocating_one(sherd, gpu_ctx, sla
     dist = 0.2 * t * icp
     starts = np.ascontiguousarray(slab["starts"].reshape(-1, 16))
     k, n = len(starts), len(b["reg_p"])
-    expected = gpu_ctx.icp_rung(b["reg_p"], target, starts, dist, 30)
+    expected = gpu_ctx.icp_rung(b["reg_p"], target, starts, dist, 30, estimation=estimation)
 
     src = np.zeros((n, 4))
     src[:, :3] = b["reg_p"]
     d_src = torch.from_numpy(src).cuda()
     d_inits = torch.from_numpy(starts.copy()).cuda()
     d_out = torch.empty(C.sizeof(sherd.Registration) * k, dtype=torch.uint8, device="cuda")
-    opt = sherd.IcpOptions(1, 30, dist)
+    opt = sherd.IcpOptions(estimation, 30, dist)
     calls = []
     for _ in range(2):
         d_out.fill_(0xFF)
@@ -82,3 +83,14 @@ def test_the_allocation_free_rung_refuses_what_it_cannot_hold(sherd, gpu_ctx, sl
     rc = _call(sherd, gpu_ctx, d_src.data_ptr() + 8, n, target, d_inits.data_ptr(), 1, opt,
                d_out.data_ptr())
     assert rc == -1
+    # Misaligned poses or records, and host memory, are refused on the host before a launch.
+    rc = _call(sherd, gpu_ctx, d_src.data_ptr(), n, target, d_inits.data_ptr() + 4, 1, opt,
+               d_out.data_ptr())
+    assert rc == -1 and b"aligned" in sherd.lib().sherd_last_error(gpu_ctx.h)
+    rc = _call(sherd, gpu_ctx, d_src.data_ptr(), n, target, d_inits.data_ptr(), 1, opt,
+               d_out.data_ptr() + 4)
+    assert rc == -1 and b"aligned" in sherd.lib().sherd_last_error(gpu_ctx.h)
+    host_inits = np.zeros(16)
+    rc = _call(sherd, gpu_ctx, d_src.data_ptr(), n, target, host_inits.ctypes.data, 1, opt,
+               d_out.data_ptr())
+    assert rc == -1 and b"device" in sherd.lib().sherd_last_error(gpu_ctx.h)
