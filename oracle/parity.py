@@ -34,6 +34,7 @@ import numpy as np
 TOL_T = 1e-4       # final transforms within 1e-4 t of the FP64 oracle
 TOL_RAD = 1e-5     # and 1e-5 rad
 CHAOTIC_S2 = 0.4   # crosscheck.rs:76-78: the share of a pair's items the bound may excuse
+PAIR_MIN_ITEMS = 8  # the fewest items of a pair over which its chaotic share is taken
 
 
 def _as_struct(cands) -> np.ndarray:
@@ -165,17 +166,26 @@ def compare(gpu, ref, t, centre, pair_ids=None, probe=None) -> dict:
     if probe is not None and off.any():
         out["chaotic_rot_rad"] = _stats(rot[chaotic])
         out["chaotic_cloud_t"] = _stats(ct[chaotic])
+    out["chaotic_share"] = float(chaotic.sum()) / n if n else 0.0
+    out["chaotic_share_bound"] = CHAOTIC_S2
+    worst = None
     if pair_ids is not None:
+        # The reference states its bound over a pair's candidates; a share over one or two
+        # sampled items of a pair says nothing, so it is taken over pairs with PAIR_MIN_ITEMS
+        # or more items in the comparison.
         pair_ids = np.asarray(pair_ids)
-        worst = 0.0
+        shares = []
         for p in np.unique(pair_ids):
             m = pair_ids == p
-            worst = max(worst, float(chaotic[m].sum()) / float(m.sum()))
-        out["chaotic_share_worst_pair"] = worst
-        out["chaotic_share_bound"] = CHAOTIC_S2
+            if m.sum() >= PAIR_MIN_ITEMS:
+                shares.append(float(chaotic[m].sum()) / float(m.sum()))
+        worst = max(shares) if shares else None
+        out["pairs_with_share"] = len(shares)
+    out["chaotic_share_worst_pair"] = worst
     out["ok"] = bool(out["determined_past_bound"] == 0 and out["determined_verdict_mismatch"] == 0
                      and out["determined_status_mismatch"] == 0
-                     and out.get("chaotic_share_worst_pair", 0.0) <= CHAOTIC_S2)
+                     and out["chaotic_share"] <= CHAOTIC_S2
+                     and (worst is None or worst <= CHAOTIC_S2))
     return out
 
 

@@ -606,6 +606,87 @@ __device__ __forceinline__ F3 unit_point(const PenUnit &x, uint32_t i) {
   return {float(a), float(b), float(c)};
 }
 
+// The +axis ray parity of every active lane's point (RayScene::crossings,
+// spatial/bvh.rs:160-175, under crossings_axis's rule), the 32 lanes sharing
+// the work: each lane's grid cell is a run of entries, the runs of the warp are
+// laid end to end (a prefix sum of their lengths), and every round each lane
+// tests the next entry of that flattened list for its owner (the last lane
+// whose run starts at or before it). Rounds therefore keep every lane busy
+// however unevenly the cells are filled, and the lanes of one owner read its
+// run's rectangles as consecutive, coalesced loads. A crossing toggles the
+// owner's bit in the warp's parity word; `axis` is the same for the warp.
+__device__ __forceinline__ uint32_t warp_crossings(const MeshView *m, F3 p, int axis, bool active,
+                                                   unsigned *par_word) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  uint32_t b = 0, len = 0;
+  unsigned long long rect = 0, tri = 0;
+  if (active && m->nf) {
+    const AxisGrid &g = m->grid[axis];
+    float pc[3] = {p.x, p.y, p.z};
+    float pu = pc[(axis + 1) % 3], pv = pc[(axis + 2) % 3];
+    float fu = floorf((pu - g.lo_u) * g.inv_cell), fv = floorf((pv - g.lo_v) * g.inv_cell);
+    if (fu >= 0.0f && fv >= 0.0f && fu < float(g.nu) && fv < float(g.nv)) {
+      size_t cell = size_t(fu) * g.nv + size_t(fv);
+      b = __ldg(g.start + cell);
+      len = __ldg(g.start + cell + 1) - b;
+      rect = reinterpret_cast<unsigned long long>(g.rect);
+      tri = reinterpret_cast<unsigned long long>(g.tri);
+    }
+  }
+  uint32_t incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t off = incl - len, total = __shfl_sync(FULL, incl, 31);
+  if (lane == 0) *par_word = 0u;
+  __syncwarp();
+  const F3 d = {axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f};
+  for (uint32_t base = 0; base < total; base += 32) {
+    const uint32_t w = base + lane;
+    int j = 0;  // the last lane whose run starts at or before w (off[0] = 0 <= w)
+#pragma unroll
+    for (int step = 16; step; step >>= 1)
+      if (__shfl_sync(FULL, off, j + step) <= w) j += step;
+    const float qx = __shfl_sync(FULL, p.x, j), qy = __shfl_sync(FULL, p.y, j),
+                qz = __shfl_sync(FULL, p.z, j);
+    const uint32_t bj = __shfl_sync(FULL, b, j), oj = __shfl_sync(FULL, off, j);
+    const float4 *rj = reinterpret_cast<const float4 *>(__shfl_sync(FULL, rect, j));
+    const float4 *tj = reinterpret_cast<const float4 *>(__shfl_sync(FULL, tri, j));
+    if (w < total) {
+      const size_t k = size_t(bj) + (w - oj);
+      const float qc[3] = {qx, qy, qz};
+      const float qu = qc[(axis + 1) % 3], qv = qc[(axis + 2) % 3];
+      const float4 r = __ldg(rj + k);
+      if (!(qu < r.x || qu > r.y || qv < r.z || qv > r.w)) {
+        const float4 t0 = __ldg(tj + 3 * k), t1 = __ldg(tj + 3 * k + 1), t2 = __ldg(tj + 3 * k + 2);
+        if (moller_trumbore_edges({qx, qy, qz}, d, {t0.x, t0.y, t0.z}, {t1.x, t1.y, t1.z},
+                                  {t2.x, t2.y, t2.z}) >= 0.0f)
+          atomicXor(par_word, 1u << j);
+      }
+    }
+  }
+  __syncwarp();
+  const uint32_t bits = *par_word;
+  __syncwarp();
+  return (bits >> lane) & 1u;
+}
+
+// RayScene::inside (spatial/bvh.rs:146-157) for every lane's point at once, by
+// warp_crossings: the majority of the three parities, the third ray cast only
+// for the lanes whose first two disagree.
+__device__ __forceinline__ bool warp_inside(const MeshView *m, F3 p, bool active,
+                                            unsigned *par_word) {
+  const uint32_t a = warp_crossings(m, p, 0, active, par_word);
+  const uint32_t b = warp_crossings(m, p, 1, active, par_word);
+  const bool third = active && a != b;
+  uint32_t c = 0;
+  if (__any_sync(0xffffffffu, third)) c = warp_crossings(m, p, 2, third, par_word);
+  return active && (a == b ? a != 0u : c != 0u);
+}
+
 __global__ void k_pen_init(PenState ps) {
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < ps.n_units; u += gridDim.x * blockDim.x) {
     ps.deeper[u] = 0;
@@ -621,21 +702,47 @@ __global__ void __launch_bounds__(256) k_pen_inside(const PairView *pairs, const
                                                     const uint32_t *abort_flag,
                                                     unsigned long long budget, uint32_t *status) {
   __shared__ WarpQueue wqs[8];
+  __shared__ unsigned parity[8];
   WarpQueue &q = wqs[threadIdx.x >> 5];
+  unsigned *par_word = parity + (threadIdx.x >> 5);
   int lane = threadIdx.x & 31;
   if (lane == 0) q.n_box = q.n_in = 0;
   __syncwarp();
   uint32_t st = 0;
   unsigned long long start = global_ns();
+  // An inside point's depth D (its distance to the mesh) enters the unit's
+  // statistics twice: whether D > pen, and the unit's deepest D. Both are
+  // exact without the full nearest-face search of every point. With w the
+  // largest f32 <= pen (so D > pen exactly when D > w): the bound grid or a
+  // walk that stops at the first face within w decides "deeper"; then the
+  // point can only raise the running maximum M if no face lies within M, and
+  // only then is D itself searched (within w when not deeper, unbounded
+  // otherwise; the same value mesh_distance gives). M only ever holds depths
+  // of inside points, so the last point to raise it holds the true maximum.
   auto depth_stage = [&](bool drain) {
     while (q.n_in >= 32 || (drain && q.n_in > 0)) {
       unsigned long long e;
       if (wq_pop(q.in, &q.n_in, e)) {
         uint32_t u = uint32_t(e >> 32), i = uint32_t(e);
         PenUnit x = pen_unit(pairs, items, cands, inv, u);
-        float depth = mesh_distance(*x.mesh, unit_point(x, i), f_inf(), st);
-        atomicMax(&ps.deep[u], f2key(depth) + 1u);
-        if (double(depth) > x.pen) atomicAdd(&ps.deeper[u], 1u);
+        const MeshView &m = *x.mesh;
+        F3 p = unit_point(x, i);
+        const float w = __double2float_rd(x.pen);
+        const bool deeper = !(mesh_may_reach(m, p, w) && mesh_any_within(m, p, w, st));
+        if (deeper) atomicAdd(&ps.deeper[u], 1u);
+        const unsigned key = *((volatile unsigned *)&ps.deep[u]);
+        bool raise = true;
+        if (key != 0u) {
+          const float top = key2f(key - 1u);
+          if (!deeper && top >= w)
+            raise = false;  // D <= w <= M
+          else if (mesh_may_reach(m, p, top) && mesh_any_within(m, p, top, st))
+            raise = false;  // D <= M
+        }
+        if (raise) {
+          float depth = mesh_distance(m, p, deeper ? f_inf() : w, st);
+          atomicMax(&ps.deep[u], f2key(depth) + 1u);
+        }
       }
     }
   };
@@ -643,12 +750,15 @@ __global__ void __launch_bounds__(256) k_pen_inside(const PairView *pairs, const
     while (q.n_box >= 32 || (drain && q.n_box > 0)) {
       unsigned long long e = 0;
       bool got = wq_pop(q.box, &q.n_box, e);
-      bool inside = false;
+      F3 p = {0.0f, 0.0f, 0.0f};
+      const MeshView *m = nullptr;
       if (got) {
         uint32_t u = uint32_t(e >> 32), i = uint32_t(e);
         PenUnit x = pen_unit(pairs, items, cands, inv, u);
-        inside = inside_mesh(*x.mesh, unit_point(x, i), st);
+        p = unit_point(x, i);
+        m = x.mesh;
       }
+      bool inside = warp_inside(m, p, got, par_word);
       wq_push(q.in, &q.n_in, inside, e);
       depth_stage(false);
     }
@@ -731,7 +841,9 @@ __global__ void __launch_bounds__(256) k_pen_min(const PairView *pairs, const sh
       float pc[3] = {p.x, p.y, p.z};
       float window = key2f(*((volatile unsigned *)&ps.best[u]));
       float gap = sqrtf(box_dist2(x.mesh->lo, x.mesh->hi, pc));
-      want = !(gap > window + 1e-5f * window + x.mesh->pad);
+      // The window only shrinks, so a point the bound grid puts out of reach
+      // now stays out of reach when its query would run.
+      want = !(gap > window + 1e-5f * window + x.mesh->pad) && mesh_may_reach(*x.mesh, p, window);
     }
     wq_push(q.box, &q.n_box, want, (unsigned long long)u << 32 | i);
     query_stage(false);

@@ -39,6 +39,17 @@ struct AxisGrid {
   uint32_t nu, nv;
 };
 
+// The mesh's bound grid: a cube-celled grid over the mesh's box widened by a
+// quarter of its largest extent on every side, holding per cell a lower bound
+// (rounded down) on the distance from any point of the cell to any leaf box of
+// the tree, and so to any face. Null `lb` when the mesh is a single leaf.
+struct LbGrid {
+  const float *lb;
+  float lo[3];
+  float cell, inv_cell;
+  uint32_t n[3];
+};
+
 // What the traversal kernels take by value.
 struct MeshView {
   const BNode *nodes;
@@ -48,6 +59,7 @@ struct MeshView {
   float pad;           // outward padding of every node box
   float lo[3], hi[3];  // exact vertex box (RayScene::aabb)
   AxisGrid grid[3];    // crossing grids for the +x, +y, +z parity rays
+  LbGrid lbg;          // lower bounds of the distance to the mesh, per cell
 };
 
 struct CloudView {
@@ -380,6 +392,86 @@ __global__ void k_grid_fill(const float4 *tri, uint32_t nf, int axis, AxisGrid g
       edge[3 * size_t(k) + 1] = t1;
       edge[3 * size_t(k) + 2] = t2;
     }
+}
+
+// One thread per cell of the bound grid: the smallest box-to-box distance
+// from the cell (widened by 1e-3 cell on every side) to a leaf box of the
+// tree, every step rounded down, by a nearest-first walk that skips subtrees
+// whose box is no nearer than the best so far.
+__global__ void k_lb_grid(const BNode *nodes, LbGrid g, float *lb) {
+  size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  size_t total = size_t(g.n[0]) * g.n[1] * g.n[2];
+  if (c >= total) return;
+  uint32_t iz = uint32_t(c % g.n[2]), iy = uint32_t((c / g.n[2]) % g.n[1]),
+           ix = uint32_t(c / (size_t(g.n[2]) * g.n[1]));
+  const uint32_t idx[3] = {ix, iy, iz};
+  float clo[3], chi[3];
+  for (int a = 0; a < 3; ++a) {
+    clo[a] = __fsub_rd(__fadd_rd(g.lo[a], __fmul_rd(float(idx[a]), g.cell)), 1e-3f * g.cell);
+    chi[a] = __fadd_ru(__fadd_ru(g.lo[a], __fmul_ru(float(idx[a] + 1), g.cell)), 1e-3f * g.cell);
+  }
+  auto gap2 = [&](const float4 &a, const float4 &b, const float4 &cc, int child) {
+    float blo[3], bhi[3];
+    if (child == 0) {
+      blo[0] = a.x; blo[1] = a.y; blo[2] = a.z; bhi[0] = a.w; bhi[1] = b.x; bhi[2] = b.y;
+    } else {
+      blo[0] = b.z; blo[1] = b.w; blo[2] = cc.x; bhi[0] = cc.y; bhi[1] = cc.z; bhi[2] = cc.w;
+    }
+    float s = 0.0f;
+    for (int k = 0; k < 3; ++k) {
+      float d = fmaxf(fmaxf(__fsub_rd(blo[k], chi[k]), __fsub_rd(clo[k], bhi[k])), 0.0f);
+      s = __fadd_rd(s, __fmul_rd(d, d));
+    }
+    return s;
+  };
+  float best = f_inf();
+  int stack_n[STACK];
+  float stack_k[STACK];
+  int sp = 0, node = 0;
+  for (int visits = 0; visits < (1 << 22); ++visits) {
+    const float4 *q = reinterpret_cast<const float4 *>(nodes + node);
+    float4 a = q[0], b = q[1], cc = q[2];
+    int4 d = reinterpret_cast<const int4 *>(q)[3];
+    const int ref[2] = {d.x, d.y}, cnt[2] = {d.z, d.w};
+    float k[2] = {gap2(a, b, cc, 0), gap2(a, b, cc, 1)};
+    int near_c = k[1] < k[0] ? 1 : 0;
+    int next = -1;
+    for (int qq = 0; qq < 2; ++qq) {
+      int ch = qq == 0 ? near_c : 1 - near_c;
+      if (!(k[ch] < best)) continue;
+      if (cnt[ch]) {
+        best = k[ch];
+      } else if (next < 0) {
+        next = ref[ch];
+      } else if (sp < STACK) {
+        stack_n[sp] = ref[ch];
+        stack_k[sp++] = k[ch];
+      } else {
+        best = 0.0f;  // out of stack: the bound falls back to 0 (no pruning)
+        sp = 0;
+        next = -1;
+        break;
+      }
+    }
+    if (next >= 0) {
+      node = next;
+      continue;
+    }
+    bool more = false;
+    while (sp > 0) {
+      --sp;
+      if (stack_k[sp] < best) {
+        node = stack_n[sp];
+        more = true;
+        break;
+      }
+    }
+    if (!more) {
+      lb[c] = best == f_inf() ? 0.0f : __fsqrt_rd(best);
+      return;
+    }
+  }
+  lb[c] = 0.0f;  // walk cap reached: no bound
 }
 
 __global__ void k_store_tris(const float *v, const uint32_t *f, const uint32_t *sorted, uint32_t nf,

@@ -203,6 +203,7 @@ struct sherd_mesh {
   DBuf<float4> tri;
   DBuf<uint32_t> gstart[3];
   DBuf<float4> grect[3], gtri[3];
+  DBuf<float> lb;            // the bound grid's cells
   MeshView view{};
 };
 
@@ -396,6 +397,31 @@ int mesh_build(sherd_ctx *ctx, sherd_mesh *m) {
   for (int k = 0; k < 3; ++k) {
     v.lo[k] = vlo[k];
     v.hi[k] = vhi[k];
+  }
+  // The bound grid (LbGrid): cube cells, 64 across the largest extent of the
+  // vertex box widened by a quarter of that extent on every side.
+  v.lbg = LbGrid{};
+  if (!v.root_leaf && nf > 0) {
+    double mx = 0.0;
+    for (int k = 0; k < 3; ++k) mx = std::max(mx, double(vhi[k]) - double(vlo[k]));
+    const double margin = 0.25 * mx + 2.0 * double(pad);
+    const double cell = (mx + 2.0 * margin) / 64.0;
+    if (cell > 0.0 && std::isfinite(cell)) {
+      LbGrid g{};
+      size_t total = 1;
+      for (int k = 0; k < 3; ++k) {
+        g.lo[k] = std::nextafter(float(double(vlo[k]) - margin), -f_inf());
+        g.n[k] = uint32_t(std::ceil((double(vhi[k]) - double(vlo[k]) + 2.0 * margin) / cell)) + 1;
+        total *= g.n[k];
+      }
+      g.cell = float(cell);
+      g.inv_cell = float(1.0 / double(g.cell));
+      CK(m->lb.alloc(total));
+      k_lb_grid<<<unsigned((total + 255) / 256), 256, 0, ctx->stream>>>(m->nodes.p, g, m->lb.p);
+      CK(cudaGetLastError());
+      g.lb = m->lb.p;
+      v.lbg = g;
+    }
   }
   return SHERD_OK;
 }

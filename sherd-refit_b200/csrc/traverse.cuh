@@ -280,6 +280,85 @@ __device__ __noinline__ float mesh_distance(const MeshView &m, F3 p, float windo
   return best;
 }
 
+// Whether some face lies within `window` of p (inclusive): the same walk as
+// mesh_distance with its bound held at the window, stopping at the first face
+// found. True exactly when mesh_distance(m, p, window) would be finite, so a
+// caller that only needs "within the window or not" is spared the rest of the
+// nearest-face search.
+__device__ __noinline__ bool mesh_any_within(const MeshView &m, F3 p, float window,
+                                             uint32_t &status) {
+  if (m.nf == 0 || !(window >= 0.0f)) return false;
+  const float pc[3] = {p.x, p.y, p.z};
+  auto test = [&](int first, int count) {
+    for (int s = first; s < first + count; ++s) {
+      F3 a, b, c;
+      uint32_t id;
+      tri_at(m, s, a, b, c, id);
+      if (tri_distance(p, a, b, c) <= window) return true;
+    }
+    return false;
+  };
+  if (m.root_leaf) return test(0, int(m.root_leaf));
+  const float s = window + 4e-6f * window + m.pad;
+  const float bound2 = s * s;
+  int stack_n[STACK];
+  int sp = 0, node = 0;
+  uint32_t visits = 0;
+  for (;;) {
+    if (++visits > 2u * m.nf + 64u) {
+      status |= ST_STACK;
+      return false;
+    }
+    Child2 n = load_node(m.nodes, node);
+    float k[2] = {box_dist2(n.lo0, n.hi0, pc), box_dist2(n.lo1, n.hi1, pc)};
+    int near_c = k[1] < k[0] ? 1 : 0;
+    int next = -1;
+    for (int q = 0; q < 2; ++q) {
+      int c = q == 0 ? near_c : 1 - near_c;
+      if (!(k[c] <= bound2)) continue;
+      if (n.cnt[c]) {
+        if (test(n.ref[c], n.cnt[c])) return true;
+      } else if (next < 0) {
+        next = n.ref[c];
+      } else if (sp < STACK) {
+        stack_n[sp++] = n.ref[c];
+      } else {
+        status |= ST_STACK;
+      }
+    }
+    if (next >= 0) {
+      node = next;
+      continue;
+    }
+    if (sp == 0) return false;
+    node = stack_n[--sp];
+  }
+}
+
+// A lower bound on the distance from p to every face of the mesh, read from
+// the mesh's bound grid (0 where p is off the grid or the mesh has none): the
+// smallest distance from p's grid cell, widened by a thousandth of a cell, to
+// any leaf box of the tree, rounded down. A walk whose bound stays below it
+// scores no leaf.
+__device__ __forceinline__ float mesh_lower_bound(const MeshView &m, F3 p) {
+  const LbGrid &g = m.lbg;
+  if (!g.lb) return 0.0f;
+  float fx = floorf((p.x - g.lo[0]) * g.inv_cell), fy = floorf((p.y - g.lo[1]) * g.inv_cell),
+        fz = floorf((p.z - g.lo[2]) * g.inv_cell);
+  if (!(fx >= 0.0f && fy >= 0.0f && fz >= 0.0f && fx < float(g.n[0]) && fy < float(g.n[1]) &&
+        fz < float(g.n[2])))
+    return 0.0f;
+  return __ldg(g.lb + (size_t(fx) * g.n[1] + size_t(fy)) * g.n[2] + size_t(fz));
+}
+
+// Whether a walk bounded at `window` (mesh_distance, mesh_any_within) from p
+// can score a face at all: false when the mesh's bound grid puts every leaf
+// box beyond the walk's padded bound, with a relative margin of 1e-4 over the
+// rounding of the walk's own box distances.
+__device__ __forceinline__ bool mesh_may_reach(const MeshView &m, F3 p, float window) {
+  return !(mesh_lower_bound(m, p) > (window + 4e-6f * window + m.pad) * 1.0001f);
+}
+
 // mesh_distance that also names the face: the sorted slot of the nearest face
 // within the window, an exact f32 tie going to the lowest original face id
 // (the rule first_hit uses); slot = MISS when nothing is within the window.

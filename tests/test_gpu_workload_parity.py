@@ -46,6 +46,7 @@ def _check(sherd, gpu_ctx, oracle, config, pairs=None):
     assert res["determined_status_mismatch"] == 0, res
     assert res["determined_verdict_mismatch"] == 0, res
     assert res["determined_past_bound"] == 0, res
+    assert res["chaotic_share_worst_pair"] is not None, res
     assert res["chaotic_share_worst_pair"] <= parity.CHAOTIC_S2, res
     assert res["ok"], res
     del keep
