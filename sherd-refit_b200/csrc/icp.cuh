@@ -404,9 +404,10 @@ template <class H>
 __device__ void icp_pass(const double4 *src, uint32_t ns, const CloudView &tgt, double r2,
                          bool valid, IcpShared &sh, H *hint, uint32_t &status,
                          bool point_to_point = false) {
-  double t[12];
-#pragma unroll
-  for (int k = 0; k < 12; ++k) t[k] = sh.t[k];
+  // The pose is read from shared memory where it is used (a broadcast load):
+  // twelve doubles held in registers across the search and the accumulation
+  // would cost 24 registers that the ladder's occupancy cannot spare.
+  const double *t = sh.t;
   // Two kinds of loops over the moving points, so that the 29 accumulators are
   // never live across the nearest-neighbour search: the first finds every
   // point's match (kept in hint[i], which also warm-starts the next pass), the

@@ -507,6 +507,7 @@ struct PenState {
   unsigned *deep;      // per unit: f2key(deepest depth) + 1, 0 when nothing is inside
   unsigned *best;      // per unit: f2key(smallest distance) for the nothing-inside case
   const uint32_t *chunk0;  // per unit: its first chunk in the flat list (n_units + 1)
+  const uint32_t *coarse;  // the unit of every 256th chunk (chunk k << 8)
   uint32_t n_units, n_chunks;
 };
 
@@ -535,13 +536,13 @@ __device__ __forceinline__ PenUnit pen_unit(const PairView *pairs, const sherd_w
   return x;
 }
 
+// The unit a chunk belongs to: the unit of the last 256-chunk mark before it,
+// then forward over the units that start at or before it (units without
+// chunks included).
 __device__ __forceinline__ uint32_t unit_of_chunk(const PenState &ps, uint32_t chunk) {
-  uint32_t lo = 0, hi = ps.n_units;  // last unit with chunk0[u] <= chunk
-  while (hi - lo > 1) {
-    uint32_t mid = (lo + hi) >> 1;
-    if (__ldg(ps.chunk0 + mid) <= chunk) lo = mid; else hi = mid;
-  }
-  return lo;
+  uint32_t u = __ldg(ps.coarse + (chunk >> 8));
+  while (__ldg(ps.chunk0 + u + 1) <= chunk) ++u;
+  return u;
 }
 
 struct WarpQueue {
@@ -597,6 +598,57 @@ __device__ __forceinline__ bool take_chunk(unsigned *head, uint32_t n_chunks,
   }
   chunk = __shfl_sync(0xffffffffu, c, 0);
   return chunk < n_chunks;
+}
+
+// k_pen_inside takes its chunks in runs: CHUNK_RUN consecutive chunks (of
+// one unit, mostly) per atomic, the unit of each following from the previous
+// one. A unit is then shared by a few dozen warps rather than hundreds, so the
+// running deepest depth its points are checked against is known early, and
+// few points need their depth searched exactly.
+#ifndef PEN_CHUNK_RUN
+#define PEN_CHUNK_RUN 64
+#endif
+constexpr uint32_t CHUNK_RUN = PEN_CHUNK_RUN;
+
+struct ChunkRun {
+  uint32_t next = 0, end = 0;       // chunks [next, end) still to do
+  uint32_t unit = 0, unit_end = 0;  // the unit of `next` and the first chunk after it
+  uint32_t taken = 0;               // runs taken (the abort flag is polled every 8)
+};
+
+__device__ __forceinline__ bool next_chunk(ChunkRun &r, const PenState &ps, unsigned *head,
+                                           const uint32_t *abort_flag, unsigned long long budget,
+                                           unsigned long long start, uint32_t &chunk, uint32_t &u,
+                                           uint32_t &st) {
+  if (r.next >= r.end) {
+    uint32_t c = 0xFFFFFFFFu;
+    if ((threadIdx.x & 31) == 0) {
+      bool stop = false;
+      if ((r.taken++ & 7u) == 0u) {
+        if (abort_flag && *((volatile const uint32_t *)abort_flag)) {
+          st |= ST_ABORTED;
+          stop = true;
+        } else if (budget && global_ns() - start > budget) {
+          st |= ST_TIMEOUT;
+          stop = true;
+        }
+      }
+      if (!stop) c = atomicAdd(head, CHUNK_RUN);
+    }
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= ps.n_chunks) return false;
+    r.next = c;
+    r.end = min(c + CHUNK_RUN, ps.n_chunks);
+    r.unit = unit_of_chunk(ps, c);
+    r.unit_end = __ldg(ps.chunk0 + r.unit + 1);
+  }
+  chunk = r.next++;
+  while (chunk >= r.unit_end) {
+    ++r.unit;
+    r.unit_end = __ldg(ps.chunk0 + r.unit + 1);
+  }
+  u = r.unit;
+  return true;
 }
 
 __device__ __forceinline__ F3 unit_point(const PenUnit &x, uint32_t i) {
@@ -763,9 +815,9 @@ __global__ void __launch_bounds__(256) k_pen_inside(const PairView *pairs, const
       depth_stage(false);
     }
   };
-  uint32_t chunk, taken = 0;
-  while (take_chunk(head, ps.n_chunks, abort_flag, budget, start, taken, chunk, st)) {
-    uint32_t u = unit_of_chunk(ps, chunk);
+  ChunkRun run;
+  uint32_t chunk, u;
+  while (next_chunk(run, ps, head, abort_flag, budget, start, chunk, u, st)) {
     PenUnit x = pen_unit(pairs, items, cands, inv, u);
     uint32_t i = (chunk - ps.chunk0[u]) * 32u + lane;
     bool in_box = false;

@@ -1408,7 +1408,7 @@ struct sherd_batch {
   // unit its counters and its first chunk.
   DBuf<double> inv;
   DBuf<unsigned> deeper, deep, best, pen_heads;
-  DBuf<uint32_t> chunk0;
+  DBuf<uint32_t> chunk0, coarse;
   uint32_t n_chunks = 0;
   unsigned grid_p = 1, grid_m = 1;
   unsigned grid_l = 1, grid_v = 1;
@@ -1480,7 +1480,8 @@ int launch_verify_items(sherd_batch *b, cudaStream_t s) {
 }
 
 PenState pen_state(sherd_batch *b) {
-  return PenState{b->deeper.p, b->deep.p, b->best.p, b->chunk0.p, 2 * b->n_items, b->n_chunks};
+  return PenState{b->deeper.p, b->deep.p, b->best.p, b->chunk0.p, b->coarse.p, 2 * b->n_items,
+                  b->n_chunks};
 }
 
 int launch_pen_inside(sherd_batch *b, cudaStream_t s) {
@@ -1624,6 +1625,15 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
     chunk0[2 * size_t(n_items)] = uint32_t(acc);
     b->n_chunks = uint32_t(acc);
     if ((rc = upload(ctx, b->chunk0, chunk0.data(), chunk0.size()))) return rc;
+    // The unit of every 256th chunk: the last unit starting at or before it.
+    std::vector<uint32_t> coarse((size_t(acc) >> 8) + 1);
+    uint32_t cu = 0;
+    for (size_t k = 0; k < coarse.size(); ++k) {
+      uint64_t c = uint64_t(k) << 8;
+      while (cu + 1 < 2 * n_items && chunk0[cu + 1] <= c) ++cu;
+      coarse[k] = cu;
+    }
+    if ((rc = upload(ctx, b->coarse, coarse.data(), coarse.size()))) return rc;
     CK(b->inv.alloc(16 * size_t(n_items)));
     CK(b->deeper.alloc(2 * size_t(n_items)));
     CK(b->deep.alloc(2 * size_t(n_items)));
