@@ -6,7 +6,8 @@
 // radius (exact, lowest index on ties), and accumulate the correspondence
 // count, the squared error and the 27 normal-equation terms (21 of the lower
 // triangle of J^T J, 6 of J^T r) in f64 registers. A pass ends with a warp
-// shuffle tree and a fixed-order sum over the warps, so a rung is bit-for-bit
+// shuffle tree and a fixed-order sum over the warps, both compensated (TwoSum,
+// the rounding errors carried and added once), so a rung is bit-for-bit
 // reproducible run to run. One thread then runs Open3D's convergence test,
 // Eigen's pivoted LDLT (f64) and the Rz Ry Rx update, and publishes the pose.
 //
@@ -25,6 +26,7 @@ constexpr int ICP_SUMS = 29;  // count, err2, jtj[21], jtr[6]
 
 struct IcpShared {
   double red[ICP_BLOCK / 32][ICP_SUMS];
+  double carry[ICP_BLOCK / 32][ICP_SUMS];  // the rounding errors of red's warp sums
   double sums[ICP_SUMS];
   double t[16];
   int stop;
@@ -266,6 +268,31 @@ __device__ __noinline__ void point_step(IcpShared &sh) {
   matmul4(u, sh.t, sh.t);
 }
 
+// Knuth's TwoSum: s = fl(a + b) and the exact rounding error e, a + b = s + e
+// (no multiply-add is contracted in this build, so the identity holds).
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
+  s = a + b;
+  double bp = s - a;
+  e = (a - (s - bp)) + (b - bp);
+}
+
+// The sum of x over the warp for lane 0, compensated: the shuffle tree adds
+// the 32 partials pairwise and carries every addition's rounding error
+// (TwoSum) beside it; returns the sum and the carried error separately.
+__device__ __forceinline__ void warp_sum_compensated(double x, double &sum, double &carry) {
+  double c = 0.0;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    double y = __shfl_down_sync(0xffffffffu, x, o), cy = __shfl_down_sync(0xffffffffu, c, o);
+    double s, e;
+    two_sum(x, y, s, e);
+    x = s;
+    c = (c + cy) + e;
+  }
+  sum = x;
+  carry = c;
+}
+
 // A source point's match (a target slot, or -1) as the pass keeps it: an int,
 // or 16 bits (0xFFFF for none) when every target of the batch has fewer than
 // 65535 points, which halves the bytes the ladder writes and re-reads.
@@ -326,9 +353,12 @@ __device__ __forceinline__ void icp_accumulate(const double4 *src, uint32_t ns, 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < E - B; ++k) {
-    double x = acc[k];
-    for (int o = 16; o; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) sh.red[warp][B + k] = x;
+    double x, c;
+    warp_sum_compensated(acc[k], x, c);
+    if (lane == 0) {
+      sh.red[warp][B + k] = x;
+      sh.carry[warp][B + k] = c;
+    }
   }
 }
 
@@ -379,19 +409,30 @@ __device__ __forceinline__ void p2p_accumulate(const double4 *src, uint32_t ns,
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    double x = acc[k];
-    for (int o = 16; o; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) sh.red[warp][B + k] = x;
+    double x, c;
+    warp_sum_compensated(acc[k], x, c);
+    if (lane == 0) {
+      sh.red[warp][B + k] = x;
+      sh.carry[warp][B + k] = c;
+    }
   }
 }
 
-// sh.sums[lo..hi) from the warps' partial sums, in warp order.
+// sh.sums[lo..hi) from the warps' partial sums, in warp order: the final sum
+// of the partials is compensated (TwoSum over the warps' sums, their carried
+// errors added once at the end), so the block total is the partials' exact
+// sum up to a last rounding whatever their magnitudes.
 __device__ __forceinline__ void reduce_sums(IcpShared &sh, int lo, int hi) {
   __syncthreads();
   if (int(threadIdx.x) >= lo && int(threadIdx.x) < hi) {
-    double v = sh.red[0][threadIdx.x];
-    for (int w = 1; w < ICP_BLOCK / 32; ++w) v += sh.red[w][threadIdx.x];
-    sh.sums[threadIdx.x] = v;
+    double v = sh.red[0][threadIdx.x], c = sh.carry[0][threadIdx.x];
+    for (int w = 1; w < ICP_BLOCK / 32; ++w) {
+      double s, e;
+      two_sum(v, sh.red[w][threadIdx.x], s, e);
+      v = s;
+      c = (c + sh.carry[w][threadIdx.x]) + e;
+    }
+    sh.sums[threadIdx.x] = v + c;
   }
   __syncthreads();
 }
