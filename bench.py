@@ -811,7 +811,11 @@ def main():
                 "timer": ("host wall clock around the synchronous C-ABI call and the candidate "
                           "all-gather (max over ranks); bytes per rank"),
                 "matches_resident_run": same},
-        "gpu_launches": 7 * args.steps,
+        "gpu_launches": 9 * args.steps,
+        "gpu_launches_counts": ("per step: k_ladder once per point-count bucket (3), "
+                                "k_verify_items, k_pen_init, k_pen_inside, k_pen_seed, k_pen_min, "
+                                "k_pen_finalize"),
+        "ladder_autotune": ctx.stats().get("ladder_autotune"),
         "nn_queries": nn_query_rates(sbytes, stage_ms, step_ms, total_q),
         "roofline": roofline,
         "plain": plain,

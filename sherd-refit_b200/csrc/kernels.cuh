@@ -349,11 +349,12 @@ __global__ void k_penetration_share(MeshView m, const double *pts, uint32_t n, P
 
 // ---- the batched stage-2 path ----------------------------------------------------
 
-// Resident ladder CTAs per SM the register budget is cut for (65536 / (ICP_BLOCK * this)
-// registers a thread at most).
-#ifndef LADDER_BLOCKS_PER_SM
-#define LADDER_BLOCKS_PER_SM 10
-#endif
+// Resident ladder CTAs per SM a k_ladder variant's register budget is cut for
+// (65536 / (ICP_BLOCK * MINB) registers a thread at most). The batch picks a
+// variant per point-count bucket (the autotuner in sherd.cu); the last is the
+// default.
+constexpr int LADDER_VARIANTS = 3;
+constexpr int LADDER_MINB[LADDER_VARIANTS] = {6, 8, 10};
 
 struct QueueCtl {
   unsigned *head;             // next queue position to take
@@ -390,8 +391,8 @@ __device__ __forceinline__ bool take(const QueueCtl &q, unsigned long long start
 // (ladder.rs:142-161): from the item's start pose when r_lo is 0, else from
 // its rung r_lo - 1. With skip_partial, items an early rejection left partial
 // are passed over.
-template <class H>
-__global__ void __launch_bounds__(ICP_BLOCK, LADDER_BLOCKS_PER_SM) k_ladder(const PairView *pairs,
+template <class H, int MINB>
+__global__ void __launch_bounds__(ICP_BLOCK, MINB) k_ladder(const PairView *pairs,
                                                       const sherd_work_item *items, QueueCtl q,
                                                       H *hints, size_t hint_stride,
                                                       sherd_candidate *out, int r_lo, int r_hi,

@@ -55,6 +55,16 @@ struct sherd_ctx {
   uint32_t *abort_dev = nullptr;
   uint32_t *d_status = nullptr;
   std::map<std::string, MethodStats> stats;
+  // Two more streams and their events, to run the ladder's point-count buckets
+  // side by side inside the captured ladder graph.
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
+  // The ladder autotuner's choices on this context's device: per point-count
+  // bucket the k_ladder variant (-1 until tuned), the timings it was chosen
+  // from and the sample they were taken on.
+  int ladder_tuned[3] = {-1, -1, -1};
+  float ladder_tune_ms[3][3] = {};
+  uint32_t ladder_tune_items[3] = {};
 };
 
 // Working memory of sherd_icp_rung_noalloc: each source point's last match, for
@@ -559,6 +569,11 @@ int sherd_open(int device, sherd_ctx **out) {
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bad(e);
   if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess) return bad(e);
   if ((e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) return bad(e);
+  for (int k = 0; k < 2; ++k) {
+    if ((e = cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking)) != cudaSuccess) return bad(e);
+    if ((e = cudaEventCreateWithFlags(&ctx->join_ev[k], cudaEventDisableTiming)) != cudaSuccess) return bad(e);
+  }
+  if ((e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming)) != cudaSuccess) return bad(e);
   if ((e = cudaHostAlloc(&ctx->abort_host, 4, cudaHostAllocMapped)) != cudaSuccess) return bad(e);
   *ctx->abort_host = 0;
   if ((e = cudaHostGetDevicePointer(&ctx->abort_dev, ctx->abort_host, 0)) != cudaSuccess) return bad(e);
@@ -575,6 +590,11 @@ int sherd_close(sherd_ctx *ctx) {
   if (ctx->abort_host) cudaFreeHost(ctx->abort_host);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  for (int k = 0; k < 2; ++k) {
+    if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
+    if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
+  }
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   t_errors.erase(ctx);
   delete ctx;
@@ -613,6 +633,16 @@ int sherd_stats_json(sherd_ctx *ctx, char *buf, size_t len) {
                   (unsigned long long)kv.second.items, kv.second.ms);
     s += tmp;
     firstm = false;
+  }
+  s += "}, \"ladder_autotune\": {";
+  for (int b = 0; b < 3; ++b) {
+    char tmp[256];
+    int v = ctx->ladder_tuned[b];
+    std::snprintf(tmp, sizeof tmp,
+                  "%s\"bucket%d\": {\"ctas_per_sm\": %d, \"sample_items\": %u, \"ms\": [%.3f, %.3f, %.3f]}",
+                  b ? ", " : "", b, v >= 0 ? LADDER_MINB[v] : -1, ctx->ladder_tune_items[b],
+                  ctx->ladder_tune_ms[b][0], ctx->ladder_tune_ms[b][1], ctx->ladder_tune_ms[b][2]);
+    s += tmp;
   }
   s += "}}";
   if (s.size() + 1 > len) return fail(ctx, SHERD_E_INVALID, "stats buffer too small");
@@ -1388,17 +1418,44 @@ struct sherd_batch {
   DBuf<unsigned char> hints;
   bool hint16 = true;
   size_t hint_stride = 1;
-  // Launches the ladder kernel (rungs r_lo..r_hi-1) with the batch's hint width.
-  void ladder(unsigned grid, QueueCtl q, cudaStream_t s, int r_lo, int r_hi, int skip_partial) {
-    if (hint16)
-      k_ladder<uint16_t><<<grid, ICP_BLOCK, 0, s>>>(dv.p, di.p, q,
-                                                    reinterpret_cast<uint16_t *>(hints.p),
-                                                    hint_stride, dc.p, r_lo, r_hi, skip_partial,
-                                                    ctx->d_status);
+  // Launches k_ladder variant v (rungs r_lo..r_hi-1) with the batch's hint
+  // width, its CTAs using the hint slots from slot0 on.
+  template <class H, int MINB>
+  void ladder_as(unsigned grid, QueueCtl q, cudaStream_t s, int r_lo, int r_hi, int skip_partial,
+                 size_t slot0) {
+    H *h = reinterpret_cast<H *>(hints.p) + slot0 * hint_stride;
+    k_ladder<H, MINB><<<grid, ICP_BLOCK, 0, s>>>(dv.p, di.p, q, h, hint_stride, dc.p, r_lo, r_hi,
+                                                 skip_partial, ctx->d_status);
+  }
+  template <class H>
+  void ladder_h(int v, unsigned grid, QueueCtl q, cudaStream_t s, int r_lo, int r_hi,
+                int skip_partial, size_t slot0) {
+    if (v == 0)
+      ladder_as<H, LADDER_MINB[0]>(grid, q, s, r_lo, r_hi, skip_partial, slot0);
+    else if (v == 1)
+      ladder_as<H, LADDER_MINB[1]>(grid, q, s, r_lo, r_hi, skip_partial, slot0);
     else
-      k_ladder<int><<<grid, ICP_BLOCK, 0, s>>>(dv.p, di.p, q, reinterpret_cast<int *>(hints.p),
-                                               hint_stride, dc.p, r_lo, r_hi, skip_partial,
-                                               ctx->d_status);
+      ladder_as<H, LADDER_MINB[2]>(grid, q, s, r_lo, r_hi, skip_partial, slot0);
+  }
+  void ladder(unsigned grid, QueueCtl q, cudaStream_t s, int r_lo, int r_hi, int skip_partial,
+              int v = LADDER_VARIANTS - 1, size_t slot0 = 0) {
+    if (hint16)
+      ladder_h<uint16_t>(v, grid, q, s, r_lo, r_hi, skip_partial, slot0);
+    else
+      ladder_h<int>(v, grid, q, s, r_lo, r_hi, skip_partial, slot0);
+  }
+  // The ladder's point-count buckets (largest moving clouds first): each is a
+  // segment of the queue order, run by its own k_ladder variant (chosen by the
+  // autotuner) on a grid of its own, its CTAs on a slice of the hint slots.
+  static constexpr int BUCKETS = 3;
+  uint32_t seg_first[BUCKETS] = {}, seg_count[BUCKETS] = {};
+  int variant[BUCKETS] = {LADDER_VARIANTS - 1, LADDER_VARIANTS - 1, LADDER_VARIANTS - 1};
+  size_t slot0[BUCKETS] = {};
+  int occ[LADDER_VARIANTS] = {};  // resident k_ladder CTAs per SM of each variant
+  DBuf<unsigned> lheads;          // one queue head per bucket
+  unsigned bucket_grid(int b) const {
+    return std::max(1u, std::min<unsigned>(unsigned(std::max(1, occ[variant[b]]) * ctx->sm_count),
+                                           seg_count[b]));
   }
   bool early() const { return params.early_reject_tight > 0.0; }
   // Queue heads per group of items (the whole batch, or one pair of the plain
@@ -1461,11 +1518,87 @@ int ladder_stage(sherd_batch *b, cudaStream_t s, unsigned *heads, const uint32_t
   return SHERD_OK;
 }
 
+// The ladder stage of the batched schedule: one k_ladder launch per
+// point-count bucket, the three side by side (the caller's stream and the
+// context's two side streams, forked and joined by events, which a stream
+// capture records as graph edges), so the buckets share the SMs as one queue
+// would. With R 5.6's early rejection the stage stays one queue.
 int launch_ladder(sherd_batch *b, cudaStream_t s) {
   sherd_ctx *ctx = b->ctx;
   CK(cudaMemsetAsync(b->heads.p, 0, sherd_batch::HEADS * sizeof(unsigned), s));
-  return ladder_stage(b, s, b->heads.p, b->dorder.p, b->n_items,
-                      std::min<unsigned>(b->grid_l, b->n_items));
+  if (b->early())
+    return ladder_stage(b, s, b->heads.p, b->dorder.p, b->n_items,
+                        std::min<unsigned>(b->grid_l, b->n_items));
+  unsigned long long budget = (unsigned long long)ctx->timeout_ms * 1000000ULL;
+  CK(cudaMemsetAsync(b->lheads.p, 0, sherd_batch::BUCKETS * sizeof(unsigned), s));
+  CK(cudaEventRecord(ctx->fork_ev, s));
+  for (int k = 0; k < 2; ++k) CK(cudaStreamWaitEvent(ctx->side[k], ctx->fork_ev, 0));
+  for (int bk = 0; bk < sherd_batch::BUCKETS; ++bk) {
+    if (!b->seg_count[bk]) continue;
+    cudaStream_t on = bk == 0 ? s : ctx->side[bk - 1];
+    QueueCtl q{b->lheads.p + bk, b->dorder.p + b->seg_first[bk], b->seg_count[bk], ctx->abort_dev,
+               budget};
+    b->ladder(b->bucket_grid(bk), q, on, 0, 4, 0, b->variant[bk], b->slot0[bk]);
+    CK(cudaGetLastError());
+  }
+  for (int k = 0; k < 2; ++k) {
+    CK(cudaEventRecord(ctx->join_ev[k], ctx->side[k]));
+    CK(cudaStreamWaitEvent(s, ctx->join_ev[k], 0));
+  }
+  return SHERD_OK;
+}
+
+// The ladder autotuner: for each point-count bucket with enough items that the
+// context has not tuned yet, every k_ladder variant runs the four rungs of the
+// bucket's most expensive items (two full grids' worth, the same items for
+// every variant, after one untimed run), twice, timed by CUDA events on the
+// context's stream; a variant replaces the default (the last, the highest
+// occupancy) only when its faster run beats the default's by TUNE_MARGIN, so
+// run-to-run noise does not move the choice. The choice is kept for the bucket
+// on this context. The runs write those items' rungs, which every batch run
+// writes again.
+constexpr float TUNE_MARGIN = 0.05f;
+int tune_ladder(sherd_batch *b) {
+  sherd_ctx *ctx = b->ctx;
+  cudaStream_t s = ctx->stream;
+  int max_occ = 1;
+  for (int v = 0; v < LADDER_VARIANTS; ++v) max_occ = std::max(max_occ, b->occ[v]);
+  for (int bk = 0; bk < sherd_batch::BUCKETS; ++bk) {
+    if (ctx->ladder_tuned[bk] >= 0) {
+      b->variant[bk] = ctx->ladder_tuned[bk];
+      continue;
+    }
+    const uint32_t need = 2u * uint32_t(max_occ) * uint32_t(ctx->sm_count);
+    if (b->seg_count[bk] < need) continue;  // too few items to tell the variants apart
+    float ms_of[LADDER_VARIANTS];
+    for (int k = 0; k < LADDER_VARIANTS; ++k) ms_of[k] = f_inf();
+    for (int t = -1; t < 2 * LADDER_VARIANTS; ++t) {
+      const int v = t < 0 ? -1 : t % LADDER_VARIANTS;
+      const int run = v < 0 ? LADDER_VARIANTS - 1 : v;
+      const unsigned grid = std::min<unsigned>(unsigned(b->occ[run] * ctx->sm_count), need);
+      QueueCtl q{b->lheads.p + bk, b->dorder.p + b->seg_first[bk], need, ctx->abort_dev, 0ull};
+      CK(cudaMemsetAsync(b->lheads.p + bk, 0, sizeof(unsigned), s));
+      CK(cudaEventRecord(ctx->ev0, s));
+      b->ladder(grid, q, s, 0, 4, 0, run, b->slot0[bk]);
+      CK(cudaGetLastError());
+      CK(cudaEventRecord(ctx->ev1, s));
+      CK(cudaStreamSynchronize(s));
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      if (v < 0) continue;  // the untimed first run
+      ms_of[v] = std::min(ms_of[v], ms);
+    }
+    int pick = LADDER_VARIANTS - 1;
+    for (int v = 0; v < LADDER_VARIANTS; ++v) {
+      ctx->ladder_tune_ms[bk][v] = ms_of[v];
+      if (ms_of[v] < ms_of[pick] && ms_of[v] < (1.0f - TUNE_MARGIN) * ms_of[LADDER_VARIANTS - 1])
+        pick = v;
+    }
+    ctx->ladder_tuned[bk] = pick;
+    ctx->ladder_tune_items[bk] = need;
+    b->variant[bk] = pick;
+  }
+  return SHERD_OK;
 }
 
 int launch_verify_items(sherd_batch *b, cudaStream_t s) {
@@ -1579,10 +1712,21 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
   for (uint32_t i = 0; i < n_pairs; ++i) views[i] = pairs[i]->view;
   std::vector<uint32_t> order(n_items);
   if (sched == SHERD_SCHED_BATCHED) {
+    // By point-count bucket of the moving clouds (> 16384, > 4096, the rest),
+    // then longest items first within each.
+    auto bucket = [&](uint32_t pair) {
+      uint32_t m = std::max(views[pair].n_reg, views[pair].n_frac);
+      return m > 16384u ? 0 : (m > 4096u ? 1 : 2);
+    };
     for (uint32_t i = 0; i < n_items; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+      int bx = bucket(items[x].pair), by = bucket(items[y].pair);
+      if (bx != by) return bx < by;
       return pair_cost[items[x].pair] > pair_cost[items[y].pair];
     });
+    for (uint32_t k = 0; k < n_items; ++k) b->seg_count[bucket(items[order[k]].pair)]++;
+    for (int bk = 1; bk < sherd_batch::BUCKETS; ++bk)
+      b->seg_first[bk] = b->seg_first[bk - 1] + b->seg_count[bk - 1];
   } else {
     b->pair_first.assign(n_pairs, 0);
     b->pair_count.assign(n_pairs, 0);
@@ -1602,10 +1746,18 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
   CK(b->dc.alloc(n_items));
   CK(cudaMemsetAsync(b->dc.p, 0, sizeof(sherd_candidate) * n_items, ctx->stream));
   CK(b->heads.alloc(sherd_batch::HEADS * size_t(std::max<uint32_t>(n_pairs, 1))));
-  int occ_l = 0, occ_v = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, k_ladder<uint16_t>, ICP_BLOCK, 0));
+  int occ_v = 0;
+  if (b->hint16) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ[0], k_ladder<uint16_t, LADDER_MINB[0]>, ICP_BLOCK, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ[1], k_ladder<uint16_t, LADDER_MINB[1]>, ICP_BLOCK, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ[2], k_ladder<uint16_t, LADDER_MINB[2]>, ICP_BLOCK, 0));
+  } else {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ[0], k_ladder<int, LADDER_MINB[0]>, ICP_BLOCK, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ[1], k_ladder<int, LADDER_MINB[1]>, ICP_BLOCK, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ[2], k_ladder<int, LADDER_MINB[2]>, ICP_BLOCK, 0));
+  }
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_v, k_verify_items, VER_BLOCK, 0));
-  b->grid_l = unsigned(std::max(1, occ_l) * ctx->sm_count);
+  b->grid_l = unsigned(std::max(1, b->occ[LADDER_VARIANTS - 1]) * ctx->sm_count);
   b->grid_v = unsigned(std::max(1, occ_v) * ctx->sm_count);
   CK(b->scratch.alloc(size_t(b->grid_v) * b->max_scratch));
   if (sched == SHERD_SCHED_BATCHED) {
@@ -1650,10 +1802,26 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
   // hint slots as the largest pair has items.
   size_t slots = b->grid_l;
   for (uint32_t c : b->pair_count) slots = std::max<size_t>(slots, c);
+  if (sched == SHERD_SCHED_BATCHED) {
+    // The buckets' launches run side by side, each on its own slice of slots,
+    // as wide as the largest grid any variant could take.
+    int max_occ = 1;
+    for (int v = 0; v < LADDER_VARIANTS; ++v) max_occ = std::max(max_occ, b->occ[v]);
+    size_t acc = 0;
+    for (int bk = 0; bk < sherd_batch::BUCKETS; ++bk) {
+      b->slot0[bk] = acc;
+      acc += std::min<size_t>(size_t(max_occ) * ctx->sm_count, b->seg_count[bk]);
+    }
+    slots = std::max(slots, acc);
+    CK(b->lheads.alloc(sherd_batch::BUCKETS));
+  }
   CK(b->hints.alloc(slots * b->hint_stride * (b->hint16 ? sizeof(uint16_t) : sizeof(int))));
   for (cudaEvent_t &e : b->ev) CK(cudaEventCreate(&e));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (sched == SHERD_SCHED_BATCHED) return capture(b);
+  if (sched == SHERD_SCHED_BATCHED) {
+    if (!b->early() && (rc = tune_ladder(b))) return rc;
+    return capture(b);
+  }
   return SHERD_OK;
 }
 
