@@ -579,6 +579,22 @@ int sherd_nms(const uint32_t *order, uint32_t n_order, const double *poses, cons
 int sherd_vertex_normals(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f,
                          uint32_t nf, double *normals);
 
+/* refine::fracture_cloud (refine.rs:217-227) up to the cap, in one call, so
+ * the mesh crosses to the device once and only the chosen vertices come back:
+ * the vertices of the original mesh (v, f) whose nearest working-mesh face
+ * centroid (refine::select_candidates, refine.rs:161-178: PointTree::
+ * nearest_below, strictly within `radius` = max(0.15 t, 1.5 res)) is a
+ * fracture face (`fracture`, one flag per centroid), in ascending order, with
+ * their points and their refine::vertex_normals. Writes min(count, cap)
+ * indices, points and normals (f64 triples); *n_out = count, the number
+ * selected (above `cap`, call again with a larger cap). The same values as
+ * sherd_nearest_below over a cloud of the centroids and
+ * sherd_vertex_normals. refine::cap_selection's draw stays with the caller. */
+int sherd_fracture_cloud(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f,
+                         uint32_t nf, const double *centroids, const uint8_t *fracture,
+                         uint32_t n_cent, double radius, uint32_t cap, uint32_t *idx_out,
+                         double *points_out, double *normals_out, uint32_t *n_out);
+
 /* refine::refine_one (refine.rs:334-386) for one join: the moving fragment's
  * cloud `source` (n_source points) placed by pose_moving, the fixed one's
  * `target` and `target_normals` (n_target) placed by pose_fixed, both as

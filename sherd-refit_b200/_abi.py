@@ -205,6 +205,9 @@ _SIGNATURES = {
     "sherd_nms": (C.c_int, [U32P, C.c_uint32, F64P, F64P, C.c_uint32, C.c_double, C.c_uint32,
                             C.c_double, VP, C.POINTER(C.c_uint32)]),
     "sherd_vertex_normals": (C.c_int, [VP, F64P, C.c_uint32, U32P, C.c_uint32, F64P]),
+    "sherd_fracture_cloud": (C.c_int, [VP, F64P, C.c_uint32, U32P, C.c_uint32, F64P, U8P,
+                                       C.c_uint32, C.c_double, C.c_uint32, U32P, F64P, F64P,
+                                       C.POINTER(C.c_uint32)]),
     "sherd_refine_join": (C.c_int, [VP, F64P, C.c_uint32, F64P, F64P, C.c_uint32, F64P, F64P,
                                     F64P, C.c_int32, VP]),
 }

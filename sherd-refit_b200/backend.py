@@ -420,6 +420,25 @@ class Context:
         check(self.h, A.lib().sherd_vertex_normals(self.h, v, len(v), f, len(f), out))
         return out
 
+    def fracture_cloud(self, v, f, centroids, fracture, radius):
+        """refine::fracture_cloud (refine.rs:217-227) before the cap, in one device call: the
+        selected vertex indices (ascending), their points and their vertex normals."""
+        v, f = _f64(v), _u32(f, (-1, 3))
+        cen = _f64(centroids)
+        frac = np.ascontiguousarray(np.asarray(fracture).astype(bool).reshape(-1), np.uint8)
+        if len(cen) != len(frac):
+            raise A.SherdError(A.E_INVALID, "one fracture label per centroid")
+        nv = len(v)
+        idx = np.empty(max(nv, 1), np.uint32)
+        pts = np.empty((max(nv, 1), 3))
+        nrm = np.empty((max(nv, 1), 3))
+        n = C.c_uint32(0)
+        check(self.h, A.lib().sherd_fracture_cloud(self.h, v, nv, f, len(f), cen, frac, len(cen),
+                                                   float(radius), nv, idx, pts, nrm,
+                                                   C.byref(n)))
+        m = int(n.value)
+        return idx[:m].copy(), pts[:m].copy(), nrm[:m].copy()
+
     def refine_join(self, source, target, target_normals, pose_fixed, pose_moving, dist,
                     max_iteration=40):
         """refine_one's two point-to-plane rungs (refine.rs:334-386) for one join, the clouds

@@ -71,6 +71,31 @@ __global__ void k_vertex_normals(const double *v, const uint32_t *f, const uint3
   }
 }
 
+// refine::select_candidates' predicate (refine.rs:161-178) per vertex: its
+// nearest centroid within the radius (near, MISS when none) is a fracture
+// face. Writes the flag and the vertex's own index (the select's input).
+__global__ void k_fracture_flags(const uint32_t *near, const uint8_t *fracture, uint32_t nv,
+                                 uint8_t *flags, uint32_t *lin) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  uint32_t j = near[i];
+  flags[i] = (j != MISS && fracture[j]) ? 1 : 0;
+  lin[i] = i;
+}
+
+// refine::cloud_from_indices (refine.rs:208-214): the selected vertices'
+// points and normals, in selection order.
+__global__ void k_gather_cloud(const double *v, const double *normals, const uint32_t *sel,
+                               uint32_t m, double *points_out, double *normals_out) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  size_t i = sel[k];
+  for (int a = 0; a < 3; ++a) {
+    points_out[3 * size_t(k) + a] = v[3 * i + a];
+    normals_out[3 * size_t(k) + a] = normals[3 * i + a];
+  }
+}
+
 // ---- placement (types.rs:202-214) ---------------------------------------------
 
 // Row r of the row-major pose: fma(t_r2, p2, fma(t_r1, p1, t_r0 p0)), plus

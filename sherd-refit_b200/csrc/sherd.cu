@@ -2083,6 +2083,39 @@ int to_host(sherd_ctx *ctx, T *host, const T *dev, size_t n) {
 
 }  // namespace
 
+namespace {
+
+bool all_finite(const double *p, size_t n);
+
+// refine::vertex_normals (refine.rs:121-151) of a mesh already on the device:
+// the corners sorted stably by vertex, so each vertex adds its faces'
+// unnormalised normals in ascending face order, as the reference's loop does.
+int vertex_normals_dev(sherd_ctx *ctx, const double *dv, uint32_t nv, const uint32_t *df,
+                       uint32_t nf, DBuf<double> &dn) {
+  cudaStream_t s = ctx->stream;
+  const uint32_t nc = 3u * nf;
+  DBuf<uint32_t> key, key2, face, face2;
+  CK(dn.alloc(size_t(3) * nv));
+  if (nc) {
+    CK(key.alloc(nc));
+    CK(key2.alloc(nc));
+    CK(face.alloc(nc));
+    CK(face2.alloc(nc));
+    k_incidence<<<blocks_for(nc), 256, 0, s>>>(df, nc, key.p, face.p);
+    CK(cudaGetLastError());
+    int bits = 1;  // vertex ids are below nv <= 2^bits
+    while (bits < 32 && (uint64_t(1) << bits) < uint64_t(nv)) ++bits;
+    // LSD radix sort is stable: each vertex keeps its faces in ascending order.
+    int rc = radix_sort_pairs(ctx, key.p, key2.p, face.p, face2.p, nc, bits);
+    if (rc) return rc;
+  }
+  k_vertex_normals<<<blocks_for(nv), 256, 0, s>>>(dv, df, key2.p, face2.p, nc, nv, dn.p);
+  CK(cudaGetLastError());
+  return SHERD_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int sherd_segment(sherd_ctx *ctx, const sherd_mesh *mesh, const double *v, uint32_t nv,
@@ -2303,28 +2336,83 @@ int sherd_vertex_normals(sherd_ctx *ctx, const double *v, uint32_t nv, const uin
   NvtxRange range("sherd vertex_normals");
   int rc = begin(ctx);
   if (rc) return rc;
-  cudaStream_t s = ctx->stream;
-  const uint32_t nc = 3u * nf;
   DBuf<double> dv, dn;
-  DBuf<uint32_t> df, key, key2, face, face2;
-  if ((rc = upload(ctx, dv, v, size_t(3) * nv)) || (rc = upload(ctx, df, f, size_t(nc)))) return rc;
-  CK(dn.alloc(size_t(3) * nv));
-  if (nc) {
-    CK(key.alloc(nc));
-    CK(key2.alloc(nc));
-    CK(face.alloc(nc));
-    CK(face2.alloc(nc));
-    k_incidence<<<blocks_for(nc), 256, 0, s>>>(df.p, nc, key.p, face.p);
-    CK(cudaGetLastError());
-    int bits = 1;  // vertex ids are below nv <= 2^bits
-    while (bits < 32 && (uint64_t(1) << bits) < uint64_t(nv)) ++bits;
-    // LSD radix sort is stable: each vertex keeps its faces in ascending order.
-    if ((rc = radix_sort_pairs(ctx, key.p, key2.p, face.p, face2.p, nc, bits))) return rc;
-  }
-  k_vertex_normals<<<blocks_for(nv), 256, 0, s>>>(dv.p, df.p, key2.p, face2.p, nc, nv, dn.p);
-  CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(normals, dn.p, 24 * size_t(nv), cudaMemcpyDeviceToHost, s));
+  DBuf<uint32_t> df;
+  if ((rc = upload(ctx, dv, v, size_t(3) * nv)) || (rc = upload(ctx, df, f, size_t(3) * nf))) return rc;
+  if ((rc = vertex_normals_dev(ctx, dv.p, nv, df.p, nf, dn))) return rc;
+  CK(cudaMemcpyAsync(normals, dn.p, 24 * size_t(nv), cudaMemcpyDeviceToHost, ctx->stream));
   return finish(ctx, "vertex_normals", nv, true);
+}
+
+int sherd_fracture_cloud(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f,
+                         uint32_t nf, const double *centroids, const uint8_t *fracture,
+                         uint32_t n_cent, double radius, uint32_t cap, uint32_t *idx_out,
+                         double *points_out, double *normals_out, uint32_t *n_out) {
+  if (!ctx || !n_out || ((!v) && nv) || (!f && nf) || ((!centroids || !fracture) && n_cent) ||
+      ((!idx_out || !points_out || !normals_out) && cap))
+    return fail(ctx, SHERD_E_INVALID, "null argument");
+  *n_out = 0;
+  if (uint64_t(nf) * 3u >= (uint64_t(1) << 31)) return fail(ctx, SHERD_E_INVALID, "too many faces");
+  for (size_t i = 0; i < size_t(3) * nf; ++i)
+    if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
+  if (!all_finite(centroids, size_t(3) * n_cent) || !all_finite(v, size_t(3) * nv))
+    return fail(ctx, SHERD_E_INVALID, "coordinates must be finite");
+  if (nv == 0 || n_cent == 0 || !(radius > 0.0)) return SHERD_OK;
+  double mag = 1.0;
+  for (size_t i = 0; i < size_t(3) * n_cent; ++i) mag = std::max(mag, std::fabs(centroids[i]));
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  NvtxRange range("sherd fracture_cloud");
+  int rc = begin(ctx);
+  if (rc) return rc;
+  cudaStream_t s = ctx->stream;
+  DBuf<double> dv, dc, dn, dist;
+  DBuf<uint32_t> df, near, lin, sel, nsel;
+  DBuf<uint8_t> dfrac, flags;
+  if ((rc = upload(ctx, dv, v, size_t(3) * nv)) || (rc = upload(ctx, df, f, size_t(3) * nf)) ||
+      (rc = upload(ctx, dc, centroids, size_t(3) * n_cent)) ||
+      (rc = upload(ctx, dfrac, fracture, size_t(n_cent))))
+    return rc;
+  // The centroids' tree, the nearest centroid of every vertex strictly within
+  // the radius (refine.rs:161-178), and the vertices whose nearest is a
+  // fracture face, ascending.
+  sherd_cloud cent;
+  if ((rc = cloud_build_dev(ctx, dc.p, nullptr, n_cent, float(1e-6 * mag), &cent))) return rc;
+  CK(near.alloc(nv));
+  CK(dist.alloc(nv));
+  k_nn_below<<<blocks_for(nv, 128), 128, 0, s>>>(cent.view, dv.p, nv, radius, near.p, dist.p,
+                                                 ctx->d_status);
+  CK(cudaGetLastError());
+  CK(flags.alloc(nv));
+  CK(lin.alloc(nv));
+  k_fracture_flags<<<blocks_for(nv), 256, 0, s>>>(near.p, dfrac.p, nv, flags.p, lin.p);
+  CK(cudaGetLastError());
+  CK(sel.alloc(nv));
+  CK(nsel.alloc(1));
+  size_t bytes = 0;
+  CK(cub::DeviceSelect::Flagged(nullptr, bytes, lin.p, flags.p, sel.p, nsel.p, int(nv), s));
+  DBuf<unsigned char> tmp;
+  CK(tmp.alloc(bytes));
+  CK(cub::DeviceSelect::Flagged(tmp.p, bytes, lin.p, flags.p, sel.p, nsel.p, int(nv), s));
+  // Every vertex's normal (refine.rs:121-151), then the selected vertices'
+  // points and normals gathered in selection order.
+  if ((rc = vertex_normals_dev(ctx, dv.p, nv, df.p, nf, dn))) return rc;
+  uint32_t count = 0;
+  CK(cudaMemcpyAsync(&count, nsel.p, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *n_out = count;
+  const uint32_t m = std::min(count, cap);
+  if (m) {
+    DBuf<double> gp, gn;
+    CK(gp.alloc(size_t(3) * m));
+    CK(gn.alloc(size_t(3) * m));
+    k_gather_cloud<<<blocks_for(m), 256, 0, s>>>(dv.p, dn.p, sel.p, m, gp.p, gn.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(idx_out, sel.p, 4 * size_t(m), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(points_out, gp.p, 24 * size_t(m), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(normals_out, gn.p, 24 * size_t(m), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  return finish(ctx, "fracture_cloud", nv, true);
 }
 
 }  // extern "C"

@@ -129,9 +129,20 @@ def cloud_from_indices(v, normals, idx) -> FractureCloud:
 
 def fracture_cloud(ctx: Context, v, f, centroids, fracture, thick, res,
                    seed: int = CAP_SEED) -> FractureCloud:
-    """refine::fracture_cloud (refine.rs:217-227): the original mesh (v, f) in, its cloud out."""
-    idx = select_vertices(ctx, v, centroids, fracture, thick, res, MAX_POINTS, seed)
-    return cloud_from_indices(v, vertex_normals(ctx, v, f), idx)
+    """refine::fracture_cloud (refine.rs:217-227): the original mesh (v, f) in, its cloud out.
+    One device call (sherd_fracture_cloud) uploads the mesh once and returns only the selected
+    vertices with their points and normals; the cap's draw (cap_selection) then picks among
+    them on the host."""
+    if len(centroids) != len(np.asarray(fracture).reshape(-1)):
+        raise A.SherdError(A.E_INVALID, "one fracture label per centroid")
+    radius = max(SELECT_T * float(thick), SELECT_RES * float(res))
+    idx, pts, nrm = ctx.fracture_cloud(v, f, centroids, fracture, radius)
+    capped = cap_selection(idx, MAX_POINTS, seed)
+    if len(capped) != len(idx):
+        at = np.searchsorted(idx, capped)
+        idx, pts, nrm = capped, pts[at], nrm[at]
+    return FractureCloud(np.asarray(idx, np.uint32), np.ascontiguousarray(pts),
+                         np.ascontiguousarray(nrm))
 
 
 def matmul4(a, b) -> np.ndarray:

@@ -254,6 +254,16 @@ class _OracleDevice:
     def vertex_normals(self, v, f):
         return self.oracle.vertex_normals(v, f)
 
+    def fracture_cloud(self, v, f, centroids, fracture, radius):
+        """sherd_fracture_cloud's contract on the oracle: the selected vertices (nearest
+        centroid strictly within the radius is a fracture face), their points and normals."""
+        v = np.ascontiguousarray(v, np.float64).reshape(-1, 3)
+        j, _ = self.oracle.Cloud(np.ascontiguousarray(centroids, np.float64)).nearest_below(v, radius)
+        keep = j != 0xFFFFFFFF
+        keep[keep] = np.asarray(fracture).astype(bool).reshape(-1)[j[keep]]
+        idx = np.flatnonzero(keep).astype(np.uint32)
+        return idx, v[idx.astype(np.int64)], self.oracle.vertex_normals(v, f)[idx.astype(np.int64)]
+
     def refine_join(self, source, target, target_normals, pose_fixed, pose_moving, dist,
                     max_iteration=40):
         return _oracle_join(self.oracle, source, target, target_normals, pose_fixed,
@@ -319,6 +329,38 @@ def test_device_selection_is_the_fixture_selection(gpu_ctx, slab):
         cloud = rf.fracture_cloud(gpu_ctx, p["V0"], p["F"], _centroids(p["V"], p["F"]),
                                   p["frac"], thick, res)
         assert np.array_equal(cloud.idx, p["refine_idx"])
+
+
+@pytest.mark.gpu
+def test_fused_fracture_cloud_equals_the_two_call_path(gpu_ctx, oracle, slab):
+    """sherd_fracture_cloud (one upload, selection, normals and gathers on the device) gives the
+    selection of sherd_nearest_below over the centroids and the sherd_vertex_normals values,
+    bit for bit, on both slab pieces and on a pot fragment (with a cap that draws)."""
+    rf = _refine_mod()
+    synth = importlib.import_module("sherd-refit_b200.synth")
+    cases = []
+    for name in ("pieceA", "pieceB"):
+        p = piece(slab, name)
+        cases.append((p["V0"], p["F"], _centroids(p["V"], p["F"]), p["frac"],
+                      *(float(x) for x in p["stats_thick_res"])))
+    fr = synth.make("pot", 0).fragments[1]
+    v = fr.v.astype(np.float64)
+    cases.append((v, fr.f, _centroids(v, fr.f), fr.frac, float(fr.t), float(fr.res)))
+    for v, f, cen, frac, thick, res in cases:
+        idx = rf.select_candidates(gpu_ctx, v, cen, frac, thick, res)
+        nrm = gpu_ctx.vertex_normals(v, f)
+        radius = max(rf.SELECT_T * thick, rf.SELECT_RES * res)
+        got_idx, got_p, got_n = gpu_ctx.fracture_cloud(v, f, cen, frac, radius)
+        assert len(idx) > 0 and np.array_equal(got_idx, idx)
+        assert np.array_equal(got_p, np.asarray(v, np.float64)[idx.astype(np.int64)])
+        assert np.array_equal(got_n, nrm[idx.astype(np.int64)])
+        assert np.array_equal(got_n, oracle.vertex_normals(v, f)[idx.astype(np.int64)])
+        small = max(1, len(idx) // 3)   # the cap's draw among the fused path's vertices
+        want = rf.cap_selection(idx, small, 0)
+        got = rf.FractureCloud(got_idx, got_p, got_n)
+        at = np.searchsorted(got.idx, want)
+        assert np.array_equal(got.idx[at], want)
+        assert np.array_equal(got.normals[at], nrm[want.astype(np.int64)])
 
 
 @pytest.mark.gpu
