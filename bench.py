@@ -44,7 +44,11 @@ L2_FLUSH_BYTES = 256 << 20
 # kernel, ranks), from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of
 # `python bench.py --steps 1 --warmup 3 --no-cpu --no-plain`, with the digest of the CUDA sources
 # it was taken on: a capture of other sources is not reported.
-TRAFFIC = {}
+TRAFFIC = {
+    # the ladder stage's bucket launches together (> 16384 and > 4096 moving points; ncu runs
+    # them one after the other): 138.86 + 139.74 GB read, 36.19 + 121.77 GB written
+    ("collection", 0, "k_ladder", 1): (436.57e9, "647f5e0390d5"),
+}
 
 
 def _pkg(name=""):
@@ -772,8 +776,9 @@ def main():
     traffic = rec[0] if rec and rec[1] == src else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                   f"full-size launch of this build (CUDA sources {src})"
+                "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
+                                   f"stage's launches in one full-size step of this build (CUDA "
+                                   f"sources {src})"
                                    if traffic else
                                    f"no ncu capture recorded for this build (CUDA sources {src})"),
                 "kernel": stages[dom]["kernel"],
