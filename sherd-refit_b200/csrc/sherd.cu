@@ -65,6 +65,23 @@ struct sherd_ctx {
   int ladder_tuned[3] = {-1, -1, -1};
   float ladder_tune_ms[3][3] = {};
   uint32_t ladder_tune_items[3] = {};
+  // Device buffers the entry points allocate (stream-ordered, on `stream`).
+  cudaMemPool_t pool = nullptr;
+};
+
+// The context an entry point allocates its device buffers from (its pool, on
+// its stream), for as long as the entry point holds it (CtxLock); null
+// otherwise, and while a stage graph is being captured.
+thread_local sherd_ctx *t_alloc_ctx = nullptr;
+constexpr uint64_t POOL_KEEP_BYTES = uint64_t(4) << 30;
+
+// An entry point's hold on its context: the context's lock, and its stream as
+// the stream device buffers are allocated and freed on (stream-ordered).
+struct CtxLock {
+  std::lock_guard<std::mutex> guard;
+  sherd_ctx *prev;
+  explicit CtxLock(sherd_ctx *c) : guard(c->mu), prev(t_alloc_ctx) { t_alloc_ctx = c; }
+  ~CtxLock() { t_alloc_ctx = prev; }
 };
 
 // Working memory of sherd_icp_rung_noalloc: each source point's last match, for
@@ -126,19 +143,36 @@ template <typename T>
 struct DBuf {  // owning device buffer
   T *p = nullptr;
   size_t n = 0;
+  cudaStream_t s = nullptr;  // the stream it came from the context's pool on
   DBuf() = default;
   DBuf(const DBuf &) = delete;
   DBuf &operator=(const DBuf &) = delete;
   ~DBuf() { reset(); }
+  // Allocated inside an entry point, a buffer comes from the context's pool on
+  // the context's stream and goes back on that stream: the free is ordered
+  // after the work queued before it, and neither call waits for the device.
+  // Allocated anywhere else, the plain synchronous calls.
   void reset() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (s)
+        cudaFreeAsync(p, s);
+      else
+        cudaFree(p);
+    }
     p = nullptr;
     n = 0;
+    s = nullptr;
   }
   cudaError_t alloc(size_t count) {
     reset();
     n = count;
     if (!count) return cudaSuccess;
+    if (sherd_ctx *c = t_alloc_ctx) {
+      cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&p), count * sizeof(T), c->pool,
+                                              c->stream);
+      if (e == cudaSuccess) s = c->stream;
+      return e;
+    }
     return cudaMalloc(&p, count * sizeof(T));
   }
 };
@@ -574,6 +608,19 @@ int sherd_open(int device, sherd_ctx **out) {
     if ((e = cudaEventCreateWithFlags(&ctx->join_ev[k], cudaEventDisableTiming)) != cudaSuccess) return bad(e);
   }
   if ((e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming)) != cudaSuccess) return bad(e);
+  // The context's own stream-ordered pool: it keeps up to POOL_KEEP_BYTES of
+  // what the entry points free for their next buffers instead of handing it
+  // back to the device at every synchronisation.
+  {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if ((e = cudaMemPoolCreate(&ctx->pool, &props)) != cudaSuccess) return bad(e);
+    uint64_t keep = POOL_KEEP_BYTES;
+    if ((e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess)
+      return bad(e);
+  }
   if ((e = cudaHostAlloc(&ctx->abort_host, 4, cudaHostAllocMapped)) != cudaSuccess) return bad(e);
   *ctx->abort_host = 0;
   if ((e = cudaHostGetDevicePointer(&ctx->abort_dev, ctx->abort_host, 0)) != cudaSuccess) return bad(e);
@@ -595,6 +642,7 @@ int sherd_close(sherd_ctx *ctx) {
     if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
   }
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   t_errors.erase(ctx);
   delete ctx;
@@ -608,7 +656,7 @@ const char *sherd_last_error(const sherd_ctx *ctx) {
 
 int sherd_set_timeout_ms(sherd_ctx *ctx, uint32_t ms) {
   if (!ctx) return SHERD_E_INVALID;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   ctx->timeout_ms = ms;
   return SHERD_OK;
 }
@@ -622,7 +670,7 @@ int sherd_abort(sherd_ctx *ctx) {
 
 int sherd_stats_json(sherd_ctx *ctx, char *buf, size_t len) {
   if (!ctx || !buf || !len) return SHERD_E_INVALID;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   std::string s = "{\"backend\": \"cuda\", \"device\": " + std::to_string(ctx->device) +
                   ", \"sm_count\": " + std::to_string(ctx->sm_count) + ", \"methods\": {";
   bool firstm = true;
@@ -667,7 +715,7 @@ int sherd_mesh_upload(sherd_ctx *ctx, const float *v, uint32_t nv, const uint32_
     if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
   for (size_t i = 0; i < size_t(3) * nv; ++i)
     if (!std::isfinite(v[i])) return fail(ctx, SHERD_E_INVALID, "non-finite vertex");
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   CK(cudaSetDevice(ctx->device));
   sherd_mesh *m = new sherd_mesh;
   m->ctx = ctx;
@@ -685,7 +733,7 @@ int sherd_mesh_upload(sherd_ctx *ctx, const float *v, uint32_t nv, const uint32_
 int sherd_mesh_subset(sherd_ctx *ctx, const sherd_mesh *mesh, const uint8_t *keep, sherd_mesh **out) {
   if (!ctx || !mesh || !keep || !out) return fail(ctx, SHERD_E_INVALID, "null argument");
   *out = nullptr;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   CK(cudaSetDevice(ctx->device));
   sherd_mesh *m = new sherd_mesh;
   m->ctx = ctx;
@@ -706,6 +754,7 @@ int sherd_mesh_subset(sherd_ctx *ctx, const sherd_mesh *mesh, const uint8_t *kee
 int sherd_mesh_free(sherd_mesh *mesh) {
   if (!mesh) return SHERD_E_INVALID;
   cudaSetDevice(mesh->ctx->device);
+  CtxLock lock(mesh->ctx);
   delete mesh;
   return SHERD_OK;
 }
@@ -726,7 +775,7 @@ int sherd_first_hit(sherd_ctx *ctx, const sherd_mesh *mesh, const float *origins
   if (!ctx || !mesh || ((!origins || !dirs || !t_out || !prim_out) && n))
     return fail(ctx, SHERD_E_INVALID, "null argument");
   if (n == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<float> o, d, t;
@@ -755,7 +804,7 @@ int sherd_bounded_distance(sherd_ctx *ctx, const sherd_mesh *mesh, const double 
     return SHERD_OK;
   }
   if (n == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> p, o;
@@ -797,7 +846,7 @@ int sherd_inside(sherd_ctx *ctx, const sherd_mesh *mesh, const double *points, u
   if (!ctx || !mesh || ((!points || !out) && n)) return fail(ctx, SHERD_E_INVALID, "null argument");
   if (!finite_pose(pose)) return fail(ctx, SHERD_E_INVALID, "pose is not finite");
   if (n == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> p;
@@ -818,7 +867,7 @@ int sherd_penetration_share(sherd_ctx *ctx, const sherd_mesh *mesh, const double
   if (!finite_pose(pose)) return fail(ctx, SHERD_E_INVALID, "pose is not finite");
   *share = 0.0;
   if (n == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> p;
@@ -847,7 +896,7 @@ int sherd_face_geometry(sherd_ctx *ctx, const double *v, uint32_t nv, const uint
   for (size_t i = 0; i < size_t(3) * nf; ++i)
     if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
   if (nf == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> dv, dn, da, dc;
@@ -919,7 +968,7 @@ int sherd_thickness(sherd_ctx *ctx, const sherd_mesh *mesh, const double *centro
   uint32_t n_req = max_rays ? max_rays : 1;
   uint32_t stride = std::max<uint32_t>(1, (nf + n_req - 1) / n_req);
   uint32_t n = (nf + stride - 1) / stride;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> dc, dn;
@@ -953,7 +1002,7 @@ int sherd_thickness_from_hits(sherd_ctx *ctx, const double *normals, uint32_t nf
     if (idx[k] >= nf) return fail(ctx, SHERD_E_INVALID, "ray face id beyond the mesh");
   *found = 0;
   if (n == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> dn;
@@ -983,7 +1032,7 @@ int sherd_cone_votes(sherd_ctx *ctx, const sherd_mesh *mesh, const double *centr
   if (nf != mesh->view.nf) return fail(ctx, SHERD_E_INVALID, "face count differs from the mesh");
   if (nf == 0) return SHERD_OK;
   ConeConsts cc = cone_consts();
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> dc, dn, dns, dh;
@@ -1008,7 +1057,7 @@ int sherd_cloud_upload(sherd_ctx *ctx, const double *points, const double *norma
   if (np == 0) return fail(ctx, SHERD_E_EMPTY, "a cloud needs at least one point");
   for (size_t i = 0; i < size_t(3) * np; ++i)
     if (!std::isfinite(points[i])) return fail(ctx, SHERD_E_INVALID, "non-finite point");
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   CK(cudaSetDevice(ctx->device));
   sherd_cloud *c = new sherd_cloud;
   int rc = cloud_build(ctx, points, normals, np, c);
@@ -1023,6 +1072,7 @@ int sherd_cloud_upload(sherd_ctx *ctx, const double *points, const double *norma
 int sherd_cloud_free(sherd_cloud *cloud) {
   if (!cloud) return SHERD_E_INVALID;
   cudaSetDevice(cloud->ctx->device);
+  CtxLock lock(cloud->ctx);
   delete cloud;
   return SHERD_OK;
 }
@@ -1033,7 +1083,7 @@ int sherd_nearest_within_sq(sherd_ctx *ctx, const sherd_cloud *cloud, const doub
                             double r2, uint32_t *idx, double *d2) {
   if (!ctx || !cloud || ((!queries || !idx || !d2) && n)) return fail(ctx, SHERD_E_INVALID, "null argument");
   if (n == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> q, o;
@@ -1053,7 +1103,7 @@ int sherd_nearest_below(sherd_ctx *ctx, const sherd_cloud *cloud, const double *
                         double bound, uint32_t *idx, double *dist) {
   if (!ctx || !cloud || ((!queries || !idx || !dist) && n)) return fail(ctx, SHERD_E_INVALID, "null argument");
   if (n == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> q, o;
@@ -1082,7 +1132,7 @@ int sherd_coarse_scores(sherd_ctx *ctx, const sherd_cloud *target, const double 
     std::fill(out, out + k, 0.0);
     return SHERD_OK;
   }
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<double> dp, dn, dt, dout;
@@ -1111,7 +1161,7 @@ int sherd_icp_rung(sherd_ctx *ctx, const double *source, uint32_t n_source, cons
   for (uint32_t c = 0; c < k; ++c)
     if (!finite_pose(inits + 16 * size_t(c))) return fail(ctx, SHERD_E_INVALID, "init pose is not finite");
   if (k == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   sherd_cloud src;
@@ -1169,7 +1219,7 @@ int sherd_icp_rung_noalloc(sherd_ctx *ctx, const double *source, uint32_t n_sour
       return fail(ctx, SHERD_E_INVALID,
                   "source, inits and out must be device (or managed) memory of the context's GPU");
   }
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);  // makes the context's device current
   if (rc) return rc;
   // The first call on a device looks the array's address up; that call should
@@ -1194,7 +1244,7 @@ int sherd_surfaces_create(sherd_ctx *ctx, const sherd_mesh *fracture, const sher
       ((!margin_p || !margin_n) && n_margin))
     return fail(ctx, SHERD_E_INVALID, "null argument");
   *out = nullptr;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   CK(cudaSetDevice(ctx->device));
   sherd_surfaces *x = new sherd_surfaces;
   x->ctx = ctx;
@@ -1254,6 +1304,7 @@ int sherd_surfaces_create(sherd_ctx *ctx, const sherd_mesh *fracture, const sher
 int sherd_surfaces_free(sherd_surfaces *s) {
   if (!s) return SHERD_E_INVALID;
   cudaSetDevice(s->ctx->device);
+  CtxLock lock(s->ctx);
   delete s;
   return SHERD_OK;
 }
@@ -1313,7 +1364,7 @@ int sherd_verify(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfaces *
   if (!ctx || !a || !b || !sc || !out) return fail(ctx, SHERD_E_INVALID, "null argument");
   if (!finite_pose(pose)) return fail(ctx, SHERD_E_INVALID, "pose is not finite");
   if (!(sc->t > 0.0)) return fail(ctx, SHERD_E_INVALID, "scales need t > 0");
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   int rc = begin(ctx);
   if (rc) return rc;
   DBuf<uint32_t> cells;
@@ -1361,7 +1412,7 @@ int sherd_pair_create(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfa
     return fail(ctx, SHERD_E_INVALID, "point-to-plane targets need normals");
   if ((n_reg && has_nan(reg_source, size_t(3) * n_reg)) || (n_frac && has_nan(frac_source, size_t(3) * n_frac)))
     return fail(ctx, SHERD_E_INVALID, "non-finite source point");
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   CK(cudaSetDevice(ctx->device));
   sherd_pair *p = new sherd_pair;
   p->ctx = ctx;
@@ -1396,6 +1447,7 @@ int sherd_pair_create(sherd_ctx *ctx, const sherd_surfaces *a, const sherd_surfa
 int sherd_pair_free(sherd_pair *pair) {
   if (!pair) return SHERD_E_INVALID;
   cudaSetDevice(pair->ctx->device);
+  CtxLock lock(pair->ctx);
   delete pair;
   return SHERD_OK;
 }
@@ -1663,7 +1715,10 @@ int capture_one(sherd_batch *b, int (*launch)(sherd_batch *, cudaStream_t), cuda
   exec = nullptr;
   graph = nullptr;
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  sherd_ctx *held = t_alloc_ctx;  // no pool calls recorded into the graph
+  t_alloc_ctx = nullptr;
   int rc = launch(b, ctx->stream);
+  t_alloc_ctx = held;
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
   if (rc) {
@@ -1902,7 +1957,7 @@ int sherd_batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pair
   int rc = check_batch_args(ctx, pairs, n_pairs, items, n_items, p, sched);
   if (rc) return rc;
   if (n_items == 0) return fail(ctx, SHERD_E_EMPTY, "a batch needs at least one work item");
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   CK(cudaSetDevice(ctx->device));
   sherd_batch *b = new sherd_batch;
   rc = batch_create(ctx, pairs, n_pairs, items, n_items, p, sched, b);
@@ -1916,14 +1971,14 @@ int sherd_batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pair
 
 int sherd_batch_run(sherd_batch *batch, float ms[SHERD_BATCH_TIMES]) {
   if (!batch) return SHERD_E_INVALID;
-  std::lock_guard<std::mutex> lock(batch->ctx->mu);
+  CtxLock lock(batch->ctx);
   return batch_run(batch, ms);
 }
 
 int sherd_batch_results(sherd_batch *batch, sherd_candidate *out) {
   if (!batch || !out) return SHERD_E_INVALID;
   sherd_ctx *ctx = batch->ctx;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   CK(cudaSetDevice(ctx->device));
   CK(cudaMemcpyAsync(out, batch->dc.p, sizeof(sherd_candidate) * batch->n_items,
                      cudaMemcpyDeviceToHost, ctx->stream));
@@ -1934,6 +1989,7 @@ int sherd_batch_results(sherd_batch *batch, sherd_candidate *out) {
 int sherd_batch_free(sherd_batch *batch) {
   if (!batch) return SHERD_E_INVALID;
   cudaSetDevice(batch->ctx->device);
+  CtxLock lock(batch->ctx);
   delete batch;
   return SHERD_OK;
 }
@@ -1945,7 +2001,7 @@ int sherd_ladder_verify_batch(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t
   if (rc) return rc;
   if (n_items == 0) return SHERD_OK;
   if (!out) return fail(ctx, SHERD_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   CK(cudaSetDevice(ctx->device));
   sherd_batch b;
   if ((rc = batch_create(ctx, pairs, n_pairs, items, n_items, p, sched, &b))) return rc;
@@ -1979,7 +2035,7 @@ int sherd_adjoint(sherd_ctx *ctx, sherd_pair *const *edges, uint32_t n_edges, co
     views[e] = edges[e]->view;
     if (!views[e].frac_tgt.nrm) return fail(ctx, SHERD_E_INVALID, "edge target without normals");
   }
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   NvtxRange range("sherd adjoint");
   int rc = begin(ctx);
   if (rc) return rc;
@@ -2143,7 +2199,7 @@ int sherd_segment(sherd_ctx *ctx, const sherd_mesh *mesh, const double *v, uint3
     mag = std::max(mag, std::fabs(v[i]));
   }
   const float pad = float(1e-6 * mag);
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   NvtxRange range("sherd segment");
   int rc = begin(ctx);
   if (rc) return rc;
@@ -2332,7 +2388,7 @@ int sherd_vertex_normals(sherd_ctx *ctx, const double *v, uint32_t nv, const uin
   for (size_t i = 0; i < size_t(3) * nf; ++i)
     if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
   if (nv == 0) return SHERD_OK;
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   NvtxRange range("sherd vertex_normals");
   int rc = begin(ctx);
   if (rc) return rc;
@@ -2360,7 +2416,7 @@ int sherd_fracture_cloud(sherd_ctx *ctx, const double *v, uint32_t nv, const uin
   if (nv == 0 || n_cent == 0 || !(radius > 0.0)) return SHERD_OK;
   double mag = 1.0;
   for (size_t i = 0; i < size_t(3) * n_cent; ++i) mag = std::max(mag, std::fabs(centroids[i]));
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   NvtxRange range("sherd fracture_cloud");
   int rc = begin(ctx);
   if (rc) return rc;
@@ -2468,7 +2524,7 @@ int sherd_refine_join(sherd_ctx *ctx, const double *source, uint32_t n_source,
     identity_registration(out[1]);
     return SHERD_OK;
   }
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   NvtxRange range("sherd refine_join");
   int rc = begin(ctx);
   if (rc) return rc;
@@ -2578,7 +2634,7 @@ int sherd_hypotheses_coarse(sherd_ctx *ctx, const sherd_frames *a, const sherd_f
   for (uint32_t j = 0; j < n_ib; ++j)
     if (ib[j] >= b->n) return fail(ctx, SHERD_E_INVALID, "ib names a point beyond b's frames");
   if (n_ia == 0 || n_ib == 0) return SHERD_OK;  // no hypothesis (R 5.1's empty return)
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   NvtxRange range("sherd hypotheses_coarse");
   int rc = begin(ctx);
   if (rc) return rc;
@@ -2858,7 +2914,7 @@ int sherd_breaklines(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_
   }
   if (nf == 0) return SHERD_OK;
   const float pad = float(1e-6 * mag);
-  std::lock_guard<std::mutex> lock(ctx->mu);
+  CtxLock lock(ctx);
   NvtxRange range("sherd breaklines");
   int rc = begin(ctx);
   if (rc) return rc;
