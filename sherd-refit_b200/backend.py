@@ -216,6 +216,18 @@ class Context:
                                             opt, C.cast(out, C.c_void_p)))
         return list(out)[:len(inits)]
 
+    def icp_rung_array(self, source, target: "Cloud", inits, distance, max_iteration=30,
+                       estimation=A.POINT_TO_PLANE) -> np.ndarray:
+        """icp_rung with its registrations as one REGISTRATION record array (no per-start
+        Python objects): rec["transform"] is the (n, 16) row-major poses."""
+        s = _f64(source)
+        inits = _f64(inits, (-1, 16))
+        out = np.zeros(max(len(inits), 1), REGISTRATION)
+        opt = A.IcpOptions(int(estimation), int(max_iteration), float(distance))
+        check(self.h, A.lib().sherd_icp_rung(self.h, ptr(s), len(s), target.h, inits, len(inits),
+                                            opt, out.ctypes.data_as(C.c_void_p)))
+        return out[:len(inits)]
+
     # -- preprocessing rays ---------------------------------------------------------------------
     def face_geometry(self, v, f):
         """mesh::geometry::face_geometry (mesh/geometry.rs:70-96): normals, areas, centroids."""
@@ -457,6 +469,7 @@ class Context:
 
 WORK_ITEM = np.dtype(A.WorkItem)
 CANDIDATE = np.dtype(A.Candidate)
+REGISTRATION = np.dtype(A.Registration)
 
 
 def work_items(items) -> C.Array:

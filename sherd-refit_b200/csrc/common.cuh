@@ -163,6 +163,55 @@ __device__ __forceinline__ double key2d(unsigned long long k) {
   return __longlong_as_double(b);
 }
 
+// What the input checks found in an uploaded array: the largest |x| of its
+// finite coordinates (the f64 bits of a non-negative value, which order as
+// u64), whether any coordinate was not finite, and whether any index reached
+// its limit.
+struct InputCheck {
+  unsigned long long max_abs;
+  unsigned non_finite;
+  unsigned bad_index;
+};
+
+__device__ __forceinline__ void input_check_commit(InputCheck *out, unsigned long long m, unsigned nonf,
+                                                   unsigned bad) {
+  for (int o = 16; o; o >>= 1) {
+    unsigned long long other = __shfl_xor_sync(0xffffffffu, m, o);
+    m = other > m ? other : m;
+    nonf |= __shfl_xor_sync(0xffffffffu, nonf, o);
+    bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (m) atomicMax(&out->max_abs, m);
+    if (nonf) atomicOr(&out->non_finite, 1u);
+    if (bad) atomicOr(&out->bad_index, 1u);
+  }
+}
+
+// Coordinates: every value finite, and the largest magnitude.
+__global__ void k_check_coords(const double *p, size_t n, InputCheck *out) {
+  unsigned long long m = 0;
+  unsigned nonf = 0;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    double x = p[i];
+    if (isfinite(x)) {
+      unsigned long long b = (unsigned long long)__double_as_longlong(fabs(x));
+      m = b > m ? b : m;
+    } else {
+      nonf = 1;
+    }
+  }
+  input_check_commit(out, m, nonf, 0);
+}
+
+// Indices: every one below `limit`.
+__global__ void k_check_indices(const uint32_t *f, size_t n, uint32_t limit, InputCheck *out) {
+  unsigned bad = 0;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    bad |= f[i] >= limit ? 1u : 0u;
+  input_check_commit(out, 0, 0, bad);
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

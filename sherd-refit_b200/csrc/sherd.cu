@@ -233,6 +233,44 @@ int upload(sherd_ctx *ctx, DBuf<T> &buf, const T *host, size_t n) {
   return SHERD_OK;
 }
 
+// Checks of inputs already on the device, in place of host loops over them:
+// each call of coords/indices adds one launch into `slot`, read() waits for
+// them and hands back what they found.
+struct DevInputCheck {
+  DBuf<InputCheck> d;
+  int open(sherd_ctx *ctx, int slots) {
+    CK(d.alloc(slots));
+    CK(cudaMemsetAsync(d.p, 0, sizeof(InputCheck) * slots, ctx->stream));
+    return SHERD_OK;
+  }
+  int coords(sherd_ctx *ctx, int slot, const double *p, size_t n) {
+    if (!n) return SHERD_OK;
+    k_check_coords<<<std::min(blocks_for(n), unsigned(ctx->sm_count) * 8u), 256, 0, ctx->stream>>>(
+        p, n, d.p + slot);
+    CK(cudaGetLastError());
+    return SHERD_OK;
+  }
+  int indices(sherd_ctx *ctx, int slot, const uint32_t *f, size_t n, uint32_t limit) {
+    if (!n) return SHERD_OK;
+    k_check_indices<<<std::min(blocks_for(n), unsigned(ctx->sm_count) * 8u), 256, 0, ctx->stream>>>(
+        f, n, limit, d.p + slot);
+    CK(cudaGetLastError());
+    return SHERD_OK;
+  }
+  int read(sherd_ctx *ctx, InputCheck *h) {
+    CK(cudaMemcpyAsync(h, d.p, sizeof(InputCheck) * d.n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SHERD_OK;
+  }
+};
+
+// The largest finite magnitude a coordinate check saw, at least 1.
+double checked_mag(const InputCheck &c) {
+  double m;
+  std::memcpy(&m, &c.max_abs, 8);
+  return std::max(1.0, m);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -893,8 +931,6 @@ int sherd_penetration_share(sherd_ctx *ctx, const sherd_mesh *mesh, const double
 int sherd_face_geometry(sherd_ctx *ctx, const double *v, uint32_t nv, const uint32_t *f, uint32_t nf,
                         double *normals, double *areas, double *centroids) {
   if (!ctx || ((!v && nv) || (!f && nf))) return fail(ctx, SHERD_E_INVALID, "null argument");
-  for (size_t i = 0; i < size_t(3) * nf; ++i)
-    if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
   if (nf == 0) return SHERD_OK;
   CtxLock lock(ctx);
   int rc = begin(ctx);
@@ -902,6 +938,12 @@ int sherd_face_geometry(sherd_ctx *ctx, const double *v, uint32_t nv, const uint
   DBuf<double> dv, dn, da, dc;
   DBuf<uint32_t> df;
   if ((rc = upload(ctx, dv, v, size_t(3) * nv)) || (rc = upload(ctx, df, f, size_t(3) * nf))) return rc;
+  DevInputCheck chk;
+  InputCheck got;
+  if ((rc = chk.open(ctx, 1)) || (rc = chk.indices(ctx, 0, df.p, size_t(3) * nf, nv)) ||
+      (rc = chk.read(ctx, &got)))
+    return rc;
+  if (got.bad_index) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
   if (normals) CK(dn.alloc(size_t(3) * nf));
   if (areas) CK(da.alloc(nf));
   if (centroids) CK(dc.alloc(size_t(3) * nf));
@@ -2385,8 +2427,7 @@ int sherd_vertex_normals(sherd_ctx *ctx, const double *v, uint32_t nv, const uin
                          uint32_t nf, double *normals) {
   if (!ctx || ((!v || !normals) && nv) || (!f && nf)) return fail(ctx, SHERD_E_INVALID, "null argument");
   if (uint64_t(nf) * 3u >= (uint64_t(1) << 31)) return fail(ctx, SHERD_E_INVALID, "too many faces");
-  for (size_t i = 0; i < size_t(3) * nf; ++i)
-    if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
+  if (nv == 0 && nf) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
   if (nv == 0) return SHERD_OK;
   CtxLock lock(ctx);
   NvtxRange range("sherd vertex_normals");
@@ -2395,6 +2436,12 @@ int sherd_vertex_normals(sherd_ctx *ctx, const double *v, uint32_t nv, const uin
   DBuf<double> dv, dn;
   DBuf<uint32_t> df;
   if ((rc = upload(ctx, dv, v, size_t(3) * nv)) || (rc = upload(ctx, df, f, size_t(3) * nf))) return rc;
+  DevInputCheck chk;
+  InputCheck got;
+  if ((rc = chk.open(ctx, 1)) || (rc = chk.indices(ctx, 0, df.p, size_t(3) * nf, nv)) ||
+      (rc = chk.read(ctx, &got)))
+    return rc;
+  if (got.bad_index) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
   if ((rc = vertex_normals_dev(ctx, dv.p, nv, df.p, nf, dn))) return rc;
   CK(cudaMemcpyAsync(normals, dn.p, 24 * size_t(nv), cudaMemcpyDeviceToHost, ctx->stream));
   return finish(ctx, "vertex_normals", nv, true);
@@ -2409,13 +2456,6 @@ int sherd_fracture_cloud(sherd_ctx *ctx, const double *v, uint32_t nv, const uin
     return fail(ctx, SHERD_E_INVALID, "null argument");
   *n_out = 0;
   if (uint64_t(nf) * 3u >= (uint64_t(1) << 31)) return fail(ctx, SHERD_E_INVALID, "too many faces");
-  for (size_t i = 0; i < size_t(3) * nf; ++i)
-    if (f[i] >= nv) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
-  if (!all_finite(centroids, size_t(3) * n_cent) || !all_finite(v, size_t(3) * nv))
-    return fail(ctx, SHERD_E_INVALID, "coordinates must be finite");
-  if (nv == 0 || n_cent == 0 || !(radius > 0.0)) return SHERD_OK;
-  double mag = 1.0;
-  for (size_t i = 0; i < size_t(3) * n_cent; ++i) mag = std::max(mag, std::fabs(centroids[i]));
   CtxLock lock(ctx);
   NvtxRange range("sherd fracture_cloud");
   int rc = begin(ctx);
@@ -2428,6 +2468,18 @@ int sherd_fracture_cloud(sherd_ctx *ctx, const double *v, uint32_t nv, const uin
       (rc = upload(ctx, dc, centroids, size_t(3) * n_cent)) ||
       (rc = upload(ctx, dfrac, fracture, size_t(n_cent))))
     return rc;
+  // The face indices, and the vertices and centroids finite, checked where
+  // they now lie; the centroids' largest magnitude sizes their tree's padding.
+  DevInputCheck chk;
+  InputCheck got[2];
+  if ((rc = chk.open(ctx, 2)) || (rc = chk.indices(ctx, 0, df.p, size_t(3) * nf, nv)) ||
+      (rc = chk.coords(ctx, 0, dv.p, size_t(3) * nv)) ||
+      (rc = chk.coords(ctx, 1, dc.p, size_t(3) * n_cent)) || (rc = chk.read(ctx, got)))
+    return rc;
+  if (got[0].bad_index) return fail(ctx, SHERD_E_INVALID, "face index beyond the vertex array");
+  if (got[0].non_finite || got[1].non_finite) return fail(ctx, SHERD_E_INVALID, "coordinates must be finite");
+  if (nv == 0 || n_cent == 0 || !(radius > 0.0)) return SHERD_OK;
+  const double mag = checked_mag(got[1]);
   // The centroids' tree, the nearest centroid of every vertex strictly within
   // the radius (refine.rs:161-178), and the vertices whose nearest is a
   // fracture face, ascending.
@@ -2723,14 +2775,20 @@ extern "C" {
 int sherd_order_by_score(const double *score, uint32_t n, uint32_t limit, uint32_t *order,
                          uint32_t *n_order) {
   if (!n_order || ((!score || (!order && limit)) && n)) return SHERD_E_INVALID;
-  std::vector<uint32_t> idx(n);
-  for (uint32_t i = 0; i < n; ++i) idx[i] = i;
-  std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
-    int64_t kx = total_key(score[x]), ky = total_key(score[y]);
-    return kx != ky ? kx > ky : x < y;
-  });
-  uint32_t m = std::min(n, limit);
-  std::copy(idx.begin(), idx.begin() + m, order);
+  // Each score's total-order key computed once, beside its index; the first
+  // `limit` of the order selected, then only they sorted. The order is total
+  // (no two entries compare equal), so the result is the full sort's head.
+  struct Keyed {
+    int64_t key;
+    uint32_t i;
+  };
+  std::vector<Keyed> keyed(n);
+  for (uint32_t i = 0; i < n; ++i) keyed[i] = {total_key(score[i]), i};
+  auto before = [](const Keyed &x, const Keyed &y) { return x.key != y.key ? x.key > y.key : x.i < y.i; };
+  const uint32_t m = std::min(n, limit);
+  if (m < n) std::nth_element(keyed.begin(), keyed.begin() + m, keyed.end(), before);
+  std::sort(keyed.begin(), keyed.begin() + m, before);
+  for (uint32_t k = 0; k < m; ++k) order[k] = keyed[k].i;
   *n_order = m;
   return SHERD_OK;
 }

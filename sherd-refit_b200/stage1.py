@@ -136,10 +136,10 @@ class PairStage1:
             return np.zeros((0, 4, 4)), np.zeros(0)
         poses = hyp.poses[kept]
         for k in STAGE1_RUNGS:
-            regs = self.ctx.icp_rung(self.brk_points, self.target, poses,
-                                     k * self.scales.t * self.scales.icp, STAGE1_ITERATIONS,
-                                     estimation=A.POINT_TO_POINT)
-            poses = np.stack([r.pose() for r in regs])
+            regs = self.ctx.icp_rung_array(self.brk_points, self.target, poses,
+                                           k * self.scales.t * self.scales.icp, STAGE1_ITERATIONS,
+                                           estimation=A.POINT_TO_POINT)
+            poses = np.ascontiguousarray(regs["transform"]).reshape(-1, 4, 4)
         scores = self.ctx.coarse_scores(self.target, self.brk_points, self.brk_normals, poses,
                                         self.scales.stage1, NORMAL_AGREE)
         return poses, np.asarray(scores, np.float64)

@@ -398,6 +398,15 @@ def test_point_to_point_rungs_match_the_oracle(sherd, gpu_ctx, oracle, slab):
                             sherd._abi.POINT_TO_POINT)
     for r, pose in zip(held, slab["s1_T"]):
         assert trace_deg(r.pose(), pose) < 1e-3 and origin_t(r.pose(), pose, t) < 1e-6
+    # The record-array form of the same call carries the same registrations, field for field.
+    rec = gpu_ctx.icp_rung_array(src, target_g, slab["s1_T"], 0.08 * t * icp, 20,
+                                 sherd._abi.POINT_TO_POINT)
+    assert len(rec) == len(held)
+    for r, h in zip(rec, held):
+        assert np.array_equal(r["transform"], np.array(h.transform[:]))
+        assert (r["fitness"], r["inlier_rmse"], r["correspondences"], r["iterations"],
+                r["converged"]) == (h.fitness, h.inlier_rmse, h.correspondences, h.iterations,
+                                    h.converged)
 
 
 def test_penetration_share_matches_verify_and_the_oracle(sherd, gpu_ctx, gpu_slab, cpu_slab,

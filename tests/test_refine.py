@@ -456,3 +456,39 @@ def test_device_walk_saddle_and_edge_cases(sherd, gpu_ctx):
         gpu_ctx.refine_join(pts, pts, nrm, np.eye(4), np.eye(4), [0.1, 0.05], -1)
     with pytest.raises(sherd.SherdError):
         gpu_ctx.vertex_normals(pts, np.array([[0, 1, 400]], np.uint32))
+
+
+@pytest.mark.gpu
+def test_fused_cloud_and_face_inputs_are_checked_on_the_device(sherd, gpu_ctx, slab):
+    """The face indices, the vertices and the centroids are checked after their upload: an index
+    at the vertex count, or one non-finite coordinate anywhere, is refused with E_INVALID and the
+    context stays usable; with clean inputs the call then gives the same cloud as before."""
+    _abi = importlib.import_module("sherd-refit_b200._abi")
+    p = piece(slab, "pieceA")
+    v = np.asarray(p["V0"], np.float64)
+    f = np.asarray(p["F"], np.uint32)
+    cen = _centroids(p["V"], p["F"])
+    frac = p["frac"]
+    thick, res = (float(x) for x in p["stats_thick_res"])
+    radius = max(_refine_mod().SELECT_T * thick, _refine_mod().SELECT_RES * res)
+    want = gpu_ctx.fracture_cloud(v, f, cen, frac, radius)
+    bad_f = f.copy()
+    bad_f[len(f) // 2, 1] = len(v)
+    for call in (lambda: gpu_ctx.fracture_cloud(v, bad_f, cen, frac, radius),
+                 lambda: gpu_ctx.vertex_normals(v, bad_f),
+                 lambda: gpu_ctx.face_geometry(v, bad_f)):
+        with pytest.raises(sherd.SherdError) as e:
+            call()
+        assert e.value.code == _abi.E_INVALID
+    for which in ("v", "cen"):
+        for x in (np.nan, np.inf):
+            vv, cc = v.copy(), cen.copy()
+            (vv if which == "v" else cc)[len(vv if which == "v" else cc) - 1, 2] = x
+            with pytest.raises(sherd.SherdError) as e:
+                gpu_ctx.fracture_cloud(vv, f, cc, frac, radius)
+            assert e.value.code == _abi.E_INVALID
+    # No vertices but faces: every index is out of range.
+    with pytest.raises(sherd.SherdError):
+        gpu_ctx.vertex_normals(np.zeros((0, 3)), f[:1])
+    got = gpu_ctx.fracture_cloud(v, f, cen, frac, radius)
+    assert all(np.array_equal(a, b) for a, b in zip(got, want))

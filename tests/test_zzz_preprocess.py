@@ -57,6 +57,11 @@ class _OracleDevice:
                                point_to_point=estimation == A.POINT_TO_POINT)
         return [A.Registration.from_buffer_copy(r) for r in regs]
 
+    def icp_rung_array(self, *a, **k):
+        regs = self.icp_rung(*a, **k)
+        rec = importlib.import_module("sherd-refit_b200.backend").REGISTRATION
+        return np.frombuffer(b"".join(bytes(r) for r in regs), rec)
+
     def coarse_scores(self, target, points, normals, poses, radius, normal_agree=0.7):
         return self.o.coarse_scores(target, points, normals, poses, radius, normal_agree)
 
