@@ -410,6 +410,19 @@ class Context:
         q, qn = _f64(q), _f64(qn)
         fa, fb = _frames(frames_a), _frames(frames_b)
         count = C.c_uint32(0)
+        grid = len(ia) * len(ib)
+        if grid <= HYP_ONE_CALL:
+            # Room for every (i, j): one call, the outputs cut to the count.
+            pa, pb = np.empty(grid, np.uint32), np.empty(grid, np.uint32)
+            poses, scores = np.empty((grid, 4, 4)), np.empty(grid)
+            if grid:
+                check(self.h, A.lib().sherd_hypotheses_coarse(
+                    self.h, C.byref(fa[0]), C.byref(fb[0]), ia, len(ia), ib, len(ib),
+                    float(dihedral_tol), target.h, q, qn, len(q), float(delta),
+                    float(normal_agree), grid, ptr(pa), ptr(pb), ptr(poses), ptr(scores),
+                    C.byref(count)))
+            n = count.value
+            return pa[:n].copy(), pb[:n].copy(), poses[:n].copy(), scores[:n].copy()
         check(self.h, A.lib().sherd_hypotheses_coarse(
             self.h, C.byref(fa[0]), C.byref(fb[0]), ia, len(ia), ib, len(ib), float(dihedral_tol),
             target.h, q, qn, len(q), float(delta), float(normal_agree), 0, None, None, None, None,
@@ -466,6 +479,10 @@ class Context:
                                                 C.cast(out, C.c_void_p)))
         return list(out)
 
+
+# Up to this many (i, j) frame pairs, hypotheses_coarse makes one call with room for all of
+# them (128 B of poses each); above it, a counting call first.
+HYP_ONE_CALL = 1 << 20
 
 WORK_ITEM = np.dtype(A.WorkItem)
 CANDIDATE = np.dtype(A.Candidate)

@@ -496,7 +496,7 @@ template <class H>
 __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView &tgt,
                                double distance, int max_iter, IcpShared &sh, H *hint,
                                sherd_registration *out, uint32_t &status,
-                               bool point_to_point = false) {
+                               bool point_to_point = false, bool keep_hints = false) {
   if (ns == 0 || tgt.n == 0) {
     if (threadIdx.x == 0) {
       for (int k = 0; k < 16; ++k) out->transform[k] = sh.t[k];
@@ -511,7 +511,11 @@ __device__ void icp_rung_block(const double4 *src, uint32_t ns, const CloudView 
   }
   bool valid = distance > 0.0;  // a NaN radius is not valid either
   double r2 = distance * distance;
-  for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) hint_set(hint, i, -1);
+  // keep_hints: the previous rung ran over the same source and target, so its
+  // last matches seed this rung's first searches (the answers do not depend on
+  // the seed, only the work does).
+  if (!keep_hints)
+    for (uint32_t i = threadIdx.x; i < ns; i += ICP_BLOCK) hint_set(hint, i, -1);
   icp_pass(src, ns, tgt, r2, valid, sh, hint, status, point_to_point);
   double fit, rmse;
   fit_rmse(sh.sums, ns, fit, rmse);

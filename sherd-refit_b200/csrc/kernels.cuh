@@ -417,11 +417,15 @@ __global__ void __launch_bounds__(ICP_BLOCK, MINB) k_ladder(const PairView *pair
     const double k[4] = {0.2, 0.08, 0.08, 0.04};
     for (int r = r_lo; r < r_hi; ++r) {
       double distance = k[r] * pr.sc.t * pr.sc.icp;
+      // Rungs 1 and 3 follow a rung over the same clouds (0 and 2): when that
+      // rung ran in this launch, its matches are this block's hints.
+      const bool keep = (r & 1) && r > r_lo;
       if (r < 2)
-        icp_rung_block(pr.reg_src, pr.n_reg, pr.reg_tgt, distance, 30, sh, hint, &c->rungs[r], st);
+        icp_rung_block(pr.reg_src, pr.n_reg, pr.reg_tgt, distance, 30, sh, hint, &c->rungs[r], st,
+                       false, keep);
       else
         icp_rung_block(pr.frac_src, pr.n_frac, pr.frac_tgt, distance, 30, sh, hint, &c->rungs[r],
-                       st);
+                       st, false, keep);
     }
   }
   if (st) atomicOr(status, st);
