@@ -17,6 +17,10 @@ namespace sherd {
 constexpr uint32_t MISS = 0xFFFFFFFFu;
 constexpr int TRI_LEAF = 4;    // faces per BVH leaf
 constexpr int POINT_LEAF = 8;  // points per BVH leaf
+// Whether point clouds carry the 4-wide tree that nearest_within_sq walks.
+#ifndef WIDE_NN
+#define WIDE_NN 1
+#endif
 constexpr int STACK = 64;      // traversal stack entries (Karras depth <= 63 + log2 n)
 
 __host__ __device__ inline float f_inf() { return __builtin_huge_valf(); }

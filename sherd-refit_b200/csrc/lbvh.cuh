@@ -27,6 +27,18 @@ struct __align__(16) BNode {
   int4 d;    // ref0 ref1 cnt0 cnt1  (cnt > 0: leaf range at ref; cnt == 0: node ref)
 };
 
+// The 4-wide form of a point tree for the nearest-point search: the node at a
+// binary node's index holds that node's grandchildren (or a child itself where
+// the child is a leaf range), so a descent takes half as many dependent loads.
+// The boxes are the binary tree's own padded boxes. 128 B, eight 16-byte loads:
+// the four children's boxes by coordinate, then per child the internal node
+// index or the leaf's first slot, and the leaf's count (0 for a node, -1 for no
+// child; an absent child's box is empty, so every box distance to it is +inf).
+struct __align__(16) WNode {
+  float4 lox, loy, loz, hix, hiy, hiz;
+  int4 ref, cnt;
+};
+
 // The crossing grid of one axis: the mesh projected onto the plane of the other
 // two axes (u, v) = ((a+1)%3, (a+2)%3), cut into square cells; each cell lists
 // (CSR) the sorted slots of every face whose padded projected rectangle
@@ -69,6 +81,7 @@ struct CloudView {
   uint32_t n;
   uint32_t root_leaf;
   float pad;
+  const WNode *wide;   // the 4-wide form of `nodes`, or null
 };
 
 // ---- Morton codes -----------------------------------------------------------
@@ -330,6 +343,59 @@ __global__ void k_emit(const float *v, const uint32_t *f, const double *p, const
   nd.c = make_float4(bx[1].lo[2], bx[1].hi[0], bx[1].hi[1], bx[1].hi[2]);
   nd.d = make_int4(ref[0], ref[1], cnt[0], cnt[1]);
   nodes[i] = nd;
+}
+
+// One WNode per binary node i: i's children, a child that is an internal node
+// replaced by that node's two children.
+__global__ void k_widen(const BNode *nodes, int ni, WNode *wide) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ni) return;
+  float lo[4][3], hi[4][3];
+  int ref[4], cnt[4], m = 0;
+  auto put = [&](const BNode &b, int c) {
+    const float4 a = b.a, bb = b.b, cc = b.c;
+    if (c == 0) {
+      lo[m][0] = a.x; lo[m][1] = a.y; lo[m][2] = a.z;
+      hi[m][0] = a.w; hi[m][1] = bb.x; hi[m][2] = bb.y;
+      ref[m] = b.d.x;
+      cnt[m] = b.d.z;
+    } else {
+      lo[m][0] = bb.z; lo[m][1] = bb.w; lo[m][2] = cc.x;
+      hi[m][0] = cc.y; hi[m][1] = cc.z; hi[m][2] = cc.w;
+      ref[m] = b.d.y;
+      cnt[m] = b.d.w;
+    }
+    ++m;
+  };
+  const BNode b = nodes[i];
+  for (int c = 0; c < 2; ++c) {
+    const int r = c == 0 ? b.d.x : b.d.y, n = c == 0 ? b.d.z : b.d.w;
+    if (n > 0) {
+      put(b, c);
+    } else {
+      const BNode g = nodes[r];
+      put(g, 0);
+      put(g, 1);
+    }
+  }
+  for (; m < 4; ++m) {
+    for (int a = 0; a < 3; ++a) {
+      lo[m][a] = f_inf();
+      hi[m][a] = -f_inf();
+    }
+    ref[m] = -1;
+    cnt[m] = -1;
+  }
+  WNode w;
+  w.lox = make_float4(lo[0][0], lo[1][0], lo[2][0], lo[3][0]);
+  w.loy = make_float4(lo[0][1], lo[1][1], lo[2][1], lo[3][1]);
+  w.loz = make_float4(lo[0][2], lo[1][2], lo[2][2], lo[3][2]);
+  w.hix = make_float4(hi[0][0], hi[1][0], hi[2][0], hi[3][0]);
+  w.hiy = make_float4(hi[0][1], hi[1][1], hi[2][1], hi[3][1]);
+  w.hiz = make_float4(hi[0][2], hi[1][2], hi[2][2], hi[3][2]);
+  w.ref = make_int4(ref[0], ref[1], ref[2], ref[3]);
+  w.cnt = make_int4(cnt[0], cnt[1], cnt[2], cnt[3]);
+  wide[i] = w;
 }
 
 // ---- crossing grids ---------------------------------------------------------

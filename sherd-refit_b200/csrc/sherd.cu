@@ -292,6 +292,7 @@ struct sherd_mesh {
 struct sherd_cloud {
   sherd_ctx *ctx = nullptr;
   DBuf<BNode> nodes;
+  DBuf<WNode> wide;  // the 4-wide form of nodes, for the nearest-point search
   DBuf<double4> pts, nrm;
   CloudView view{};
 };
@@ -522,6 +523,12 @@ int cloud_build_dev(sherd_ctx *ctx, const double *dp, const double *dn, uint32_t
   k_store_pts<<<blocks_for(np), 256, 0, ctx->stream>>>(dp, dn, sorted.p, np, c->pts.p,
                                                        dn ? c->nrm.p : nullptr);
   CK(cudaGetLastError());
+  const bool tree = np > uint32_t(POINT_LEAF);
+  if (tree && WIDE_NN) {
+    CK(c->wide.alloc(np - 1));
+    k_widen<<<blocks_for(np - 1), 256, 0, ctx->stream>>>(c->nodes.p, int(np - 1), c->wide.p);
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   c->ctx = ctx;
   CloudView &v = c->view;
@@ -531,6 +538,7 @@ int cloud_build_dev(sherd_ctx *ctx, const double *dp, const double *dn, uint32_t
   v.n = np;
   v.root_leaf = np <= uint32_t(POINT_LEAF) ? np : 0;
   v.pad = pad;
+  v.wide = tree && WIDE_NN ? c->wide.p : nullptr;
   return SHERD_OK;
 }
 
