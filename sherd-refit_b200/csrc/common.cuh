@@ -15,8 +15,14 @@
 namespace sherd {
 
 constexpr uint32_t MISS = 0xFFFFFFFFu;
-constexpr int TRI_LEAF = 4;    // faces per BVH leaf
-constexpr int POINT_LEAF = 8;  // points per BVH leaf
+#ifndef TRI_LEAF_MAX
+#define TRI_LEAF_MAX 6
+#endif
+constexpr int TRI_LEAF = TRI_LEAF_MAX;  // faces per BVH leaf, at most
+#ifndef POINT_LEAF_MAX
+#define POINT_LEAF_MAX 2
+#endif
+constexpr int POINT_LEAF = POINT_LEAF_MAX;  // points per BVH leaf, at most
 // Whether point clouds carry the 4-wide tree that nearest_within_sq walks.
 #ifndef WIDE_NN
 #define WIDE_NN 1
