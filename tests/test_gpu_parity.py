@@ -247,6 +247,34 @@ def test_invalid_inputs_are_refused(sherd, gpu_ctx, gpu_slab):
         gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], [(3, 0, np.eye(4))], sherd.default_params())
 
 
+def test_nearest_neighbours_on_every_tree_shape(gpu_ctx, oracle):
+    """The 4-wide walk (k_widen's collapse of the binary tree, leaves of at most two points)
+    against the oracle, bit for bit: clouds of 1 to 1000 points (a root leaf, one internal node,
+    wide nodes with absent children), clouds of few distinct points repeated many times (equal
+    Morton codes split by index), collinear and coplanar clouds (flat boxes), queries inside,
+    on and far outside the cloud, at several radii."""
+    rng = np.random.default_rng(11)
+    clouds = []
+    for n in (1, 2, 3, 4, 5, 7, 8, 9, 16, 17, 33, 100, 1000):
+        clouds.append(rng.uniform(-3, 3, size=(n, 3)))
+    base = rng.uniform(-1, 1, size=(7, 3))
+    clouds.append(base[rng.integers(0, 7, size=300)])                  # 7 points, 300 copies
+    t = rng.uniform(-2, 2, size=200)
+    clouds.append(np.column_stack([t, 0.5 * t, np.full(200, 0.25)]))   # collinear
+    clouds.append(np.column_stack([rng.uniform(-2, 2, (300, 2)), np.zeros(300)]))  # coplanar
+    for pts in clouds:
+        q = np.vstack([pts[: min(len(pts), 50)] + rng.normal(0, 0.05, (min(len(pts), 50), 3)),
+                       rng.uniform(-4, 4, size=(100, 3)), rng.uniform(-40, 40, size=(20, 3))])
+        cg, cc = gpu_ctx.cloud(pts), oracle.Cloud(pts)
+        for r in (0.01, 0.3, 2.0, 100.0):
+            i_g, d_g = cg.nearest_within_sq(q, r * r)
+            i_c, d_c = cc.nearest_within_sq(q, r * r)
+            assert np.array_equal(i_g, i_c) and np.array_equal(d_g, d_c), (len(pts), r)
+            j_g, e_g = cg.nearest_below(q, r)
+            j_c, e_c = cc.nearest_below(q, r)
+            assert np.array_equal(j_g, j_c) and np.array_equal(e_g, e_c), (len(pts), r)
+
+
 def test_empty_and_tiny_inputs(sherd, gpu_ctx, oracle):
     tri_v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
     tri_f = np.array([[0, 1, 2]], np.uint32)
