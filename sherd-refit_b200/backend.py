@@ -292,17 +292,38 @@ class Context:
     def batch(self, pairs, items, params: A.Params, sched=A.SCHED_BATCHED) -> "Batch":
         return Batch(self, pairs, items, params, sched)
 
-    def ladder_verify_batch(self, pairs, items, params: A.Params, sched=A.SCHED_BATCHED):
-        """R 5.6 + R 6 + R 6.5 for every (pair, start); `items` is a ctypes WorkItem array or a
-        list of (pair, start, init 4x4) tuples. Returns the ctypes Candidate array."""
-        if not isinstance(items, C.Array):
-            items = work_items(items)
+    def ladder_verify_batch(self, pairs, items, params: A.Params, sched=A.SCHED_BATCHED,
+                            out=None):
+        """R 5.6 + R 6 + R 6.5 for every (pair, start); `items` is a ctypes WorkItem array, a
+        WORK_ITEM numpy array, or a list of (pair, start, init 4x4) tuples. The candidates go
+        into `out` when given (a CANDIDATE numpy array or ctypes Candidate array with room for
+        every item, e.g. in pinned memory reused from call to call), else into a new ctypes
+        Candidate array; either is returned."""
+        if isinstance(items, np.ndarray):
+            if items.dtype != WORK_ITEM or not items.flags.c_contiguous:
+                raise A.SherdError(A.E_INVALID, "items must be a contiguous WORK_ITEM array")
+            n_items, items_ptr = len(items), items.ctypes.data_as(C.c_void_p)
+        else:
+            if not isinstance(items, C.Array):
+                items = work_items(items)
+            n_items, items_ptr = len(items), C.cast(items, C.c_void_p)
+        if out is None:
+            out = (A.Candidate * max(n_items, 1))()
+            out_ptr = C.cast(out, C.c_void_p)
+        elif isinstance(out, np.ndarray):
+            if out.dtype != CANDIDATE or not out.flags.c_contiguous or not out.flags.writeable \
+                    or len(out) < n_items:
+                raise A.SherdError(A.E_INVALID, "out must be a writable contiguous CANDIDATE "
+                                                "array with room for every item")
+            out_ptr = out.ctypes.data_as(C.c_void_p)
+        else:
+            if len(out) < n_items:
+                raise A.SherdError(A.E_INVALID, "out has no room for every item")
+            out_ptr = C.cast(out, C.c_void_p)
         arr = (C.c_void_p * max(len(pairs), 1))(*[p.h for p in pairs])
-        out = (A.Candidate * max(len(items), 1))()
-        check(self.h, A.lib().sherd_ladder_verify_batch(self.h, arr, len(pairs),
-                                                       C.cast(items, C.c_void_p), len(items),
-                                                       C.byref(params), int(sched),
-                                                       C.cast(out, C.c_void_p)))
+        check(self.h, A.lib().sherd_ladder_verify_batch(self.h, arr, len(pairs), items_ptr,
+                                                       n_items, C.byref(params), int(sched),
+                                                       out_ptr))
         return out
 
     def penetration_share(self, mesh: "Mesh", points, pose, pen) -> float:

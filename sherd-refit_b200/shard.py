@@ -50,8 +50,13 @@ def gather_candidates(wl, dev, cands, device=None) -> np.ndarray:
     """Every item's candidate in the collection's item order, on every rank: this rank's
     candidates (a structured sherd_candidate array over dev's items) get the collection's pair
     index and travel with their item index in one all-gather of fixed-size records."""
+    import torch.distributed as dist
     from .backend import CANDIDATE
     cands = np.asarray(cands)
+    alone = not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1
+    if alone and len(cands) == wl.n_items and _identity(dev.item_index) \
+            and _identity(dev.pair_index):
+        return cands  # one rank holding the whole collection in its own order: nothing to move
     mine = cands.copy()
     mine["pair"] = np.asarray(dev.pair_index, np.int64)[cands["pair"].astype(np.int64)]
     rec = np.dtype([("item", np.uint64), ("cand", CANDIDATE)])
@@ -67,6 +72,14 @@ def gather_candidates(wl, dev, cands, device=None) -> np.ndarray:
     if not seen.all():
         raise RuntimeError(f"{int((~seen).sum())} items were verified by no rank")
     return out
+
+
+def _identity(index) -> bool:
+    """Whether an index array is 0, 1, ..., len - 1 (no array: the identity)."""
+    if index is None:
+        return True
+    index = np.asarray(index)
+    return bool(np.array_equal(index, np.arange(len(index), dtype=index.dtype)))
 
 
 def max_over_ranks(x: float, device=None) -> float:

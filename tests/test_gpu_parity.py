@@ -10,6 +10,7 @@ rows of the fixture.
 from __future__ import annotations
 
 import ctypes as C
+import importlib
 import threading
 import time
 
@@ -230,6 +231,19 @@ def test_batched_path_is_deterministic(sherd, gpu_ctx, gpu_slab, slab):
     a = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items, p)
     b = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items, p)
     assert bytes(a) == bytes(b)
+    # The same call with the work items and the candidates in caller-held numpy buffers (the
+    # bench's pinned ones), the output buffer longer than needed and reused.
+    import torch
+    be = importlib.import_module("sherd-refit_b200.backend")
+    raw = torch.empty(len(items) * be.WORK_ITEM.itemsize, dtype=torch.uint8, pin_memory=True)
+    items_host = raw.numpy().view(be.WORK_ITEM)
+    items_host[:] = np.ctypeslib.as_array(sherd.work_items(items))[:len(items)]
+    out = np.zeros(len(items) + 5, be.CANDIDATE)
+    for _ in range(2):
+        got = gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items_host, p, out=out)
+        assert got is out and bytes(out[:len(items)]) == bytes(a)
+    with pytest.raises(sherd.SherdError):
+        gpu_ctx.ladder_verify_batch([gpu_slab["pair"]], items_host, p, out=out[:3])
 
 
 def test_invalid_inputs_are_refused(sherd, gpu_ctx, gpu_slab):
