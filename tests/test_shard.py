@@ -106,6 +106,33 @@ def test_two_gloo_ranks_split_a_collection_by_pairs_and_gather_every_candidate()
     mp.spawn(_rank_main, args=(2, _free_port()), nprocs=2, join=True)
 
 
+def test_one_rank_gather_is_the_candidates_themselves():
+    """Without a process group, a device collection that holds every pair and item in the
+    workload's order gathers to the candidates array itself (nothing to move); one that holds
+    them in another order goes through the general path and comes back in the workload's
+    order with the workload's pair indices."""
+    from types import SimpleNamespace
+    oracle = importlib.import_module("oracle")
+    shard = importlib.import_module("sherd-refit_b200.shard")
+    backend = importlib.import_module("sherd-refit_b200.backend")
+    workload = importlib.import_module("sherd-refit_b200.workload")
+    wl = small_collection()
+    ctx = _OracleContext(oracle)
+    params = backend.default_params()
+    dev = workload.to_device(ctx, wl, params)
+    got = backend.candidates(ctx.ladder_verify_batch(dev.pairs, dev.items, params))[:wl.n_items]
+    assert shard.gather_candidates(wl, dev, got) is got
+    # The same candidates as a rank that holds the pairs reversed (device pair k is the
+    # workload's pair n - 1 - k) and its items in reverse order.
+    n_pairs = len(wl.pairs)
+    flipped = got[::-1].copy()
+    flipped["pair"] = n_pairs - 1 - flipped["pair"].astype(np.int64)
+    fake = SimpleNamespace(pair_index=np.arange(n_pairs)[::-1].copy(),
+                           item_index=np.arange(wl.n_items)[::-1].copy())
+    back = shard.gather_candidates(wl, fake, flipped)
+    assert back is not flipped and back.tobytes() == got.tobytes()
+
+
 def test_partition_pairs_balances_and_covers():
     shard = importlib.import_module("sherd-refit_b200.shard")
     parts = shard.partition_pairs([5, 1, 4, 2, 3, 3], 2)
