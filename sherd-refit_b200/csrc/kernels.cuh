@@ -355,6 +355,10 @@ __global__ void k_penetration_share(MeshView m, const double *pts, uint32_t n, P
 // default.
 constexpr int LADDER_VARIANTS = 3;
 constexpr int LADDER_MINB[LADDER_VARIANTS] = {6, 8, 10};
+// The variant a bucket runs until the autotuner has timed it (and when it has
+// too few items to time): 8 CTAs per SM, which the 4-wide nearest-point walk
+// made 15-20 % faster than 10 on the collection.
+constexpr int LADDER_DEFAULT = 1;
 
 struct QueueCtl {
   unsigned *head;             // next queue position to take

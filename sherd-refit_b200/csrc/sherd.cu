@@ -1540,7 +1540,7 @@ struct sherd_batch {
       ladder_as<H, LADDER_MINB[2]>(grid, q, s, r_lo, r_hi, skip_partial, slot0);
   }
   void ladder(unsigned grid, QueueCtl q, cudaStream_t s, int r_lo, int r_hi, int skip_partial,
-              int v = LADDER_VARIANTS - 1, size_t slot0 = 0) {
+              int v = LADDER_DEFAULT, size_t slot0 = 0) {
     if (hint16)
       ladder_h<uint16_t>(v, grid, q, s, r_lo, r_hi, skip_partial, slot0);
     else
@@ -1551,7 +1551,7 @@ struct sherd_batch {
   // autotuner) on a grid of its own, its CTAs on a slice of the hint slots.
   static constexpr int BUCKETS = 3;
   uint32_t seg_first[BUCKETS] = {}, seg_count[BUCKETS] = {};
-  int variant[BUCKETS] = {LADDER_VARIANTS - 1, LADDER_VARIANTS - 1, LADDER_VARIANTS - 1};
+  int variant[BUCKETS] = {LADDER_DEFAULT, LADDER_DEFAULT, LADDER_DEFAULT};
   size_t slot0[BUCKETS] = {};
   int occ[LADDER_VARIANTS] = {};  // resident k_ladder CTAs per SM of each variant
   DBuf<unsigned> lheads;          // one queue head per bucket
@@ -1654,8 +1654,8 @@ int launch_ladder(sherd_batch *b, cudaStream_t s) {
 // context has not tuned yet, every k_ladder variant runs the four rungs of the
 // bucket's most expensive items (two full grids' worth, the same items for
 // every variant, after one untimed run), twice, timed by CUDA events on the
-// context's stream; a variant replaces the default (the last, the highest
-// occupancy) only when its faster run beats the default's by TUNE_MARGIN, so
+// context's stream; a variant replaces the default (LADDER_DEFAULT) only when
+// its faster run beats the default's by TUNE_MARGIN, so
 // run-to-run noise does not move the choice. The choice is kept for the bucket
 // on this context. The runs write those items' rungs, which every batch run
 // writes again.
@@ -1676,7 +1676,7 @@ int tune_ladder(sherd_batch *b) {
     for (int k = 0; k < LADDER_VARIANTS; ++k) ms_of[k] = f_inf();
     for (int t = -1; t < 2 * LADDER_VARIANTS; ++t) {
       const int v = t < 0 ? -1 : t % LADDER_VARIANTS;
-      const int run = v < 0 ? LADDER_VARIANTS - 1 : v;
+      const int run = v < 0 ? LADDER_DEFAULT : v;
       const unsigned grid = std::min<unsigned>(unsigned(b->occ[run] * ctx->sm_count), need);
       QueueCtl q{b->lheads.p + bk, b->dorder.p + b->seg_first[bk], need, ctx->abort_dev, 0ull};
       CK(cudaMemsetAsync(b->lheads.p + bk, 0, sizeof(unsigned), s));
@@ -1690,10 +1690,10 @@ int tune_ladder(sherd_batch *b) {
       if (v < 0) continue;  // the untimed first run
       ms_of[v] = std::min(ms_of[v], ms);
     }
-    int pick = LADDER_VARIANTS - 1;
+    int pick = LADDER_DEFAULT;
     for (int v = 0; v < LADDER_VARIANTS; ++v) {
       ctx->ladder_tune_ms[bk][v] = ms_of[v];
-      if (ms_of[v] < ms_of[pick] && ms_of[v] < (1.0f - TUNE_MARGIN) * ms_of[LADDER_VARIANTS - 1])
+      if (ms_of[v] < ms_of[pick] && ms_of[v] < (1.0f - TUNE_MARGIN) * ms_of[LADDER_DEFAULT])
         pick = v;
     }
     ctx->ladder_tuned[bk] = pick;
@@ -1862,7 +1862,7 @@ int batch_create(sherd_ctx *ctx, sherd_pair *const *pairs, uint32_t n_pairs,
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ[2], k_ladder<int, LADDER_MINB[2]>, ICP_BLOCK, 0));
   }
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_v, k_verify_items, VER_BLOCK, 0));
-  b->grid_l = unsigned(std::max(1, b->occ[LADDER_VARIANTS - 1]) * ctx->sm_count);
+  b->grid_l = unsigned(std::max(1, b->occ[LADDER_DEFAULT]) * ctx->sm_count);
   b->grid_v = unsigned(std::max(1, occ_v) * ctx->sm_count);
   CK(b->scratch.alloc(size_t(b->grid_v) * b->max_scratch));
   if (sched == SHERD_SCHED_BATCHED) {
