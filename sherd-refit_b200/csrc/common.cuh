@@ -23,6 +23,12 @@ constexpr int TRI_LEAF = TRI_LEAF_MAX;  // faces per BVH leaf, at most
 #define POINT_LEAF_MAX 2
 #endif
 constexpr int POINT_LEAF = POINT_LEAF_MAX;  // points per BVH leaf, at most
+// Resident 256-thread CTAs per SM k_pen_inside is compiled for (48 registers a
+// thread): 5 measured 916 ms on the collection against 990 with the compiler's
+// own 64 registers (3-4 CTAs) and 1003 at 4; k_pen_min gained nothing at 4-6.
+#ifndef PEN_INSIDE_MINB
+#define PEN_INSIDE_MINB 5
+#endif
 // Whether point clouds carry the 4-wide tree that nearest_within_sq walks.
 #ifndef WIDE_NN
 #define WIDE_NN 1

@@ -757,7 +757,7 @@ __global__ void k_pen_init(PenState ps) {
 }
 
 // Box test, parity, depth: the first pass of one_penetration (verify.rs:541-568).
-__global__ void __launch_bounds__(256) k_pen_inside(const PairView *pairs, const sherd_work_item *items,
+__global__ void __launch_bounds__(256, PEN_INSIDE_MINB) k_pen_inside(const PairView *pairs, const sherd_work_item *items,
                                                     const sherd_candidate *cands, const double *inv,
                                                     PenState ps, unsigned *head,
                                                     const uint32_t *abort_flag,
